@@ -1,0 +1,192 @@
+/*
+ * snapb.h — C ABI of the B200 hydro step (snapy finite-volume forward path).
+ *
+ * Every entry point takes plain device pointers, a pointer to a
+ * snapb_hydro_config and a CUDA stream passed as void* (NULL = legacy default
+ * stream).  No torch types cross this boundary.  Arrays use snapy's layout
+ * [nvar, nc3, nc2, nc1] in row-major order, x1 (vertical) contiguous, with
+ * nc = nx + 2*nghost on active axes and nc = 1 on inactive ones
+ * (reference: src/hydro/hydro.cpp:87-115, src/coord/coordinate.hpp:58-60).
+ * Variable order is IDN=0, IVX=1, IVY=2, IVZ=3, IPR=4 (src/snap.h:34-46).
+ *
+ * Every function returns SNAPB_OK (0) or a non-zero status; snapb_last_error()
+ * gives the message of the last failure on the calling thread.  The caller
+ * owns every buffer; scratch memory is sized with snapb_workspace_size().
+ * Scalars that change every step (dt) are read from DEVICE memory so that a
+ * step can be captured in a CUDA graph and replayed.
+ */
+#ifndef SNAPB_H
+#define SNAPB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SNAPB_ABI_VERSION 1
+
+/* interpolation types; factory: src/recon/interpolation.cpp:11-39 */
+enum {
+  SNAPB_RECON_DC = 0,
+  SNAPB_RECON_PLM = 1,
+  SNAPB_RECON_CP3 = 2,
+  SNAPB_RECON_CP5 = 3,
+  SNAPB_RECON_WENO3 = 4,
+  SNAPB_RECON_WENO5 = 5
+};
+
+/* Riemann solvers; factory: src/riemann/riemann_solver.cpp:47-68 */
+enum {
+  SNAPB_RIEMANN_ROE = 0,
+  SNAPB_RIEMANN_LMARS = 1,
+  SNAPB_RIEMANN_HLLC = 2,
+  SNAPB_RIEMANN_UPWIND = 3
+};
+
+/* external boundary functions; registry: src/bc/bc_func.cpp:4-63 */
+enum {
+  SNAPB_BC_CUSTOM = 0, /* no-op, as custom_inner/custom_outer */
+  SNAPB_BC_REFLECTING = 1,
+  SNAPB_BC_PERIODIC = 2,
+  SNAPB_BC_OUTFLOW = 3
+};
+
+/* variable kinds for boundary fills; src/snap.h:53-62 */
+enum { SNAPB_PRIMITIVE = 0, SNAPB_CONSERVED = 1, SNAPB_SCALAR = 2 };
+
+/* status codes */
+enum {
+  SNAPB_OK = 0,
+  SNAPB_ERR_ARG = 1,
+  SNAPB_ERR_CUDA = 2,
+  SNAPB_ERR_UNSUPPORTED = 3,
+  SNAPB_ERR_WORKSPACE = 4,
+  SNAPB_ERR_TIMEOUT = 5
+};
+
+/*
+ * One mesh block's hydro configuration.  Mirrors the YAML keys that
+ * MeshBlockOptionsImpl::from_yaml reads for this path (geometry.*,
+ * dynamics.equation-of-state.*, dynamics.reconstruct.*,
+ * dynamics.riemann-solver.type, integration.implicit-scheme,
+ * forcing.const-gravity.*, forcing.diffusion.*,
+ * boundary-condition.external.*, scalar.nvar).
+ */
+typedef struct snapb_hydro_config {
+  int32_t nx1, nx2, nx3; /* interior cells per axis; 1 = inactive axis */
+  int32_t nghost;        /* ghost layers on active axes */
+  int32_t nvar;          /* hydro variables (5 for the ideal gas) */
+  int32_t nscalar;       /* passive scalars carried in scalar_s */
+  double x1min, x1max, x2min, x2max, x3min, x3max;
+  double gammad; /* ratio of specific heats */
+  double rgas;   /* specific gas constant R = Rgas / weight (W->T) */
+  int32_t recon1_type, recon1_shock, recon1_scale;    /* vertical (x1) */
+  int32_t recon23_type, recon23_shock, recon23_scale; /* horizontal */
+  int32_t scalar_recon_type, scalar_recon_scale;
+  int32_t riemann;
+  int32_t implicit_scheme; /* 0 none, 1 partial 3x3, 9 full 5x5 */
+  double grav1, grav2, grav3, non_hydrostatic;
+  double nu_iso, kappa_iso;
+  int32_t bc[6]; /* x1-inner, x1-outer, x2-inner, x2-outer, x3-inner, x3-outer */
+  int32_t disable_flux[3];
+  int32_t reserved;
+} snapb_hydro_config;
+
+/* ---- library ---- */
+int snapb_abi_version(void);
+const char* snapb_last_error(void);
+
+/* Bytes of device scratch that snapb_stage / snapb_hydro_forward need. */
+size_t snapb_workspace_size(const snapb_hydro_config* cfg);
+
+/* ---- equation of state (ideal gas) ---- */
+
+/* U -> W over the whole array, ghosts included.
+ * Replaces IdealGasImpl::_cons2prim (src/eos/ideal_gas.cpp:90-109) and the
+ * ideal_gas_cons2prim DispatchStub (src/eos/eos_dispatch.cu:16-30). */
+int snapb_cons2prim(const snapb_hydro_config* cfg, const double* u, double* w,
+                    void* stream);
+
+/* W -> U over the whole array.
+ * Replaces IdealGasImpl::_prim2cons (src/eos/ideal_gas.cpp:67-88). */
+int snapb_prim2cons(const snapb_hydro_config* cfg, const double* w, double* u,
+                    void* stream);
+
+/* ---- operator level (one module call each) ---- */
+
+/* wlr[2, nv, nc3, nc2, nc1] = reconstruction of w along dim (3 = x1, 2 = x2,
+ * 1 = x3).  group 0 = hydro variables with the vertical (dim 3) or horizontal
+ * (dim 1, 2) options; group 1 = passive scalars (interp1 for every variable,
+ * then clamp at 0).  Replaces ReconstructImpl::forward
+ * (src/recon/reconstruct.cpp:75-154) with the call_weno5 / call_poly5 /
+ * PLM stubs it dispatches to (src/recon/recon_dispatch.hpp:9-18). */
+int snapb_reconstruct(const snapb_hydro_config* cfg, int dim, int group,
+                      const double* w, int nv, double* wlr, void* stream);
+
+/* flx[nv, ...] (and face_pressure[nc3, nc2, nc1] when not NULL) from the
+ * left/right states along dim.  solver = SNAPB_RIEMANN_*; for UPWIND `vel`
+ * is the face velocity (mass flux) array.  Replaces
+ * RiemannSolverImpl::forward and the call_hllc / call_lmars / call_roe stubs
+ * (src/riemann/riemann_dispatch.hpp:10-20, src/riemann/hllc.cpp:30-106,
+ * src/riemann/lmars.cpp:30-103, src/riemann/roe.cpp:14-59,
+ * src/riemann/riemann_solver.cpp:544-553). */
+int snapb_riemann(const snapb_hydro_config* cfg, int solver, int dim,
+                  const double* wl, const double* wr, int nv, double* flx,
+                  double* face_pressure, const double* vel, void* stream);
+
+/* ---- block level ---- */
+
+/* Stage tendency du (already multiplied by dt) of the hydro forward step:
+ * cons2prim into w, hydrostatic x1 ghost revision, fused per-direction
+ * reconstruct + Riemann + flux difference, gravity, hydrostatic correction
+ * and the vertically implicit correction.  mass_corr (may be NULL when the
+ * implicit scheme is off) receives the implicit mass fix per cell.
+ * Replaces HydroImpl::forward (src/hydro/hydro_forward.cpp:14-217). */
+int snapb_hydro_forward(const snapb_hydro_config* cfg, const double* dt,
+                        const double* u, double* w, double* du,
+                        double* mass_corr, void* workspace,
+                        size_t workspace_bytes, void* stream);
+
+/* One RK stage of a mesh block, in place: du = forward(u), optional scalar
+ * transport, u = wght0*u0 + wght1*u + wght2*du, boundary fills.  At stage 0
+ * u0 (and s0) are filled from u (and s).  s, s0, r may be NULL when
+ * cfg->nscalar == 0.  Replaces MeshBlockImpl::advance_local
+ * (src/mesh/meshblock.cpp:577-786) with its harp RK3 combination
+ * (stage weights (1,0,1), (3/4,1/4,1/4), (1/3,2/3,2/3)). */
+int snapb_stage(const snapb_hydro_config* cfg, int stage, const double* dt,
+                double* u, double* u0, double* w, double* s, double* s0,
+                double* r, void* workspace, size_t workspace_bytes,
+                void* stream);
+
+/* External boundary fills of var[nv, nc3, nc2, nc1] in the order x1-inner,
+ * x1-outer, x2-inner, x2-outer, x3-inner, x3-outer; kind = SNAPB_PRIMITIVE,
+ * SNAPB_CONSERVED or SNAPB_SCALAR.  Replaces the bfuncs loop
+ * (src/mesh/meshblock.cpp:717-730) over src/bc/bc_func.cpp:7-63. */
+int snapb_bc_apply(const snapb_hydro_config* cfg, double* var, int nv,
+                   int kind, void* stream);
+
+/* Hyperbolic (and diffusive) time-step limit from w, written to *dt_out
+ * (device).  The CFL factor and redo halving are NOT applied.
+ * Replaces HydroImpl::max_time_step (src/hydro/hydro.cpp:118-180) and
+ * DiffusionImpl::max_time_step (src/forcing/diffusion.cpp:242-265). */
+int snapb_max_time_step(const snapb_hydro_config* cfg, const double* w,
+                        double* dt_out, void* workspace,
+                        size_t workspace_bytes, void* stream);
+
+/* dt_out = cfl * 2^-redo * (*dt_in) on the device. */
+int snapb_scale_dt(const double* dt_in, double cfl, int redo, double* dt_out,
+                   void* stream);
+
+/* flags[0] = 1 if min interior density <= 0, flags[1] = 1 if min interior
+ * pressure <= 0 (device ints).  Replaces the tests of
+ * MeshBlockImpl::check_redo (src/mesh/meshblock.cpp:974-1016). */
+int snapb_check_positive(const snapb_hydro_config* cfg, const double* u,
+                         int* flags, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SNAPB_H */
