@@ -1,0 +1,357 @@
+"""Benchmark of the hydro forward step (one JSON line on rank 0).
+
+Workload (default ``c5``): the large single 3-D domain of the benchmark
+configurations — 384 x 384 x 192 cells, H2-He ideal gas, WENO5 + Roe,
+vertically implicit solve (3x3 VIC), 2 passive tracers, doubly periodic,
+synthetic seeded initial state.  A "step" is one RK3 step (3 stages) of the
+whole domain; the unit counts interior cells x RK stages.
+
+Arms:
+  --impl ours       (default) the CUDA path through the C ABI
+  --impl reference  the reference's CPU implementation of the path: the
+                    oracle/_ref build (the reference's own *_impl.h kernels
+                    under the restated orchestration), all host threads, on a
+                    bounded sub-domain of the same workload.
+Multi-GPU: the hydro step is run as independent replicas (one domain per
+rank, no exchange) — ``scaling: weak``.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "Mcell-updates/s batched FP32 vs plain FP64 at rel L1<=1e-5; adjoint/fwd time"
+UNIT = "Mcell-updates/s"
+
+
+WORKLOAD_DESC = {
+    "c5": "large_3d_h2he_384x384x192_weno5_roe_vic3_2tracers",
+    "c5s": "large_3d_h2he_96x96x192_weno5_roe_vic3_2tracers",
+    "c2": "straka_1024x128_weno5_lmars_vic3_diffusion",
+    "c1": "sod_1024_weno5_hllc",
+}
+
+
+def workload(name: str):
+    from snapy_linfel_b200 import problems
+
+    if name == "c5":
+        opts, w, r = problems.large_3d()
+        desc = "large_3d_h2he_384x384x192_weno5_roe_vic3_2tracers"
+    elif name == "c5s":  # smaller variant for quick checks
+        opts, w, r = problems.large_3d(nx3=96, nx2=96, nx1=192)
+        desc = "large_3d_h2he_96x96x192_weno5_roe_vic3_2tracers"
+    elif name == "c2":
+        opts, w, r = problems.straka()
+        desc = "straka_1024x128_weno5_lmars_vic3_diffusion"
+    elif name == "c1":
+        opts, w, r = problems.sod()
+        desc = "sod_1024_weno5_hllc"
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    return opts, w, r, desc
+
+
+def interior_cells(cfg) -> int:
+    return cfg.nx1 * cfg.nx2 * cfg.nx3
+
+
+def algo_bytes_per_cell_update(cfg, elem=8) -> int:
+    """Compulsory traffic of one fused RK stage: read u, read u0, write u."""
+    return 3 * (cfg.nvar + cfg.nscalar) * elem
+
+
+def launches_per_step(cfg) -> int:
+    diff = cfg.nu_iso > 0 or cfg.kappa_iso > 0
+    a2, a3 = cfg.nx2 > 1, cfg.nx3 > 1
+    sep_final = (not a2 and not a3) and diff
+    per_stage = 1 + int(diff) + int(a2) + int(a3) + int(sep_final) + int(cfg.implicit_scheme != 0)
+    per_stage += 1 + int(cfg.nscalar > 0)  # boundary fills of u (and s)
+    return 3 * per_stage + 4  # + CFL fill / reduce / final + dt scaling
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            f = [x.strip() for x in ln.split(",")]
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# --------------------------------------------------------------------------
+# CPU arm / baseline (the checker's builds; only bench.py's baseline legs run them)
+# --------------------------------------------------------------------------
+def cpu_sample_run(kind: str, steps: int, warmup: int, threads: int | None = None,
+                   nx_h: int = 64):
+    """Time RK3 steps of a bounded sub-domain (nx_h x nx_h x 192) on the host."""
+    from oracle.pyoracle import Oracle
+    from snapy_linfel_b200 import problems
+    from snapy_linfel_b200.config import CONSERVED, PRIMITIVE, SCALAR
+
+    orc = Oracle(kind)
+    nthreads = threads or os.cpu_count() or 1
+    orc.set_threads(nthreads)
+    opts, w, r = problems.large_3d(nx3=nx_h, nx2=nx_h, nx1=192)
+    c = opts.hydro
+    orc.bc_apply(c, w, PRIMITIVE)
+    orc.bc_apply(c, r, SCALAR)
+    u = orc.prim2cons(c, w)
+    s = w[0:1] * r
+    orc.bc_apply(c, u, CONSERVED)
+    orc.bc_apply(c, s, SCALAR)
+    u0, s0 = np.empty_like(u), np.empty_like(s)
+    blk = orc.block(c)
+    times = []
+    for n in range(warmup + steps):
+        t0 = time.perf_counter()
+        dt = opts.integration.cfl * orc.max_time_step(c, w)
+        for st in range(3):
+            blk.stage(st, dt, u, u0, w, s, s0, r)
+        if n >= warmup:
+            times.append(time.perf_counter() - t0)
+    cells = interior_cells(c)
+    per_step = statistics.median(times)
+    value = cells * 3 / per_step / 1e6
+    sample = (f"{nx_h}x{nx_h}x192 sub-domain of the same workload (WENO5+Roe+VIC3+2 tracers), "
+              f"{steps} RK3 step(s), median wall time")
+    return value, per_step, nthreads, sample, orc.kind
+
+
+def run_reference(args):
+    from oracle.pyoracle import lib_path
+
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    desc = WORKLOAD_DESC[args.workload]
+    kind = "reference" if os.path.exists(lib_path("reference")) else "port"
+    value, per_step, cores, sample, _ = cpu_sample_run(kind, args.steps, args.warmup)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": per_step * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": desc, "form": "plain_fp64", "cpu_sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------
+# GPU arm
+# --------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from snapy_linfel_b200 import _lib
+    from snapy_linfel_b200.mesh import MeshBlock
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    opts, w, r, desc = workload(args.workload)
+    cfg = opts.hydro
+    mb = MeshBlock(opts, device=f"cuda:{local}")
+    mb.initialize(w, r)
+    del w
+    cells = interior_cells(cfg)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-resident throughput (value) ----
+    for _ in range(args.warmup):
+        mb.step()
+    barrier()
+    _lib.timing_enable(True)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            mb.step()
+        ev1.record(stream)
+        barrier()
+    ms = ev0.elapsed_time(ev1)
+    kern = _lib.timing_query()
+    _lib.timing_enable(False)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = t.item()
+    value = world * cells * 3 * args.steps / (ms_max / 1e3) / 1e6
+
+    # ---- end to end through the public API with host buffers ----
+    hu = torch.empty(cfg.shape, dtype=torch.float64).pin_memory()
+    hu.copy_(mb.hydro_u.cpu())
+    hs = None
+    if cfg.nscalar:
+        hs = torch.empty(cfg.scalar_shape, dtype=torch.float64).pin_memory()
+        hs.copy_(mb.scalar_s.cpu())
+    h2d = hu.numel() * 8 + (hs.numel() * 8 if hs is not None else 0)
+    d2h = h2d
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        mb.hydro_u.copy_(hu, non_blocking=True)
+        if hs is not None:
+            mb.scalar_s.copy_(hs, non_blocking=True)
+        mb.step()
+        hu.copy_(mb.hydro_u, non_blocking=True)
+        if hs is not None:
+            hs.copy_(mb.scalar_s, non_blocking=True)
+    e1.record(stream)
+    barrier()
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e = world * cells * 3 * args.steps / (t.item() / 1e3) / 1e6
+
+    # ---- roofline of the dominant kernel (live CUDA-event durations) ----
+    peak, peak_src = measured_peaks()
+    top = max(kern.items(), key=lambda kv: kv[1][0]) if kern else None
+    roof = None
+    if top:
+        name, (tot_ms, n) = top
+        per_launch_s = tot_ms / n / 1e3
+        bytes_launch = algo_bytes_per_cell_update(cfg) * cells
+        ach = bytes_launch / per_launch_s / 1e9
+        roof = {"kernel": name, "bound": "hbm", "achieved": ach, "peak": peak,
+                "peak_source": peak_src, "unit": "GB/s", "frac": ach / peak,
+                "traffic": None, "algorithmic_bytes_per_cell_update":
+                    algo_bytes_per_cell_update(cfg)}
+    stage_s = ms_max / 1e3 / (3 * args.steps)
+    stage_bw = algo_bytes_per_cell_update(cfg) * cells / stage_s / 1e9
+    kern_ms = {k: round(v[0] / v[1], 4) for k, v in kern.items()}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            from oracle.pyoracle import lib_path
+
+            kind = "reference" if os.path.exists(lib_path("reference")) else "port"
+            v, per_step, cores, sample, _ = cpu_sample_run(kind, 1, 0)
+            cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": UNIT, "cores": None, "kind": None,
+                   "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": desc, "form": "plain_fp64",
+                       "cells_per_gpu": cells, "rk_stages_per_step": 3,
+                       "l2_policy": "inputs larger than L2 (state > 126 MB)",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": roof,
+            "stage_roofline": {"achieved": stage_bw, "peak": peak, "unit": "GB/s",
+                               "frac": stage_bw / peak},
+            "kernel_ms_per_launch": kern_ms,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches_per_step(cfg) * args.steps,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c5")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -149,6 +149,21 @@ int snapb_hydro_forward(const snapb_hydro_config* cfg, const double* dt,
                         double* mass_corr, void* workspace,
                         size_t workspace_bytes, void* stream);
 
+/* Vertically implicit correction of a stage tendency, in place.  du holds
+ * -dt*div + forcing on interior cells; on return its interior carries the
+ * VIC result (block-tridiagonal solve per x1 column, 3x3 for scheme 1, 5x5
+ * for scheme 9, then the MS-VIC mass redistribution).  w must hold the
+ * primitive state including the x1 ghost cells.  mass_corr (NULL allowed,
+ * [nvar, nc3, nc2, nc1]) receives the mass fix in its IDN row at interior
+ * cells; other entries are left untouched.  The workspace must hold
+ * snapb_workspace_size(cfg) bytes.  Replaces ImplicitHydroImpl::forward
+ * (src/implicit/implicit_hydro.cpp:99-189), which returns du_new - du_old
+ * instead of updating du. */
+int snapb_implicit_correction(const snapb_hydro_config* cfg, const double* dt,
+                              double* du, const double* w, double* mass_corr,
+                              void* workspace, size_t workspace_bytes,
+                              void* stream);
+
 /* One RK stage of a mesh block, in place: du = forward(u), optional scalar
  * transport, u = wght0*u0 + wght1*u + wght2*du, boundary fills.  At stage 0
  * u0 (and s0) are filled from u (and s).  s, s0, r may be NULL when
@@ -179,11 +194,32 @@ int snapb_max_time_step(const snapb_hydro_config* cfg, const double* w,
 int snapb_scale_dt(const double* dt_in, double cfl, int redo, double* dt_out,
                    void* stream);
 
-/* flags[0] = 1 if min interior density <= 0, flags[1] = 1 if min interior
- * pressure <= 0 (device ints).  Replaces the tests of
- * MeshBlockImpl::check_redo (src/mesh/meshblock.cpp:974-1016). */
+/* Positivity screen of the interior (device ints): flags[0] = 1 if some
+ * density <= 0, flags[1] = 1 if some total energy <= 0, flags[2] = 1 if some
+ * cons2prim pressure <= 0.  A step is redone when flags[0] || (flags[1] &&
+ * flags[2]), as MeshBlockImpl::check_redo decides
+ * (src/mesh/meshblock.cpp:974-1016). */
 int snapb_check_positive(const snapb_hydro_config* cfg, const double* u,
                          int* flags, void* stream);
+
+/* ---- diagnostics: per-kernel device time ----
+ * While enabled, snapb_stage and snapb_hydro_forward record a CUDA event pair
+ * around every kernel they launch.  snapb_timing_query synchronizes those
+ * events and returns the summed device milliseconds and the launch count of
+ * one kernel kind.  Enabling clears the record.  (Plays the role of the
+ * reference's verbose phase timers, src/hydro/hydro_forward.cpp:26-31.) */
+enum {
+  SNAPB_K_X1 = 0,   /* U->W + x1 sweep */
+  SNAPB_K_DIFF = 1, /* diffusion fluxes */
+  SNAPB_K_X2 = 2,   /* x2 sweep */
+  SNAPB_K_X3 = 3,   /* x3 sweep */
+  SNAPB_K_FINAL = 4,
+  SNAPB_K_VIC = 5,  /* implicit column solve */
+  SNAPB_K_BC = 6,   /* boundary fills */
+  SNAPB_K_COUNT = 7
+};
+int snapb_timing_enable(int on);
+int snapb_timing_query(int kernel, double* total_ms, int* launches);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,74 @@
+// kernels.cuh — launchers shared between the translation units of libsnapb.
+#pragma once
+
+#include <string>
+
+#include "common.cuh"
+
+namespace snapb {
+
+// Device buffers of one RK stage.  State arrays are caller-owned; the rest
+// live in the workspace (see ws_layout in capi.cu).
+struct StageBufs {
+  const double* dt;  // device scalar
+  double* u;         // hydro_u, updated in place
+  double* u0;        // hydro_u at stage 0 (interior kept)
+  double* w;         // hydro_w, written from u
+  double* s;         // scalar_s (nscalar vars) or null
+  double* s0;
+  double* r;         // scalar_r of the previous stage (mass-correction term)
+  double* D;         // [nvar + nscalar][sv] flux-difference sums, then du
+  double* RG;        // [sv] hydrostatic correction rho_grav
+  double* DD;        // [nvar][sv] diffusion flux differences (undivided)
+  double* R;         // [nscalar][sv] scalar mixing ratio of the stage input
+  double* M;         // [nvar][sv] implicit mass correction (IDN row used)
+  double* vic;       // implicit-solve scratch
+  int stage;
+  double wgt0, wgt1, wgt2;
+  int write_du;      // 1: finalize writes du into D instead of updating u
+  int vic_du_only;   // 1: the implicit solve leaves du in D (no RK update)
+};
+
+// RK3 (Shu-Osher) stage weights: u = wgt0*u0 + wgt1*u + wgt2*du
+inline void rk3_weights(int stage, double& a, double& b, double& c) {
+  static const double W[3][3] = {{1., 0., 1.}, {3. / 4., 1. / 4., 1. / 4.},
+                                 {1. / 3., 2. / 3., 2. / 3.}};
+  a = W[stage][0];
+  b = W[stage][1];
+  c = W[stage][2];
+}
+
+// launchers (return a cudaError_t of the launch)
+cudaError_t launch_x1(const Geo& g, const Phys& p, const StageBufs& b, bool last,
+                      cudaStream_t st);
+cudaError_t launch_c2p_only(const Geo& g, const Phys& p, const StageBufs& b, cudaStream_t st);
+cudaError_t launch_march(int axis, const Geo& g, const Phys& p, const StageBufs& b, bool first,
+                         bool last, cudaStream_t st);
+cudaError_t launch_finalize(const Geo& g, const Phys& p, const StageBufs& b, cudaStream_t st);
+cudaError_t launch_diffusion(const Geo& g, const Phys& p, const StageBufs& b, cudaStream_t st);
+cudaError_t launch_vic(const Geo& g, const Phys& p, const StageBufs& b, cudaStream_t st);
+size_t vic_scratch_bytes(const Geo& g, const Phys& p);
+
+cudaError_t launch_cons2prim(const Geo& g, const Phys& p, const double* u, double* w,
+                             cudaStream_t st);
+cudaError_t launch_prim2cons(const Geo& g, const Phys& p, const double* w, double* u,
+                             cudaStream_t st);
+cudaError_t launch_bc(const Geo& g, const snapb_hydro_config& c, double* var, int nv, int kind,
+                      cudaStream_t st);
+cudaError_t launch_cfl(const Geo& g, const Phys& p, const double* w, double* slots,
+                       double* dt_out, cudaStream_t st);
+cudaError_t launch_scale_dt(const double* dt_in, double cfl, int redo, double* dt_out,
+                            cudaStream_t st);
+cudaError_t launch_check_positive(const Geo& g, const Phys& p, const double* u, int* flags,
+                                  cudaStream_t st);
+cudaError_t launch_reconstruct(const Geo& g, const Phys& p, int dim, int group, const double* w,
+                               int nv, double* wlr, cudaStream_t st);
+cudaError_t launch_riemann(const Geo& g, const Phys& p, int solver, int dim, const double* wl,
+                           const double* wr, int nv, double* flx, double* fp, const double* vel,
+                           cudaStream_t st);
+
+// bytes of dynamic shared memory the x1 column kernel needs per column
+size_t x1_smem_per_column(const Geo& g, int nvt);
+int x1_columns_per_cta(const Geo& g, int nvt);
+
+}  // namespace snapb

@@ -1,0 +1,459 @@
+// vic.cu — vertically implicit correction (VIC) of one RK stage, FP64.
+//
+// One thread owns one x1 column (the vertical, contiguous axis).  It assembles
+// the block-tridiagonal rows on the fly while it runs the block-Thomas forward
+// elimination, so every Roe eigen-decomposition |A| = R |Lambda| R^-1 is
+// computed once per interface instead of twice; the reduced blocks
+// a'_i = (a_i - b_i a'_{i-1})^-1 c_i and the partial solutions delta_i go to a
+// workspace laid out [layer][entry][column] so that the 32 columns of a warp
+// hit consecutive addresses.  Back substitution, the per-column MS-VIC sums,
+// the mass redistribution and the RK combination follow in the same thread.
+//
+// Reference: ImplicitHydroImpl::forward (src/implicit/implicit_hydro.cpp:99-189),
+// vic_assemble_partial_impl (src/implicit/vic_assemble_partial_impl.h:29-111),
+// vic_assemble_full_impl (src/implicit/vic_assemble_full_impl.h:16-106),
+// ForwardSweep (src/implicit/forward_sweep_impl.h:20-109), ludcmp/lubksb
+// (src/math/ludcmp.h:24-76, src/math/lubksb.h:124-147),
+// vic_backward_reduce / vic_redistribute_cell (src/implicit/vic_redistribute_impl.h:26-106),
+// flux Jacobian and Roe eigenvectors (src/implicit/flux_decomposition_impl.h:133-245).
+#include "kernels.cuh"
+
+namespace snapb {
+
+// rows / columns of the 5x5 system kept by the N-block form: N = 3 keeps
+// (IDN, IVX, IPR), N = 5 keeps everything
+template <int N>
+__device__ __forceinline__ int sel(int r) {
+  if constexpr (N == 3) return r == 2 ? IPR : r;
+  return r;
+}
+
+// N x N block of the x1 flux Jacobian dF/dU at primitive state w
+template <int N>
+__device__ __forceinline__ void jac_block(double gm1, const double* w, double (&J)[N][N]) {
+  double v1 = w[IVX], v2 = w[IVY], v3 = w[IVZ], rho = w[IDN], pres = w[IPR];
+  double s2 = v1 * v1 + v2 * v2 + v3 * v3;
+  double hp = (gm1 + 1) / gm1 * pres / rho;
+  double c1 = ((gm1 - 1) * s2 / 2 - hp) * v1;
+  double c2 = hp + s2 / 2 - gm1 * v1 * v1;
+  double full[5][5] = {{0., 1., 0., 0., 0.},
+                       {gm1 * s2 / 2 - v1 * v1, (2. - gm1) * v1, -gm1 * v2, -gm1 * v3, gm1},
+                       {-v1 * v2, v2, v1, 0., 0.},
+                       {-v1 * v3, v3, 0., v1, 0.},
+                       {c1, c2, -gm1 * v2 * v1, -gm1 * v3 * v1, (gm1 + 1) * v1}};
+#pragma unroll
+  for (int r = 0; r < N; ++r)
+#pragma unroll
+    for (int q = 0; q < N; ++q) J[r][q] = full[sel<N>(r)][sel<N>(q)];
+}
+
+// N x N block of |A| = R |Lambda| R^-1 at the Roe average of (wl, wr)
+template <int N>
+__device__ __forceinline__ void absA_block(double gm1, const double* wl, const double* wr,
+                                           double (&A)[N][N]) {
+  double sdl = sqrt(wl[IDN]), sdr = sqrt(wr[IDN]);
+  double isd = 1.0 / (sdl + sdr);
+  double r = sdl * sdr;
+  double u = (sdl * wl[IVX] + sdr * wr[IVX]) * isd;
+  double v = (sdl * wl[IVY] + sdr * wr[IVY]) * isd;
+  double w = (sdl * wl[IVZ] + sdr * wr[IVZ]) * isd;
+  double el = wl[IPR] / gm1 + 0.5 * wl[IDN] * (sqr(wl[IVX]) + sqr(wl[IVY]) + sqr(wl[IVZ]));
+  double er = wr[IPR] / gm1 + 0.5 * wr[IDN] * (sqr(wr[IVX]) + sqr(wr[IVY]) + sqr(wr[IVZ]));
+  double hbar = ((el + wl[IPR]) / sdl + (er + wr[IPR]) / sdr) * isd;
+  double p = (hbar - 0.5 * (u * u + v * v + w * w)) * gm1 / (gm1 + 1.) * r;
+  double cs = sqrt(p * (gm1 + 1.) / r);
+  double lam[5] = {fabs(u - cs), fabs(u), fabs(u + cs), fabs(u), fabs(u)};
+  double ke = 0.5 * (u * u + v * v + w * w);
+  double hp = (gm1 + 1.) / gm1 * p / r;
+  double h = hp + ke;
+  double i2chp = 1. / (2. * cs * hp), ihp = 1. / hp, i2hp = 0.5 * ihp;
+  double R[5][5] = {{1., 1., 1., 0., 0.},
+                    {u - cs, u, u + cs, 0., 0.},
+                    {v, v, v, 1., 0.},
+                    {w, w, w, 0., 1.},
+                    {h - u * cs, ke, h + u * cs, v, w}};
+  double Ri[5][5] = {{(cs * ke + u * hp) * i2chp, (-hp - cs * u) * i2chp, -v * i2hp, -w * i2hp,
+                      i2hp},
+                     {(hp - ke) * ihp, u * ihp, v * ihp, w * ihp, -ihp},
+                     {(cs * ke - u * hp) * i2chp, (hp - cs * u) * i2chp, -v * i2hp, -w * i2hp,
+                      i2hp},
+                     {-v, 0., 1., 0., 0.},
+                     {-w, 0., 0., 1., 0.}};
+#pragma unroll
+  for (int a = 0; a < N; ++a)
+#pragma unroll
+    for (int b = 0; b < N; ++b) {
+      int ra = sel<N>(a), cb = sel<N>(b);
+      double s = 0.;
+#pragma unroll
+      for (int k = 0; k < 5; ++k) s += (R[ra][k] * lam[k]) * Ri[k][cb];
+      A[a][b] = s;
+    }
+}
+
+// X = M^-1 [C | rhs] for an N x N block: cofactor inverse for N = 3,
+// LU with implicit-scaling partial pivoting (Crout) for N = 5
+template <int N>
+__device__ __forceinline__ void block_solve(double (&M)[N][N], double (&C)[N][N],
+                                            double (&rhs)[N]) {
+  if constexpr (N == 3) {
+    auto cof = [&](int i, int j) {
+      int i1 = (i + 1) % 3, i2 = (i + 2) % 3, j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+      return M[i1][j1] * M[i2][j2] - M[i1][j2] * M[i2][j1];
+    };
+    double c00 = cof(0, 0), c10 = cof(1, 0), c20 = cof(2, 0);
+    double det = c00 * M[0][0] + c10 * M[1][0] + c20 * M[2][0];
+    double id = 1. / det;
+    double inv[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) inv[i][j] = cof(j, i) * id;
+    double x[3], X[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      x[i] = inv[i][0] * rhs[0] + inv[i][1] * rhs[1] + inv[i][2] * rhs[2];
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+        X[i][j] = inv[i][0] * C[0][j] + inv[i][1] * C[1][j] + inv[i][2] * C[2][j];
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      rhs[i] = x[i];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) C[i][j] = X[i][j];
+    }
+  } else {
+    double vv[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      double big = 0.;
+#pragma unroll
+      for (int j = 0; j < N; ++j) big = fmax(big, fabs(M[i][j]));
+      vv[i] = 1.0 / big;
+    }
+    int indx[N];
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+#pragma unroll
+      for (int i = 0; i < j; ++i) {
+        double s = M[i][j];
+#pragma unroll
+        for (int k = 0; k < i; ++k) s -= M[i][k] * M[k][j];
+        M[i][j] = s;
+      }
+      double big = 0.;
+      int imax = j;
+#pragma unroll
+      for (int i = j; i < N; ++i) {
+        double s = M[i][j];
+#pragma unroll
+        for (int k = 0; k < j; ++k) s -= M[i][k] * M[k][j];
+        M[i][j] = s;
+        double d = vv[i] * fabs(s);
+        if (d >= big) {
+          big = d;
+          imax = i;
+        }
+      }
+      // row swap j <-> imax done with selects so the arrays stay in registers
+#pragma unroll
+      for (int i = j + 1; i < N; ++i) {
+        if (i == imax) {
+#pragma unroll
+          for (int k = 0; k < N; ++k) {
+            double t = M[i][k];
+            M[i][k] = M[j][k];
+            M[j][k] = t;
+          }
+          double t = vv[i];
+          vv[i] = vv[j];
+          vv[j] = t;
+        }
+      }
+      indx[j] = imax;
+      if (j != N - 1) {
+        double d = 1.0 / M[j][j];
+#pragma unroll
+        for (int i = j + 1; i < N; ++i) M[i][j] *= d;
+      }
+    }
+    // forward / back substitution on the N+1 columns [C | rhs]
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      int ip = indx[i];
+#pragma unroll
+      for (int r2 = i + 1; r2 < N; ++r2) {
+        if (r2 == ip) {
+#pragma unroll
+          for (int c = 0; c < N; ++c) {
+            double t = C[r2][c];
+            C[r2][c] = C[i][c];
+            C[i][c] = t;
+          }
+          double t = rhs[r2];
+          rhs[r2] = rhs[i];
+          rhs[i] = t;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < i; ++j) {
+#pragma unroll
+        for (int c = 0; c < N; ++c) C[i][c] -= M[i][j] * C[j][c];
+        rhs[i] -= M[i][j] * rhs[j];
+      }
+    }
+#pragma unroll
+    for (int i = N - 1; i >= 0; --i) {
+#pragma unroll
+      for (int j = i + 1; j < N; ++j) {
+#pragma unroll
+        for (int c = 0; c < N; ++c) C[i][c] -= M[i][j] * C[j][c];
+        rhs[i] -= M[i][j] * rhs[j];
+      }
+      double d = 1. / M[i][i];
+#pragma unroll
+      for (int c = 0; c < N; ++c) C[i][c] *= d;
+      rhs[i] *= d;
+    }
+  }
+}
+
+size_t vic_scratch_bytes(const Geo& g, const Phys& p) {
+  if (p.implicit_scheme == 0) return 0;
+  int N = ((p.implicit_scheme >> 3) & 1) ? 5 : 3;
+  int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
+  return (size_t)g.nx1 * (N * N + N) * ncol * sizeof(double);
+}
+
+template <int N, int NS>
+__global__ void __launch_bounds__(128) k_vic(Geo g, Phys p, StageBufs b) {
+  const int nj = g.ju - g.jl + 1, nk = g.ku - g.kl + 1;
+  const int64_t ncol = (int64_t)nj * nk;
+  const int64_t col = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= ncol) return;
+  const int j = g.jl + (int)(col % nj), k = g.kl + (int)(col / nj);
+  const int64_t c0 = (int64_t)k * g.s3 + (int64_t)j * g.s2 + g.il;  // cell (k, j, il)
+  const int64_t sv = g.sv;
+  const int nl = g.nx1;
+  constexpr int NE = N * N + N;
+  double* S = b.vic;
+  auto sc = [&](int i, int e) -> double& { return S[((int64_t)i * NE + e) * ncol + col]; };
+
+  const double dt = *b.dt;
+  const double gm1c = p.gammad - 1.;
+  const double gm1f = 0.5 * (p.gammad + p.gammad) - 1.;
+  const double Aa = g.A1;  // uniform face area: (A_{i+1} - A_i) J_i vanishes
+  const double hiv = 0.5 / g.vol;
+  const double idt = 1. / dt;
+  const double grav = p.grav1;
+  double bnd[N];
+#pragma unroll
+  for (int r = 0; r < N; ++r) bnd[r] = r == 1 ? -1. : 1.;
+
+  auto prim = [&](int i, double* o) {
+#pragma unroll
+    for (int v = 0; v < 5; ++v) o[v] = b.w[v * sv + c0 + i];
+  };
+
+  double wm[5], wc[5], wp[5];
+  prim(-1, wm);
+  prim(0, wc);
+  double Jp[N][N], Am[N][N];
+  jac_block<N>(gm1c, wm, Jp);
+  absA_block<N>(gm1f, wm, wc, Am);
+  double Jc[N][N];
+  jac_block<N>(gm1c, wc, Jc);
+  double ap[N][N], dp[N];
+
+  // ---- assembly + forward elimination ----
+  for (int i = 0; i < nl; ++i) {
+    prim(i + 1, wp);
+    double Jn[N][N], Ap[N][N];
+    jac_block<N>(gm1c, wp, Jn);
+    absA_block<N>(gm1f, wc, wp, Ap);
+    double a[N][N], bb[N][N], c[N][N];
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        double phi = 0.;
+        if (r == 1 && q == 0) phi = grav;
+        if (r == 2 && q == 1 && N == 3) phi = grav;
+        if (N == 5 && r == IPR && q == IVX) phi = grav;
+        a[r][q] = (Am[r][q] * Aa + Ap[r][q] * Aa) * hiv - phi;
+        bb[r][q] = -(Am[r][q] + Jp[r][q]) * Aa * hiv;
+        c[r][q] = -(Ap[r][q] - Jn[r][q]) * Aa * hiv;
+      }
+#pragma unroll
+    for (int r = 0; r < N; ++r) a[r][r] += idt;
+    if (i == 0) {
+#pragma unroll
+      for (int r = 0; r < N; ++r)
+#pragma unroll
+        for (int q = 0; q < N; ++q) a[r][q] += bb[r][q] * bnd[q];
+    }
+    if (i == nl - 1) {
+#pragma unroll
+      for (int r = 0; r < N; ++r)
+#pragma unroll
+        for (int q = 0; q < N; ++q) a[r][q] += c[r][q] * bnd[q];
+    }
+    double rhs[N];
+#pragma unroll
+    for (int r = 0; r < N; ++r) rhs[r] = b.D[sel<N>(r) * sv + c0 + i] / dt;
+    if (i > 0) {
+#pragma unroll
+      for (int r = 0; r < N; ++r) {
+        double bd = 0.;
+#pragma unroll
+        for (int q = 0; q < N; ++q) {
+          double t = 0.;
+#pragma unroll
+          for (int kk = 0; kk < N; ++kk) t += bb[r][kk] * ap[kk][q];
+          a[r][q] -= t;
+          bd += bb[r][q] * dp[q];
+        }
+        rhs[r] = rhs[r] - bd;
+      }
+    }
+    block_solve<N>(a, c, rhs);
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      dp[r] = rhs[r];
+      sc(i, N * N + r) = rhs[r];
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        ap[r][q] = c[r][q];
+        sc(i, r * N + q) = c[r][q];
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        Am[r][q] = Ap[r][q];
+        Jp[r][q] = Jc[r][q];
+        Jc[r][q] = Jn[r][q];
+      }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      wm[v] = wc[v];
+      wc[v] = wp[v];
+    }
+  }
+
+  // ---- back substitution + column sums ----
+  double sum_a2 = 0., b_dry = 0.;
+  double dn[N];
+#pragma unroll
+  for (int r = 0; r < N; ++r) dn[r] = dp[r];
+  {
+    double rho = b.w[IDN * sv + c0 + nl - 1];
+    double ai = rho * g.vol;
+    sum_a2 += ai * ai;
+    b_dry += (b.D[IDN * sv + c0 + nl - 1] - dn[0]) * 1. * g.vol;
+  }
+  for (int i = nl - 2; i >= 0; --i) {
+    double d[N];
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      double t = 0.;
+#pragma unroll
+      for (int q = 0; q < N; ++q) t += sc(i, r * N + q) * dn[q];
+      d[r] = sc(i, N * N + r) - t;
+    }
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      dn[r] = d[r];
+      sc(i, N * N + r) = d[r];
+    }
+    double rho = b.w[IDN * sv + c0 + i];
+    double ai = rho * g.vol;
+    sum_a2 += ai * ai;
+    b_dry += (b.D[IDN * sv + c0 + i] - d[0]) * 1. * g.vol;
+  }
+
+  // ---- redistribution + scalar mass fix + RK combination ----
+  for (int i = 0; i < nl; ++i) {
+    const int64_t off = c0 + i;
+    double d[N];
+#pragma unroll
+    for (int r = 0; r < N; ++r) d[r] = sc(i, N * N + r);
+    double rho = b.w[IDN * sv + off];
+    double ai = rho * g.vol;
+    double et = b.D[IDN * sv + off];
+    double fix = d[0] - et;
+    double du[5];
+    du[IDN] = et + fix * 1. + rho * ai * b_dry / sum_a2;
+    if constexpr (N == 3) {
+      du[IVX] = d[1];
+      du[IVY] = b.D[IVY * sv + off];
+      du[IVZ] = b.D[IVZ * sv + off];
+      du[IPR] = d[2];
+    } else {
+#pragma unroll
+      for (int v = 1; v < 5; ++v) du[v] = d[v];
+    }
+    if (b.M) b.M[IDN * sv + off] = fix;
+    if (b.vic_du_only) {
+#pragma unroll
+      for (int v = 0; v < 5; ++v) b.D[v * sv + off] = du[v];
+      continue;
+    }
+    double unew_rho = 0.;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      int64_t o = v * sv + off;
+      double uo = b.u[o];
+      double u0v;
+      if (b.stage == 0) {
+        u0v = uo;
+        b.u0[o] = uo;
+      } else {
+        u0v = b.u0[o];
+      }
+      double un = b.wgt0 * u0v + b.wgt1 * uo + b.wgt2 * du[v];
+      b.u[o] = un;
+      if (v == IDN) unew_rho = un;
+    }
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+      int64_t o = n * sv + off;
+      double ds = b.D[(5 + n) * sv + off] + fix * b.r[o];
+      double so = b.s[o];
+      double s0v;
+      if (b.stage == 0) {
+        s0v = so;
+        b.s0[o] = so;
+      } else {
+        s0v = b.s0[o];
+      }
+      double sn = b.wgt0 * s0v + b.wgt1 * so + b.wgt2 * ds;
+      b.s[o] = sn;
+      b.r[o] = sn / unew_rho;
+    }
+  }
+}
+
+template <int N>
+static cudaError_t launch_vic_n(const Geo& g, const Phys& p, const StageBufs& b,
+                                cudaStream_t st) {
+  int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
+  unsigned grid = (unsigned)((ncol + 127) / 128);
+  switch (p.nscalar) {
+    case 0: k_vic<N, 0><<<grid, 128, 0, st>>>(g, p, b); break;
+    case 1: k_vic<N, 1><<<grid, 128, 0, st>>>(g, p, b); break;
+    case 2: k_vic<N, 2><<<grid, 128, 0, st>>>(g, p, b); break;
+    case 3: k_vic<N, 3><<<grid, 128, 0, st>>>(g, p, b); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_vic(const Geo& g, const Phys& p, const StageBufs& b, cudaStream_t st) {
+  if ((p.implicit_scheme >> 3) & 1) return launch_vic_n<5>(g, p, b, st);
+  return launch_vic_n<3>(g, p, b, st);
+}
+
+}  // namespace snapb

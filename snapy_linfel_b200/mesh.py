@@ -1,0 +1,154 @@
+"""Python mirror of snapy's MeshBlock for the hydro forward step.
+
+``MeshBlock`` owns the block state on one GPU (``hydro_u``, ``hydro_w``,
+``scalar_s``, ``scalar_r``, the stage-0 copies and the workspace) and drives
+the C ABI: ``initialize`` (MeshBlockImpl::initialize,
+src/mesh/meshblock.cpp:330-500), ``max_time_step``
+(src/mesh/meshblock.cpp:511-529), ``forward(dt, stage)`` (advance_local,
+src/mesh/meshblock.cpp:577-786) and ``check_redo``
+(src/mesh/meshblock.cpp:974-1016).  dt lives on the device between the CFL
+reduction and the stages, so a whole step can be captured in a CUDA graph.
+"""
+from __future__ import annotations
+
+import ctypes
+
+from . import _lib
+from .config import CONSERVED, PRIMITIVE, SCALAR, HydroConfig, MeshBlockOptions
+
+
+class MeshBlock:
+    def __init__(self, options: MeshBlockOptions | HydroConfig, device=None):
+        import torch
+
+        if isinstance(options, HydroConfig):
+            options = MeshBlockOptions(options)
+        self.options = options
+        self.cfg = options.hydro
+        self.device = torch.device(device if device is not None else "cuda")
+        if self.device.type != "cuda":
+            raise _lib.SnapbError("MeshBlock runs on CUDA devices only")
+        self.lib = _lib.lib()
+        c = self.cfg
+        f64 = dict(dtype=torch.float64, device=self.device)
+        self.hydro_u = torch.zeros(c.shape, **f64)
+        self.hydro_w = torch.zeros(c.shape, **f64)
+        self.hydro_u0 = torch.zeros(c.shape, **f64)
+        ns = c.nscalar
+        self.scalar_s = torch.zeros(c.scalar_shape, **f64) if ns else None
+        self.scalar_s0 = torch.zeros(c.scalar_shape, **f64) if ns else None
+        self.scalar_r = torch.zeros(c.scalar_shape, **f64) if ns else None
+        nbytes = self.lib.snapb_workspace_size(ctypes.byref(c))
+        if nbytes == 0:
+            raise _lib.SnapbError("invalid configuration: " + self.lib.snapb_last_error().decode())
+        self.workspace = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        self.dt_raw = torch.zeros(1, **f64)   # CFL limit before the cfl factor
+        self.dt = torch.zeros(1, **f64)       # the step's dt
+        self.flags = torch.zeros(4, dtype=torch.int32, device=self.device)
+        self.cycle = 0
+        self.current_redo = 0
+
+    # ---- helpers ----
+    def _call(self, name, *args):
+        rc = getattr(self.lib, name)(*args)
+        _lib.check(rc, name)
+
+    def _stream(self):
+        return _lib.stream_ptr()
+
+    def _ws(self):
+        return _lib.ptr(self.workspace), ctypes.c_size_t(self.workspace.numel())
+
+    # ---- MeshBlockImpl::initialize ----
+    def initialize(self, hydro_w, scalar_r=None):
+        """Primitive BCs on w, W->U, conserved BCs on u (and scalar_s = rho r)."""
+        import torch
+
+        c = self.cfg
+        self.hydro_w.copy_(torch.as_tensor(hydro_w, dtype=torch.float64))
+        st = self._stream()
+        self._call("snapb_bc_apply", ctypes.byref(c), _lib.ptr(self.hydro_w), c.nvar, PRIMITIVE, st)
+        if c.nscalar:
+            if scalar_r is None:
+                raise _lib.SnapbError("initialize: scalar_r is required for scalar model")
+            self.scalar_r.copy_(torch.as_tensor(scalar_r, dtype=torch.float64))
+            self._call("snapb_bc_apply", ctypes.byref(c), _lib.ptr(self.scalar_r), c.nscalar,
+                       SCALAR, st)
+        self._call("snapb_prim2cons", ctypes.byref(c), _lib.ptr(self.hydro_w),
+                   _lib.ptr(self.hydro_u), st)
+        if c.nscalar:
+            self.scalar_s.copy_(self.hydro_w[0:1] * self.scalar_r)
+        self._call("snapb_bc_apply", ctypes.byref(c), _lib.ptr(self.hydro_u), c.nvar, CONSERVED,
+                   st)
+        if c.nscalar:
+            self._call("snapb_bc_apply", ctypes.byref(c), _lib.ptr(self.scalar_s), c.nscalar,
+                       SCALAR, st)
+        return 0.0
+
+    # ---- MeshBlockImpl::max_time_step (device resident) ----
+    def max_time_step(self):
+        """dt = cfl * 2^-redo * CFL limit of hydro_w, left on the device."""
+        c = self.cfg
+        st = self._stream()
+        ws, nb = self._ws()
+        self._call("snapb_max_time_step", ctypes.byref(c), _lib.ptr(self.hydro_w),
+                   _lib.ptr(self.dt_raw), ws, nb, st)
+        self._call("snapb_scale_dt", _lib.ptr(self.dt_raw), ctypes.c_double(
+            self.options.integration.cfl), self.current_redo, _lib.ptr(self.dt), st)
+        return self.dt
+
+    def set_dt(self, dt: float):
+        self.dt.fill_(float(dt))
+        return self.dt
+
+    # ---- MeshBlockImpl::forward / advance_local ----
+    def forward(self, stage: int, dt=None):
+        if dt is not None and dt is not self.dt:
+            self.set_dt(dt)
+        c = self.cfg
+        ws, nb = self._ws()
+        self._call("snapb_stage", ctypes.byref(c), int(stage), _lib.ptr(self.dt),
+                   _lib.ptr(self.hydro_u), _lib.ptr(self.hydro_u0), _lib.ptr(self.hydro_w),
+                   _lib.ptr(self.scalar_s), _lib.ptr(self.scalar_s0), _lib.ptr(self.scalar_r),
+                   ws, nb, self._stream())
+
+    def step(self, dt=None):
+        """One RK3 step (three stages); dt defaults to the device CFL value."""
+        if dt is None:
+            self.max_time_step()
+        else:
+            self.set_dt(dt)
+        for s in range(3):
+            self.forward(s)
+        self.cycle += 1
+
+    # ---- MeshBlockImpl::check_redo ----
+    def check_redo(self) -> int:
+        c = self.cfg
+        self._call("snapb_check_positive", ctypes.byref(c), _lib.ptr(self.hydro_u),
+                   _lib.ptr(self.flags), self._stream())
+        f = self.flags.cpu().tolist()
+        if f[0] or (f[1] and f[2]):
+            self.current_redo += 1
+            if self.current_redo > self.options.integration.max_redo:
+                return -1
+            self.hydro_u.copy_(self.hydro_u0)
+            if c.nscalar:
+                self.scalar_s.copy_(self.scalar_s0)
+            st = self._stream()
+            self._call("snapb_bc_apply", ctypes.byref(c), _lib.ptr(self.hydro_u), c.nvar,
+                       CONSERVED, st)
+            if c.nscalar:
+                self._call("snapb_bc_apply", ctypes.byref(c), _lib.ptr(self.scalar_s),
+                           c.nscalar, SCALAR, st)
+            return 1
+        self.current_redo = 0
+        return 0
+
+    # ---- diagnostics ----
+    def interior(self, t):
+        return t[(slice(None),) + self.cfg.interior()]
+
+    def totals(self):
+        """Domain totals of the conserved variables (mass0, ..., energy)."""
+        return self.interior(self.hydro_u).sum(dim=(1, 2, 3))
