@@ -164,6 +164,25 @@ int snapb_implicit_correction(const snapb_hydro_config* cfg, const double* dt,
                               void* workspace, size_t workspace_bytes,
                               void* stream);
 
+/* The same correction as snapb_implicit_correction, for callers that cannot
+ * allocate device memory when they run it (inside a CUDA-graph capture, on a
+ * host whose device memory is pre-partitioned, or from a language binding
+ * without an allocator).  No reference counterpart: snapy always allocates
+ * its implicit-solve buffers.  It allocates nothing and takes no workspace:
+ * the column-solve scratch is a fixed 32 MiB array in the library's device
+ * memory, present on every GPU that loads the library until the process
+ * exits, so problems needing more (nx1 * columns * (N*N+N) * 8 bytes, N = 3
+ * or 5) are rejected with SNAPB_ERR_ARG.  The first call on a device looks up
+ * that array's address (once per device), so make it before any stream
+ * capture.  All calls share the one array: calls whose kernels overlap on the
+ * GPU (different streams, or different host threads) race on it; serialize
+ * them.  The solve writes every scratch entry before reading it, so nothing
+ * is carried over from the previous call. */
+int snapb_implicit_correction_noalloc(const snapb_hydro_config* cfg,
+                                      const double* dt, double* du,
+                                      const double* w, double* mass_corr,
+                                      void* stream);
+
 /* One RK stage of a mesh block, in place: du = forward(u), optional scalar
  * transport, u = wght0*u0 + wght1*u + wght2*du, boundary fills.  At stage 0
  * u0 (and s0) are filled from u (and s).  s, s0, r may be NULL when

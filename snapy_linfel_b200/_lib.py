@@ -48,6 +48,7 @@ def lib():
         "snapb_hydro_forward": (i, [cp, vp, vp, vp, vp, vp, vp, sz, vp]),
         "snapb_stage": (i, [cp, i, vp, vp, vp, vp, vp, vp, vp, vp, sz, vp]),
         "snapb_implicit_correction": (i, [cp, vp, vp, vp, vp, vp, sz, vp]),
+        "snapb_implicit_correction_noalloc": (i, [cp, vp, vp, vp, vp, vp]),
         "snapb_bc_apply": (i, [cp, vp, i, i, vp]),
         "snapb_max_time_step": (i, [cp, vp, vp, vp, sz, vp]),
         "snapb_scale_dt": (i, [vp, d, i, vp, vp]),
@@ -67,7 +68,7 @@ def exported_symbols():
     """Names of the entry points this binding declares (all in snapb.h)."""
     return ["snapb_abi_version", "snapb_last_error", "snapb_workspace_size", "snapb_cons2prim",
             "snapb_prim2cons", "snapb_reconstruct", "snapb_riemann", "snapb_hydro_forward",
-            "snapb_implicit_correction", "snapb_stage", "snapb_bc_apply", "snapb_max_time_step", "snapb_scale_dt",
+            "snapb_implicit_correction", "snapb_implicit_correction_noalloc", "snapb_stage", "snapb_bc_apply", "snapb_max_time_step", "snapb_scale_dt",
             "snapb_check_positive", "snapb_timing_enable", "snapb_timing_query"]
 
 

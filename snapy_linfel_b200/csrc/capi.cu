@@ -221,6 +221,11 @@ int run_stage(const snapb_hydro_config* c, int stage, const double* dt, double* 
 
 }  // namespace
 
+namespace snapb {
+const char* internal_check_config(const snapb_hydro_config* c) { return check_config(c); }
+int internal_fail(int code, const std::string& msg) { return fail(code, msg); }
+}  // namespace snapb
+
 extern "C" {
 
 int snapb_abi_version(void) { return SNAPB_ABI_VERSION; }

@@ -67,6 +67,11 @@ cudaError_t launch_riemann(const Geo& g, const Phys& p, int solver, int dim, con
                            const double* wr, int nv, double* flx, double* fp, const double* vel,
                            cudaStream_t st);
 
+// argument validation and last-error reporting shared with entry points that
+// live outside capi.cu
+const char* internal_check_config(const snapb_hydro_config* c);
+int internal_fail(int code, const std::string& msg);
+
 // bytes of dynamic shared memory the x1 column kernel needs per column
 size_t x1_smem_per_column(const Geo& g, int nvt);
 int x1_columns_per_cta(const Geo& g, int nvt);

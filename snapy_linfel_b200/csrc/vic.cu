@@ -16,6 +16,10 @@
 // (src/math/ludcmp.h:24-76, src/math/lubksb.h:124-147),
 // vic_backward_reduce / vic_redistribute_cell (src/implicit/vic_redistribute_impl.h:26-106),
 // flux Jacobian and Roe eigenvectors (src/implicit/flux_decomposition_impl.h:133-245).
+#include <cstring>
+#include <mutex>
+#include <string>
+
 #include "kernels.cuh"
 
 namespace snapb {
@@ -457,3 +461,87 @@ cudaError_t launch_vic(const Geo& g, const Phys& p, const StageBufs& b, cudaStre
 }
 
 }  // namespace snapb
+
+// ---------------------------------------------------------------------------
+// Implicit correction without any allocation.
+//
+// Some callers cannot allocate device memory when they need this solve: code
+// running inside a CUDA-graph capture or a stream-ordered region where
+// cudaMalloc would break the capture, embedded hosts whose memory is fully
+// pre-partitioned, and foreign-language callers that hold no allocator handle
+// (no torch, no CUDA context helper).  For them the solve's scratch lives in
+// a fixed array in the library's own device global memory instead of the
+// caller's workspace.  Every GPU that loads the library holds this array
+// (kNoAllocScratchBytes) until the process exits.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB
+static __device__ __align__(256) double
+    g_noalloc_vic_scratch[kNoAllocScratchBytes / sizeof(double)];
+
+// Device address of g_noalloc_vic_scratch on the current device.  In host code
+// the array's name only stands in for the symbol, so the address is looked up
+// with cudaGetSymbolAddress once per device (with that device current) and
+// cached.
+cudaError_t noalloc_scratch(double** out) {
+  static std::mutex mu;
+  static double* addr[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_vic_scratch);
+    if (e != cudaSuccess) return e;
+    addr[dev] = static_cast<double*>(p);
+  }
+  *out = addr[dev];
+  return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" int snapb_implicit_correction_noalloc(const snapb_hydro_config* cfg, const double* dt,
+                                                 double* du, const double* w, double* mass_corr,
+                                                 void* stream) {
+  using namespace snapb;
+  if (const char* e = internal_check_config(cfg))
+    return internal_fail(SNAPB_ERR_ARG, std::string("implicit_correction_noalloc: ") + e);
+  if (cfg->implicit_scheme == 0) return SNAPB_OK;  // null operation
+  if (!dt || !du || !w)
+    return internal_fail(SNAPB_ERR_ARG, "implicit_correction_noalloc: null pointer");
+  Geo g = make_geo(*cfg);
+  Phys p = make_phys(*cfg);
+  p.nscalar = 0;
+  size_t need = vic_scratch_bytes(g, p);
+  if (need > kNoAllocScratchBytes)
+    return internal_fail(SNAPB_ERR_ARG,
+                         "implicit_correction_noalloc: the column solve needs " +
+                             std::to_string(need) + " bytes of scratch (nx1 * columns * (N*N+N) * 8)"
+                             " but the built-in buffer holds " +
+                             std::to_string(kNoAllocScratchBytes) +
+                             " bytes; use snapb_implicit_correction with a workspace");
+  double* scratch = nullptr;
+  cudaError_t e = noalloc_scratch(&scratch);
+  if (e != cudaSuccess)
+    return internal_fail(SNAPB_ERR_CUDA, std::string("implicit_correction_noalloc: symbol address: ") +
+                                             cudaGetErrorString(e));
+  // The solve writes every scratch entry before it reads it, so nothing has
+  // to be cleared between calls.
+  StageBufs b;
+  std::memset(&b, 0, sizeof(b));
+  b.dt = dt;
+  b.w = const_cast<double*>(w);
+  b.D = du;
+  b.M = mass_corr;
+  b.vic = scratch;
+  b.vic_du_only = 1;
+  e = launch_vic(g, p, b, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess)
+    return internal_fail(SNAPB_ERR_CUDA, std::string("implicit_correction_noalloc: ") +
+                                             cudaGetErrorString(e));
+  return SNAPB_OK;
+}
