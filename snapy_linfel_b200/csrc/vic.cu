@@ -1,13 +1,19 @@
 // vic.cu — vertically implicit correction (VIC) of one RK stage, FP64.
 //
-// One thread owns one x1 column (the vertical, contiguous axis).  It assembles
-// the block-tridiagonal rows on the fly while it runs the block-Thomas forward
-// elimination, so every Roe eigen-decomposition |A| = R |Lambda| R^-1 is
-// computed once per interface instead of twice; the reduced blocks
-// a'_i = (a_i - b_i a'_{i-1})^-1 c_i and the partial solutions delta_i go to a
-// workspace laid out [layer][entry][column] so that the 32 columns of a warp
-// hit consecutive addresses.  Back substitution, the per-column MS-VIC sums,
-// the mass redistribution and the RK combination follow in the same thread.
+// Three kernels per solve:
+//   k_vic_assemble  every (column, interface) in parallel: the Roe-averaged
+//                   |A| = R |Lambda| R^-1 once per interface (the reference
+//                   forms it twice, once per neighbouring cell) and the flux
+//                   Jacobian once per cell, staged through shared memory;
+//   k_vic_sweep     one thread per x1 column (x1 is the vertical axis): the
+//                   block-Thomas elimination with nothing but small block
+//                   algebra in its sequential chain, back substitution and
+//                   the MS-VIC column sums;
+//   k_vic_finish    per cell: mass redistribution, scalar mass fix and the RK
+//                   combination (or du), with delta transposed through shared
+//                   memory.
+// Every workspace array is laid out with the column index fastest, so the
+// sequential sweep's loads and stores are coalesced across a warp's columns.
 //
 // Reference: ImplicitHydroImpl::forward (src/implicit/implicit_hydro.cpp:99-189),
 // vic_assemble_partial_impl (src/implicit/vic_assemble_partial_impl.h:29-111),
@@ -223,59 +229,151 @@ __device__ __forceinline__ void block_solve(double (&M)[N][N], double (&C)[N][N]
   }
 }
 
+// ---------------------------------------------------------------------------
+// Scratch layout (doubles, column index fastest so that the threads of a warp,
+// one column each, read consecutive addresses):
+//   T [nl+2][E1][ncol]   per index t: |A| at the face between cells t-1 and t
+//                        (N*N), the flux Jacobian of cell t-1 (N*N), the
+//                        explicit du rows of cell t (N) and rho of cell t (1)
+//   S [nl][N*N+N][ncol]  the reduced blocks a'_i then the partial solutions
+//                        delta_i (back-substituted in place)
+//   Z [2][ncol]          per-column sums: sum (rho V)^2 and B_dry
+// ---------------------------------------------------------------------------
+template <int N>
+struct VicDims {
+  static constexpr int E1 = 2 * N * N + N + 1;
+  static constexpr int ES = N * N + N;
+};
+
+static inline int vic_n(const Phys& p) { return ((p.implicit_scheme >> 3) & 1) ? 5 : 3; }
+
 size_t vic_scratch_bytes(const Geo& g, const Phys& p) {
   if (p.implicit_scheme == 0) return 0;
-  int N = ((p.implicit_scheme >> 3) & 1) ? 5 : 3;
+  int N = vic_n(p);
   int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
-  return (size_t)g.nx1 * (N * N + N) * ncol * sizeof(double);
+  int64_t nl = g.nx1;
+  int64_t e1 = 2 * N * N + N + 1, es = N * N + N;
+  return (size_t)((nl + 2) * e1 * ncol + nl * es * ncol + 2 * ncol) * sizeof(double);
 }
 
-template <int N, int NS>
-__global__ void __launch_bounds__(128) k_vic(Geo g, Phys p, StageBufs b) {
-  const int nj = g.ju - g.jl + 1, nk = g.ku - g.kl + 1;
-  const int64_t ncol = (int64_t)nj * nk;
-  const int64_t col = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= ncol) return;
-  const int j = g.jl + (int)(col % nj), k = g.kl + (int)(col / nj);
-  const int64_t c0 = (int64_t)k * g.s3 + (int64_t)j * g.s2 + g.il;  // cell (k, j, il)
-  const int64_t sv = g.sv;
-  const int nl = g.nx1;
-  constexpr int NE = N * N + N;
-  double* S = b.vic;
-  auto sc = [&](int i, int e) -> double& { return S[((int64_t)i * NE + e) * ncol + col]; };
+constexpr int kTC = 32;  // columns per tile
+constexpr int kTL = 32;  // layers per tile (redistribution)
+constexpr int kTLA = 16;  // layers per tile (assembly; static shared memory <= 48 KB)
 
-  const double dt = *b.dt;
+// (k, j, il) offset of interior column `col`
+__device__ __forceinline__ int64_t column_base(const Geo& g, int64_t col) {
+  const int nj = g.ju - g.jl + 1;
+  const int j = g.jl + (int)(col % nj), k = g.kl + (int)(col / nj);
+  return (int64_t)k * g.s3 + (int64_t)j * g.s2 + g.il;
+}
+
+// (1) assembly: every (column, t) in parallel.  The tile's cells are staged
+// through shared memory with loads along x1 (coalesced), the entries are
+// written with the column index fastest (coalesced).
+template <int N>
+__global__ void __launch_bounds__(256) k_vic_assemble(Geo g, Phys p, StageBufs b) {
+  constexpr int E1 = VicDims<N>::E1;
+  const int nl = g.nx1;
+  const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
+  const int64_t col0 = (int64_t)blockIdx.x * kTC;
+  const int t0 = blockIdx.y * kTLA;
+  const int64_t sv = g.sv;
+  __shared__ double ws[5][kTC][kTLA + 2];   // cells t0-1 .. t0+kTLA-1
+  __shared__ double ds[N][kTC][kTLA + 1];   // du rows of cells t0 .. t0+kTLA-1
+  const int tid = threadIdx.x;
+  for (int idx = tid; idx < 5 * kTC * (kTLA + 1); idx += blockDim.x) {
+    int s = idx % (kTLA + 1), rest = idx / (kTLA + 1);
+    int c = rest % kTC, v = rest / kTC;
+    int cell = t0 - 1 + s;  // relative to il; valid range [-1, nl]
+    int64_t col = col0 + c;
+    double x = 0.;
+    if (col < ncol && cell >= -1 && cell <= nl) x = b.w[v * sv + column_base(g, col) + cell];
+    ws[v][c][s] = x;
+  }
+  for (int idx = tid; idx < N * kTC * kTLA; idx += blockDim.x) {
+    int s = idx % kTLA, rest = idx / kTLA;
+    int c = rest % kTC, r = rest / kTC;
+    int cell = t0 + s;
+    int64_t col = col0 + c;
+    double x = 0.;
+    if (col < ncol && cell < nl) x = b.D[sel<N>(r) * sv + column_base(g, col) + cell];
+    ds[r][c][s] = x;
+  }
+  __syncthreads();
   const double gm1c = p.gammad - 1.;
   const double gm1f = 0.5 * (p.gammad + p.gammad) - 1.;
-  const double Aa = g.A1;  // uniform face area: (A_{i+1} - A_i) J_i vanishes
-  const double hiv = 0.5 / g.vol;
-  const double idt = 1. / dt;
-  const double grav = p.grav1;
-  double bnd[N];
+  double* T = b.vic;
+  for (int idx = tid; idx < kTC * kTLA; idx += blockDim.x) {
+    int c = idx % kTC, s = idx / kTC;
+    int t = t0 + s;
+    int64_t col = col0 + c;
+    if (col >= ncol || t > nl + 1) continue;
+    double wl[5], wr[5];
 #pragma unroll
-  for (int r = 0; r < N; ++r) bnd[r] = r == 1 ? -1. : 1.;
-
-  auto prim = [&](int i, double* o) {
+    for (int v = 0; v < 5; ++v) {
+      wl[v] = ws[v][c][s];      // cell t-1
+      wr[v] = ws[v][c][s + 1];  // cell t
+    }
+    double* out = T + (int64_t)t * E1 * ncol + col;
+    double A[N][N], J[N][N];
+    if (t <= nl) {
+      absA_block<N>(gm1f, wl, wr, A);
+    } else {
 #pragma unroll
-    for (int v = 0; v < 5; ++v) o[v] = b.w[v * sv + c0 + i];
-  };
+      for (int r = 0; r < N; ++r)
+#pragma unroll
+        for (int q = 0; q < N; ++q) A[r][q] = 0.;
+    }
+    jac_block<N>(gm1c, wl, J);
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        out[(r * N + q) * ncol] = A[r][q];
+        out[(N * N + r * N + q) * ncol] = J[r][q];
+      }
+#pragma unroll
+    for (int r = 0; r < N; ++r) out[(2 * N * N + r) * ncol] = t < nl ? ds[r][c][s] : 0.;
+    out[(2 * N * N + N) * ncol] = t < nl ? wr[IDN] : 0.;
+  }
+}
 
-  double wm[5], wc[5], wp[5];
-  prim(-1, wm);
-  prim(0, wc);
-  double Jp[N][N], Am[N][N];
-  jac_block<N>(gm1c, wm, Jp);
-  absA_block<N>(gm1f, wm, wc, Am);
-  double Jc[N][N];
-  jac_block<N>(gm1c, wc, Jc);
-  double ap[N][N], dp[N];
+// (2) block-Thomas sweep, one thread per column, every access coalesced.
+template <int N>
+__global__ void __launch_bounds__(128) k_vic_sweep(Geo g, Phys p, StageBufs b) {
+  constexpr int E1 = VicDims<N>::E1, ES = VicDims<N>::ES;
+  const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
+  const int64_t col = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= ncol) return;
+  const int nl = g.nx1;
+  const double* T = b.vic + col;
+  double* S = b.vic + (int64_t)(nl + 2) * E1 * ncol + col;
+  double* Z = S + (int64_t)nl * ES * ncol;
+  auto Tat = [&](int t, int e) { return T[((int64_t)t * E1 + e) * ncol]; };
+  auto Sat = [&](int i, int e) -> double& { return S[((int64_t)i * ES + e) * ncol]; };
 
-  // ---- assembly + forward elimination ----
+  const double dt = *b.dt;
+  const double Aa = g.A1, hiv = 0.5 / g.vol, idt = 1. / dt, grav = p.grav1;
+  double Am[N][N], Jp[N][N], Jc[N][N], ap[N][N], dp[N];
+#pragma unroll
+  for (int r = 0; r < N; ++r)
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+      Am[r][q] = Tat(0, r * N + q);
+      Jp[r][q] = Tat(0, N * N + r * N + q);  // cell -1
+      Jc[r][q] = Tat(1, N * N + r * N + q);  // cell 0
+    }
   for (int i = 0; i < nl; ++i) {
-    prim(i + 1, wp);
-    double Jn[N][N], Ap[N][N];
-    jac_block<N>(gm1c, wp, Jn);
-    absA_block<N>(gm1f, wc, wp, Ap);
+    double Ap[N][N], Jn[N][N], rhs[N];
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      rhs[r] = Tat(i, 2 * N * N + r) / dt;
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        Ap[r][q] = Tat(i + 1, r * N + q);
+        Jn[r][q] = Tat(i + 2, N * N + r * N + q);  // cell i+1
+      }
+    }
     double a[N][N], bb[N][N], c[N][N];
 #pragma unroll
     for (int r = 0; r < N; ++r)
@@ -283,7 +381,7 @@ __global__ void __launch_bounds__(128) k_vic(Geo g, Phys p, StageBufs b) {
       for (int q = 0; q < N; ++q) {
         double phi = 0.;
         if (r == 1 && q == 0) phi = grav;
-        if (r == 2 && q == 1 && N == 3) phi = grav;
+        if (N == 3 && r == 2 && q == 1) phi = grav;
         if (N == 5 && r == IPR && q == IVX) phi = grav;
         a[r][q] = (Am[r][q] * Aa + Ap[r][q] * Aa) * hiv - phi;
         bb[r][q] = -(Am[r][q] + Jp[r][q]) * Aa * hiv;
@@ -295,17 +393,14 @@ __global__ void __launch_bounds__(128) k_vic(Geo g, Phys p, StageBufs b) {
 #pragma unroll
       for (int r = 0; r < N; ++r)
 #pragma unroll
-        for (int q = 0; q < N; ++q) a[r][q] += bb[r][q] * bnd[q];
+        for (int q = 0; q < N; ++q) a[r][q] += bb[r][q] * (q == 1 ? -1. : 1.);
     }
     if (i == nl - 1) {
 #pragma unroll
       for (int r = 0; r < N; ++r)
 #pragma unroll
-        for (int q = 0; q < N; ++q) a[r][q] += c[r][q] * bnd[q];
+        for (int q = 0; q < N; ++q) a[r][q] += c[r][q] * (q == 1 ? -1. : 1.);
     }
-    double rhs[N];
-#pragma unroll
-    for (int r = 0; r < N; ++r) rhs[r] = b.D[sel<N>(r) * sv + c0 + i] / dt;
     if (i > 0) {
 #pragma unroll
       for (int r = 0; r < N; ++r) {
@@ -325,11 +420,11 @@ __global__ void __launch_bounds__(128) k_vic(Geo g, Phys p, StageBufs b) {
 #pragma unroll
     for (int r = 0; r < N; ++r) {
       dp[r] = rhs[r];
-      sc(i, N * N + r) = rhs[r];
+      Sat(i, N * N + r) = rhs[r];
 #pragma unroll
       for (int q = 0; q < N; ++q) {
         ap[r][q] = c[r][q];
-        sc(i, r * N + q) = c[r][q];
+        Sat(i, r * N + q) = c[r][q];
       }
     }
 #pragma unroll
@@ -340,64 +435,85 @@ __global__ void __launch_bounds__(128) k_vic(Geo g, Phys p, StageBufs b) {
         Jp[r][q] = Jc[r][q];
         Jc[r][q] = Jn[r][q];
       }
-#pragma unroll
-    for (int v = 0; v < 5; ++v) {
-      wm[v] = wc[v];
-      wc[v] = wp[v];
-    }
   }
-
-  // ---- back substitution + column sums ----
-  double sum_a2 = 0., b_dry = 0.;
+  // back substitution: delta_i -= a'_i delta_{i+1}
   double dn[N];
 #pragma unroll
   for (int r = 0; r < N; ++r) dn[r] = dp[r];
-  {
-    double rho = b.w[IDN * sv + c0 + nl - 1];
-    double ai = rho * g.vol;
-    sum_a2 += ai * ai;
-    b_dry += (b.D[IDN * sv + c0 + nl - 1] - dn[0]) * 1. * g.vol;
-  }
   for (int i = nl - 2; i >= 0; --i) {
     double d[N];
 #pragma unroll
     for (int r = 0; r < N; ++r) {
       double t = 0.;
 #pragma unroll
-      for (int q = 0; q < N; ++q) t += sc(i, r * N + q) * dn[q];
-      d[r] = sc(i, N * N + r) - t;
+      for (int q = 0; q < N; ++q) t += Sat(i, r * N + q) * dn[q];
+      d[r] = Sat(i, N * N + r) - t;
     }
 #pragma unroll
     for (int r = 0; r < N; ++r) {
       dn[r] = d[r];
-      sc(i, N * N + r) = d[r];
+      Sat(i, N * N + r) = d[r];
     }
-    double rho = b.w[IDN * sv + c0 + i];
-    double ai = rho * g.vol;
-    sum_a2 += ai * ai;
-    b_dry += (b.D[IDN * sv + c0 + i] - d[0]) * 1. * g.vol;
   }
-
-  // ---- redistribution + scalar mass fix + RK combination ----
+  // column sums in ascending layer order (vic_backward_reduce)
+  double sum_a2 = 0., b_dry = 0.;
   for (int i = 0; i < nl; ++i) {
-    const int64_t off = c0 + i;
-    double d[N];
-#pragma unroll
-    for (int r = 0; r < N; ++r) d[r] = sc(i, N * N + r);
+    double ai = Tat(i, 2 * N * N + N) * g.vol;
+    sum_a2 += ai * ai;
+    b_dry += (Tat(i, 2 * N * N) - Sat(i, N * N)) * 1. * g.vol;
+  }
+  Z[0] = sum_a2;
+  Z[ncol] = b_dry;
+}
+
+// (3) redistribution + RK combination (or du), tiles of 32 columns x 32
+// layers: delta is transposed through shared memory so that the state
+// arrays are read and written along x1.
+template <int N, int NS>
+__global__ void __launch_bounds__(256) k_vic_finish(Geo g, Phys p, StageBufs b) {
+  constexpr int E1 = VicDims<N>::E1, ES = VicDims<N>::ES;
+  const int nl = g.nx1;
+  const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
+  const int64_t col0 = (int64_t)blockIdx.x * kTC;
+  const int i0 = blockIdx.y * kTL;
+  const int64_t sv = g.sv;
+  const double* S = b.vic + (int64_t)(nl + 2) * E1 * ncol;
+  const double* Z = S + (int64_t)nl * ES * ncol;
+  __shared__ double dl[N][kTC][kTL + 1];
+  __shared__ double zs[2][kTC];
+  const int tid = threadIdx.x;
+  for (int idx = tid; idx < N * kTC * kTL; idx += blockDim.x) {
+    int c = idx % kTC, rest = idx / kTC;
+    int s = rest % kTL, r = rest / kTL;
+    int64_t col = col0 + c;
+    int i = i0 + s;
+    dl[r][c][s] = (col < ncol && i < nl) ? S[((int64_t)i * ES + N * N + r) * ncol + col] : 0.;
+  }
+  if (tid < 2 * kTC) {
+    int c = tid % kTC, k = tid / kTC;
+    zs[k][c] = col0 + c < ncol ? Z[k * ncol + col0 + c] : 1.;
+  }
+  __syncthreads();
+  for (int idx = tid; idx < kTC * kTL; idx += blockDim.x) {
+    int s = idx % kTL, c = idx / kTL;
+    int64_t col = col0 + c;
+    int i = i0 + s;
+    if (col >= ncol || i >= nl) continue;
+    const int64_t off = column_base(g, col) + i;
     double rho = b.w[IDN * sv + off];
     double ai = rho * g.vol;
     double et = b.D[IDN * sv + off];
-    double fix = d[0] - et;
+    double fix = dl[0][c][s] - et;
     double du[5];
-    du[IDN] = et + fix * 1. + rho * ai * b_dry / sum_a2;
+    du[IDN] = et + fix * 1. + rho * ai * zs[1][c] / zs[0][c];
     if constexpr (N == 3) {
-      du[IVX] = d[1];
+      du[IVX] = dl[1][c][s];
       du[IVY] = b.D[IVY * sv + off];
       du[IVZ] = b.D[IVZ * sv + off];
-      du[IPR] = d[2];
+      du[IPR] = dl[2][c][s];
     } else {
 #pragma unroll
-      for (int v = 1; v < 5; ++v) du[v] = d[v];
+      for (int v = 1; v < 5; ++v) du[v] = dl[v][c][s];
     }
     if (b.M) b.M[IDN * sv + off] = fix;
     if (b.vic_du_only) {
@@ -443,20 +559,26 @@ __global__ void __launch_bounds__(128) k_vic(Geo g, Phys p, StageBufs b) {
 template <int N>
 static cudaError_t launch_vic_n(const Geo& g, const Phys& p, const StageBufs& b,
                                 cudaStream_t st) {
-  int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
-  unsigned grid = (unsigned)((ncol + 127) / 128);
+  const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
+  const int nl = g.nx1;
+  dim3 ga((unsigned)((ncol + kTC - 1) / kTC), (unsigned)((nl + 2 + kTLA - 1) / kTLA));
+  k_vic_assemble<N><<<ga, 256, 0, st>>>(g, p, b);
+  // small column counts: narrower CTAs spread the sequential sweeps over more SMs
+  int bs = ncol >= 148 * 128 ? 128 : (ncol >= 148 * 64 ? 64 : 32);
+  k_vic_sweep<N><<<(unsigned)((ncol + bs - 1) / bs), bs, 0, st>>>(g, p, b);
+  dim3 gf((unsigned)((ncol + kTC - 1) / kTC), (unsigned)((nl + kTL - 1) / kTL));
   switch (p.nscalar) {
-    case 0: k_vic<N, 0><<<grid, 128, 0, st>>>(g, p, b); break;
-    case 1: k_vic<N, 1><<<grid, 128, 0, st>>>(g, p, b); break;
-    case 2: k_vic<N, 2><<<grid, 128, 0, st>>>(g, p, b); break;
-    case 3: k_vic<N, 3><<<grid, 128, 0, st>>>(g, p, b); break;
+    case 0: k_vic_finish<N, 0><<<gf, 256, 0, st>>>(g, p, b); break;
+    case 1: k_vic_finish<N, 1><<<gf, 256, 0, st>>>(g, p, b); break;
+    case 2: k_vic_finish<N, 2><<<gf, 256, 0, st>>>(g, p, b); break;
+    case 3: k_vic_finish<N, 3><<<gf, 256, 0, st>>>(g, p, b); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
 }
 
 cudaError_t launch_vic(const Geo& g, const Phys& p, const StageBufs& b, cudaStream_t st) {
-  if ((p.implicit_scheme >> 3) & 1) return launch_vic_n<5>(g, p, b, st);
+  if (vic_n(p) == 5) return launch_vic_n<5>(g, p, b, st);
   return launch_vic_n<3>(g, p, b, st);
 }
 
