@@ -204,6 +204,94 @@ def run_reference(args):
 # --------------------------------------------------------------------------
 # GPU arm
 # --------------------------------------------------------------------------
+_STATE_CACHE = {}
+
+
+def workload_state(name):
+    """The initial (w, r) of a workload, kept so both forms start alike."""
+    return _STATE_CACHE.get(name)
+
+
+def rel_errors(a, b, it):
+    """per-field rel L1 and L-inf over the interior"""
+    out = {"rel_l1": [], "linf": []}
+    for v in range(a.shape[0]):
+        x, y = a[v][it], b[v][it]
+        out["rel_l1"].append(float((x - y).abs().sum() / y.abs().sum().clamp_min(1e-300)))
+        out["linf"].append(float((x - y).abs().max() / y.abs().max().clamp_min(1e-300)))
+    return out
+
+
+def run_fp32_form(args, opts, state, mb64, cells, stream, barrier, world):
+    import torch
+
+    from snapy_linfel_b200 import _lib
+    from snapy_linfel_b200.mesh import MeshBlock, MeshBlockF32
+
+    w, r = state
+    m32 = MeshBlockF32(opts, device=mb64.device)
+    m32.initialize(w, r)
+    for _ in range(args.warmup):
+        m32.step()
+    barrier()
+    _lib.timing_enable(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        m32.step()
+    e1.record(stream)
+    barrier()
+    ms = e0.elapsed_time(e1)
+    kern = {k: round(v[0] / v[1], 4) for k, v in _lib.timing_query().items()}
+    _lib.timing_enable(False)
+    # e2e with host buffers (the FP32 perturbation state is the API's state)
+    hu = torch.empty(opts.hydro.shape, dtype=torch.float32).pin_memory()
+    hu.copy_(m32.hydro_u.cpu())
+    hs = None
+    if opts.hydro.nscalar:
+        hs = torch.empty(opts.hydro.scalar_shape, dtype=torch.float32).pin_memory()
+        hs.copy_(m32.scalar_s.cpu())
+    nbytes = hu.numel() * 4 + (hs.numel() * 4 if hs is not None else 0)
+    barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        m32.hydro_u.copy_(hu, non_blocking=True)
+        if hs is not None:
+            m32.scalar_s.copy_(hs, non_blocking=True)
+        m32.step()
+        hu.copy_(m32.hydro_u, non_blocking=True)
+        if hs is not None:
+            hs.copy_(m32.scalar_s, non_blocking=True)
+    e1.record(stream)
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+    e2e = world * cells * 3 * args.steps / (e2e_ms / 1e3) / 1e6
+    # accuracy: both forms from the same initial state, same dt sequence
+    a64 = MeshBlock(opts, device=mb64.device)
+    a64.initialize(w, r)
+    a32 = MeshBlockF32(opts, device=mb64.device)
+    a32.initialize(w, r)
+    for _ in range(args.acc_steps):
+        dt = a64.max_time_step().clone()
+        a64.step(dt)
+        a32.step(dt)
+    torch.cuda.synchronize()
+    it = (slice(None),) + opts.hydro.interior()
+    acc = rel_errors(a32.state64(), a64.hydro_u, it)
+    acc["steps"] = args.acc_steps
+    if opts.hydro.nscalar:
+        sacc = rel_errors(a32.scalar_s.double(), a64.scalar_s, it)
+        acc["scalar_rel_l1"] = sacc["rel_l1"]
+    # perturbation fields: density about the reference, momenta
+    rb = a32.ref_rho.view(1, 1, -1)
+    rp32 = (a32.state64()[0] - rb)[it[1:]]
+    rp64 = (a64.hydro_u[0] - rb)[it[1:]]
+    acc["rho_prime_rel_l1"] = float((rp32 - rp64).abs().sum() / rp64.abs().sum())
+    del a64, a32
+    return {"ms": ms, "kern": kern, "acc": acc, "e2e": {"value": e2e, "unit": UNIT},
+            "h2d": nbytes, "d2h": nbytes}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -221,10 +309,10 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
 
     opts, w, r, desc = workload(args.workload)
+    _STATE_CACHE[args.workload] = (w, r)
     cfg = opts.hydro
     mb = MeshBlock(opts, device=f"cuda:{local}")
     mb.initialize(w, r)
-    del w
     cells = interior_cells(cfg)
     stream = torch.cuda.current_stream()
 
@@ -299,6 +387,17 @@ def run_ours(args):
     stage_bw = algo_bytes_per_cell_update(cfg) * cells / stage_s / 1e9
     kern_ms = {k: round(v[0] / v[1], 4) for k, v in kern.items()}
 
+    # ---- FP32 perturbation form: throughput and accuracy against FP64 ----
+    f32 = None
+    if not args.no_fp32:
+        f32 = run_fp32_form(args, opts, workload_state(args.workload), mb, cells, stream, barrier,
+                            world)
+        if world > 1:
+            t = torch.tensor([f32["ms"]], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            f32["ms"] = t.item()
+        f32["value"] = world * cells * 3 * args.steps / (f32["ms"] / 1e3) / 1e6
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         try:
@@ -312,22 +411,36 @@ def run_ours(args):
                    "sample": f"failed: {e}"}
 
     if rank == 0:
+        forms = {"fp64_plain": {"value": value, "ms_per_step": ms_max / args.steps}}
+        head_value, head_ms, head_dtype, head_form = value, ms_max / args.steps, "f64", "plain_fp64"
+        if f32 is not None:
+            forms["fp32_perturbation"] = {
+                "value": f32["value"], "ms_per_step": f32["ms"] / args.steps,
+                "kernel_ms_per_launch": f32["kern"],
+                "accuracy_vs_fp64": f32["acc"]}
+            forms["fp32_over_fp64_speedup"] = f32["value"] / value
+            head_value, head_ms = f32["value"], f32["ms"] / args.steps
+            head_dtype, head_form = "f32 (perturbation over f64 reference)", "fp32_perturbation"
+            e2e = f32["e2e"] if f32.get("e2e") else e2e
+            h2d = f32.get("h2d", h2d)
+            d2h = f32.get("d2h", d2h)
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "metric": METRIC, "value": head_value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": desc, "form": "plain_fp64",
+            "ms_per_step": head_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": head_dtype, "data": "synthetic",
+            "forms": forms,
+            "config": {"workload": desc, "form": head_form,
                        "cells_per_gpu": cells, "rk_stages_per_step": 3,
                        "l2_policy": "inputs larger than L2 (state > 126 MB)",
                        "parallelism": f"replicas x{world}"},
             "roofline": roof,
             "stage_roofline": {"achieved": stage_bw, "peak": peak, "unit": "GB/s",
                                "frac": stage_bw / peak},
-            "kernel_ms_per_launch": kern_ms,
+            "kernel_ms_per_launch_fp64": kern_ms,
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+            "e2e": {"value": e2e if not isinstance(e2e, dict) else e2e["value"], "unit": UNIT,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches_per_step(cfg) * args.steps,
             "clocks": clk.summary(),
         }
@@ -345,6 +458,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c5")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp32", action="store_true")
+    ap.add_argument("--acc-steps", type=int, default=5)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

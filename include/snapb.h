@@ -221,6 +221,42 @@ int snapb_scale_dt(const double* dt_in, double cfl, int redo, double* dt_out,
 int snapb_check_positive(const snapb_hydro_config* cfg, const double* u,
                          int* flags, void* stream);
 
+/* ---- FP32 perturbation form ----
+ * The state is stored in FP32 as perturbations about an FP64 reference
+ * profile rho_bar(x1), p_bar(x1) (x1 = vertical, [nc1] device arrays, ghosts
+ * included): u' = u - (rho_bar, 0, 0, 0, p_bar/(gamma-1)) and
+ * w' = (rho - rho_bar, v1, v2, v3, p - p_bar).  The sweeps run in FP32; the
+ * reference's own x1 pressure-gradient / gravity balance, the isentropic
+ * ghost revision and the implicit elimination run in FP64, and the momentum
+ * fluxes carry pressure relative to an FP64 face reference, so the
+ * hydrostatic pressure never enters an FP32 difference.  No reference
+ * counterpart: snapy computes in FP64 (or plain FP32) throughout.
+ * Requirements: active x1, non-hydrostatic = 1, no diffusion, and a linear x1
+ * pressure interpolation (cp5/cp3/dc — WENO5 with shock: false) whenever a
+ * reference pressure is given.  Call snapb_reference_f32 once per reference
+ * (it fills tables in the workspace) before the other calls. */
+size_t snapb_workspace_size_f32(const snapb_hydro_config* cfg);
+int snapb_reference_f32(const snapb_hydro_config* cfg, const double* ref_rho,
+                        const double* ref_p, void* workspace,
+                        size_t workspace_bytes, void* stream);
+/* kind = SNAPB_CONSERVED (u <-> u') or SNAPB_PRIMITIVE (w <-> w') */
+int snapb_to_perturbation(const snapb_hydro_config* cfg, int kind,
+                          const double* in, float* out, void* workspace,
+                          size_t workspace_bytes, void* stream);
+int snapb_from_perturbation(const snapb_hydro_config* cfg, int kind,
+                            const float* in, double* out, void* workspace,
+                            size_t workspace_bytes, void* stream);
+int snapb_stage_f32(const snapb_hydro_config* cfg, int stage, const double* dt,
+                    float* u, float* u0, float* w, float* s, float* s0,
+                    float* r, void* workspace, size_t workspace_bytes,
+                    void* stream);
+int snapb_bc_apply_f32(const snapb_hydro_config* cfg, float* var, int nv,
+                       int kind, void* workspace, size_t workspace_bytes,
+                       void* stream);
+int snapb_max_time_step_f32(const snapb_hydro_config* cfg, const float* w,
+                            double* dt_out, void* workspace,
+                            size_t workspace_bytes, void* stream);
+
 /* ---- diagnostics: per-kernel device time ----
  * While enabled, snapb_stage and snapb_hydro_forward record a CUDA event pair
  * around every kernel they launch.  snapb_timing_query synchronizes those

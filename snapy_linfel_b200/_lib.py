@@ -53,6 +53,13 @@ def lib():
         "snapb_max_time_step": (i, [cp, vp, vp, vp, sz, vp]),
         "snapb_scale_dt": (i, [vp, d, i, vp, vp]),
         "snapb_check_positive": (i, [cp, vp, vp, vp]),
+        "snapb_workspace_size_f32": (sz, [cp]),
+        "snapb_reference_f32": (i, [cp, vp, vp, vp, sz, vp]),
+        "snapb_to_perturbation": (i, [cp, i, vp, vp, vp, sz, vp]),
+        "snapb_from_perturbation": (i, [cp, i, vp, vp, vp, sz, vp]),
+        "snapb_stage_f32": (i, [cp, i, vp, vp, vp, vp, vp, vp, vp, vp, sz, vp]),
+        "snapb_bc_apply_f32": (i, [cp, vp, i, i, vp, sz, vp]),
+        "snapb_max_time_step_f32": (i, [cp, vp, vp, vp, sz, vp]),
         "snapb_timing_enable": (i, [i]),
         "snapb_timing_query": (i, [i, ctypes.POINTER(d), ctypes.POINTER(i)]),
     }
@@ -69,7 +76,10 @@ def exported_symbols():
     return ["snapb_abi_version", "snapb_last_error", "snapb_workspace_size", "snapb_cons2prim",
             "snapb_prim2cons", "snapb_reconstruct", "snapb_riemann", "snapb_hydro_forward",
             "snapb_implicit_correction", "snapb_implicit_correction_noalloc", "snapb_stage", "snapb_bc_apply", "snapb_max_time_step", "snapb_scale_dt",
-            "snapb_check_positive", "snapb_timing_enable", "snapb_timing_query"]
+            "snapb_check_positive", "snapb_timing_enable", "snapb_timing_query",
+            "snapb_workspace_size_f32", "snapb_reference_f32", "snapb_to_perturbation",
+            "snapb_from_perturbation", "snapb_stage_f32", "snapb_bc_apply_f32",
+            "snapb_max_time_step_f32"]
 
 
 KERNELS = {"x1_sweep": 0, "diffusion": 1, "x2_sweep": 2, "x3_sweep": 3, "finalize": 4,

@@ -212,6 +212,29 @@ cudaError_t launch_cfl(const Geo& g, const Phys& p, const double* w, double* slo
   return cudaGetLastError();
 }
 
+cudaError_t launch_cfl_final(const Geo& g, const Phys& p, unsigned long long* slots,
+                             double* dt_out, cudaStream_t st) {
+  int scheme = p.implicit_scheme;
+  int use1 = g.nc1 > 1, use2 = g.nc2 > 1, use3 = g.nc3 > 1;
+  if (scheme != 0) {
+    use1 = use1 && (!(scheme & 1) || (g.nc3 == 1 && g.nc2 == 1));
+    use2 = use2 && !((scheme >> 1) & 1);
+    use3 = use3 && !((scheme >> 2) & 1);
+  }
+  double dt_diff = -1.;
+  double coeff = fmax(p.nu, p.kappa);
+  if (coeff > 0.) {
+    int ndim = 0;
+    double dxm = DBL_MAX;
+    if (g.nc1 > 1) ++ndim, dxm = fmin(dxm, g.dx1);
+    if (g.nc2 > 1) ++ndim, dxm = fmin(dxm, g.dx2);
+    if (g.nc3 > 1) ++ndim, dxm = fmin(dxm, g.dx3);
+    if (ndim > 0) dt_diff = dxm * dxm / (2. * ndim * coeff);
+  }
+  k_cfl_final<<<1, 1, 0, st>>>(slots, use1, use2, use3, dt_diff, dt_out);
+  return cudaGetLastError();
+}
+
 __global__ void k_scale_dt(const double* in, double f, double* out) { *out = f * *in; }
 
 cudaError_t launch_scale_dt(const double* dt_in, double cfl, int redo, double* dt_out,

@@ -29,6 +29,36 @@ struct StageBufs {
   int vic_du_only;   // 1: the implicit solve leaves du in D (no RK update)
 };
 
+// Buffers of one RK stage of the FP32 perturbation form: the state is stored
+// as FP32 perturbations about the FP64 reference profile rho_bar(x1),
+// p_bar(x1): u' = u - (rho_bar, 0, 0, 0, p_bar/(gamma-1)),
+// w' = (rho - rho_bar, v1, v2, v3, p - p_bar).
+struct StageBufs32 {
+  const double* dt;
+  float* u;
+  float* u0;
+  float* w;
+  float* s;
+  float* s0;
+  float* r;
+  float* D;    // [nvar + nscalar][sv] flux-difference sums, then du
+  float* R;    // [nscalar][sv]
+  double* M;   // [sv] implicit mass correction
+  double* vic;
+  const double* rb;  // [nc1] reference density (cell centres)
+  const double* pb;  // [nc1] reference pressure
+  double* pf;        // [nc1+1] x1 face reference pressure
+  float* offL;       // [nc1+1] left-state reference offset from pf
+  float* offR;       // [nc1+1] right-state reference offset from pf
+  float* rbar;       // [nc1] FP64 residual of the reference x1 momentum balance
+  float* rbf;        // [nc1] float(rho_bar)
+  float* pbf;        // [nc1] float(p_bar)
+  int stage;
+  double wgt0, wgt1, wgt2;
+  int write_du;
+  int vic_du_only;
+};
+
 // RK3 (Shu-Osher) stage weights: u = wgt0*u0 + wgt1*u + wgt2*du
 inline void rk3_weights(int stage, double& a, double& b, double& c) {
   static const double W[3][3] = {{1., 0., 1.}, {3. / 4., 1. / 4., 1. / 4.},
@@ -47,6 +77,7 @@ cudaError_t launch_march(int axis, const Geo& g, const Phys& p, const StageBufs&
 cudaError_t launch_finalize(const Geo& g, const Phys& p, const StageBufs& b, cudaStream_t st);
 cudaError_t launch_diffusion(const Geo& g, const Phys& p, const StageBufs& b, cudaStream_t st);
 cudaError_t launch_vic(const Geo& g, const Phys& p, const StageBufs& b, cudaStream_t st);
+cudaError_t launch_vic32(const Geo& g, const Phys& p, const StageBufs32& b, cudaStream_t st);
 size_t vic_scratch_bytes(const Geo& g, const Phys& p);
 
 cudaError_t launch_cons2prim(const Geo& g, const Phys& p, const double* u, double* w,
@@ -57,6 +88,8 @@ cudaError_t launch_bc(const Geo& g, const snapb_hydro_config& c, double* var, in
                       cudaStream_t st);
 cudaError_t launch_cfl(const Geo& g, const Phys& p, const double* w, double* slots,
                        double* dt_out, cudaStream_t st);
+cudaError_t launch_cfl_final(const Geo& g, const Phys& p, unsigned long long* slots,
+                             double* dt_out, cudaStream_t st);
 cudaError_t launch_scale_dt(const double* dt_in, double cfl, int redo, double* dt_out,
                             cudaStream_t st);
 cudaError_t launch_check_positive(const Geo& g, const Phys& p, const double* u, int* flags,

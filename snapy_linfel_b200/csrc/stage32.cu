@@ -1,0 +1,671 @@
+// stage32.cu — one RK stage in the FP32 perturbation form.
+//
+// State: u' = u - (rho_bar, 0, 0, 0, p_bar/(gamma-1)) in FP32 over an FP64
+// reference profile rho_bar(x1), p_bar(x1) (x1 = vertical).  The sweeps are
+// the same fused kernels as the FP64 form (stage.cu) in FP32 arithmetic, with
+// three places where FP64 stays:
+//   * the reference tables (k_ref32): x1 face reference pressures pf, the
+//     offsets of each side's reconstructed reference pressure from pf, and
+//     the residual of the reference x1 momentum balance
+//     rbar_i = -(A1 pf_{i+1} - A1 pf_i)/V + rho_bar_i g1, formed in FP64 and
+//     stored after the cancellation;
+//   * the isentropic x1 ghost revision (pow of full values) in FP64;
+//   * the implicit column solve (vic.cu, FP64 elimination on full states).
+// The momentum fluxes carry the pressure as p' = p - pf (pert.cuh), so the
+// large hydrostatic pressure never enters an FP32 difference.
+#include <algorithm>
+
+#include "kernels.cuh"
+#include "pert.cuh"
+
+namespace snapb {
+
+// ---------------------------------------------------------------------------
+// reference tables
+// ---------------------------------------------------------------------------
+__global__ void k_ref32(Geo g, Phys p, const double* rb_in, const double* pb_in, double* rbw,
+                        double* pbw, StageBufs32 b) {
+  const int nc1 = g.nc1;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t <= nc1) {
+    // reference pressure at face t from each side, with the x1 pressure
+    // interpolation (linear: cp5 / cp3 / dc)
+    int typ = (p.r1_shock) ? p.r1_type : interp2_of(p.r1_type);
+    double q[6];
+    for (int m = 0; m < 6; ++m) {
+      int c = min(max(t - 3 + m, 0), nc1 - 1);
+      q[m] = pb_in ? pb_in[c] : 0.;
+    }
+    double pl, pr;
+    face_states<double>(typ, false, q, pl, pr);
+    if (typ != SNAPB_RECON_CP5 && typ != SNAPB_RECON_CP3 && typ != SNAPB_RECON_DC) {
+      pl = pr = q[2];  // non-linear pressure interpolation: only with a zero reference
+    }
+    double pfv = 0.5 * (pl + pr);
+    b.pf[t] = pfv;
+    b.offL[t] = (float)(pl - pfv);
+    b.offR[t] = (float)(pr - pfv);
+  }
+  if (t < nc1) {
+    double r = rb_in ? rb_in[t] : 0.;
+    double pr = pb_in ? pb_in[t] : 0.;
+    rbw[t] = r;
+    pbw[t] = pr;
+    b.rbf[t] = (float)r;
+    b.pbf[t] = (float)pr;
+  }
+}
+
+// second pass: the x1 momentum residual needs pf on both faces of a cell
+__global__ void k_ref32_residual(Geo g, Phys p, StageBufs32 b) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.nc1) return;
+  double res = 0.;
+  if (i + 1 <= g.nc1) res = -(g.A1 * b.pf[i + 1] - g.A1 * b.pf[i]) / g.vol;
+  res += b.rb[i] * p.grav1;
+  b.rbar[i] = (float)res;
+}
+
+// ---------------------------------------------------------------------------
+// finalize: du' = -dt div'/V + gravity (with the FP64 reference residual),
+// then RK on u' or du for the implicit solve
+// ---------------------------------------------------------------------------
+template <int NS>
+__device__ __forceinline__ void finalize32(const Geo& g, const Phys& p, const StageBufs32& b,
+                                           int64_t off, int xi, const float* d, const float* wc) {
+  const int64_t sv = g.sv;
+  const float dt = (float)*b.dt;
+  const float ivol = (float)(1.0 / g.vol);
+  float rho = b.rbf[xi] + wc[IDN];
+  float du[5];
+#pragma unroll
+  for (int v = 0; v < 5; ++v) du[v] = -dt * (d[v] * ivol);
+  if (g.nc1 > 1) du[IVX] += dt * b.rbar[xi];  // reference pressure gradient + rho_bar g1
+  if (p.grav1 != 0.) {
+    du[IVX] += dt * wc[IDN] * (float)p.grav1;
+    du[IPR] += dt * rho * wc[IVX] * (float)p.grav1;
+  }
+  if (p.grav2 != 0.) {
+    du[IVY] += dt * rho * (float)p.grav2;
+    du[IPR] += dt * rho * wc[IVY] * (float)p.grav2;
+  }
+  if (p.grav3 != 0.) {
+    du[IVZ] += dt * rho * (float)p.grav3;
+    du[IPR] += dt * rho * wc[IVZ] * (float)p.grav3;
+  }
+  float ds[NS > 0 ? NS : 1];
+#pragma unroll
+  for (int n = 0; n < NS; ++n) ds[n] = -dt * (d[5 + n] * ivol);
+  if (b.write_du) {
+#pragma unroll
+    for (int v = 0; v < 5; ++v) b.D[v * sv + off] = du[v];
+#pragma unroll
+    for (int n = 0; n < NS; ++n) b.D[(5 + n) * sv + off] = ds[n];
+    return;
+  }
+  const float w0 = (float)b.wgt0, w1 = (float)b.wgt1, w2 = (float)b.wgt2;
+  float unew_rho = 0.f;
+#pragma unroll
+  for (int v = 0; v < 5; ++v) {
+    int64_t o = v * sv + off;
+    float uo = b.u[o];
+    float u0v;
+    if (b.stage == 0) {
+      u0v = uo;
+      b.u0[o] = uo;
+    } else {
+      u0v = b.u0[o];
+    }
+    float un = w0 * u0v + w1 * uo + w2 * du[v];
+    b.u[o] = un;
+    if (v == IDN) unew_rho = b.rbf[xi] + un;
+  }
+#pragma unroll
+  for (int n = 0; n < NS; ++n) {
+    int64_t o = n * sv + off;
+    float so = b.s[o];
+    float s0v;
+    if (b.stage == 0) {
+      s0v = so;
+      b.s0[o] = so;
+    } else {
+      s0v = b.s0[o];
+    }
+    float sn = w0 * s0v + w1 * so + w2 * ds[n];
+    b.s[o] = sn;
+    if (b.r) b.r[o] = sn / unew_rho;
+  }
+}
+
+// U' -> W' of one cell at x1 index xi (p' = (gamma-1)(E' - KE): no
+// reference-sized cancellation)
+__device__ __forceinline__ void cons2prim_pert(const float* u, float* w, float rbar, float gm1) {
+  float rho = rbar + u[IDN];
+  float ir = 1.f / rho;
+  w[IDN] = u[IDN];
+  w[IVX] = u[IVX] * ir;
+  w[IVY] = u[IVY] * ir;
+  w[IVZ] = u[IVZ] * ir;
+  float ke = 0.5f * (w[IVX] * u[IVX] + w[IVY] * u[IVY] + w[IVZ] * u[IVZ]);
+  w[IPR] = gm1 * (u[IPR] - ke);
+}
+
+// ---------------------------------------------------------------------------
+// x1 column kernel
+// ---------------------------------------------------------------------------
+size_t x1_smem32_per_column(const Geo& g, int nvt) {
+  return (size_t)(2 * nvt) * g.nc1 * sizeof(float);
+}
+
+template <int NS>
+__global__ void __launch_bounds__(256) k_x1_32(Geo g, Phys p, StageBufs32 b, int C, int last) {
+  constexpr int NV = 5 + NS;
+  extern __shared__ float smf[];
+  const int nc1 = g.nc1;
+  float* sw = smf;
+  float* sf = sw + (size_t)C * NV * nc1;
+  const int64_t ncol = (int64_t)g.nc2 * g.nc3;
+  const int64_t col0 = (int64_t)blockIdx.x * C;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int64_t sv = g.sv;
+  const float gm1 = (float)(p.gammad - 1.);
+  const float gamma = (float)p.gammad;
+
+  for (int idx = tid; idx < C * nc1; idx += nt) {
+    int c = idx / nc1, i = idx - c * nc1;
+    int64_t col = col0 + c;
+    if (col >= ncol) continue;
+    int64_t off = col * nc1 + i;
+    float uc[5], wc[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) uc[v] = b.u[v * sv + off];
+    cons2prim_pert(uc, wc, b.rbf[i], gm1);
+#pragma unroll
+    for (int v = 0; v < 5; ++v) sw[(c * NV + v) * nc1 + i] = wc[v];
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+      float rr = b.s[n * sv + off] / (b.rbf[i] + uc[IDN]);
+      sw[(c * NV + 5 + n) * nc1 + i] = rr;
+      b.R[n * sv + off] = rr;
+    }
+  }
+  __syncthreads();
+
+  // isentropic x1 ghost revision on full values, in FP64
+  if (p.grav1 != 0. && tid < C && col0 + tid < ncol) {
+    float* pp = sw + (tid * NV + IPR) * nc1;
+    float* rr = sw + (tid * NV + IDN) * nc1;
+    const double gam = p.gammad;
+    const double a = (gam - 1.) / gam, ig = 1. / gam, ia = 1. / a;
+    const double grav = -p.grav1, dz = g.dx1;
+    const int is = g.il, ie = g.iu;
+    double ps = b.pb[is] + pp[is], rs = b.rb[is] + rr[is];
+    double K = ps / pow(rs, gam), kg = pow(K, ig);
+    double pc = ps;
+    for (int n = 0; n < g.ng; ++n) {
+      double h = pow(pc, a) + a * grav * dz / kg;
+      double pn = pow(h, ia);
+      double rn = pow(pn / K, ig);
+      pp[is - n - 1] = (float)(pn - b.pb[is - n - 1]);
+      rr[is - n - 1] = (float)(rn - b.rb[is - n - 1]);
+      pc = pn;
+    }
+    ps = b.pb[ie] + pp[ie];
+    rs = b.rb[ie] + rr[ie];
+    K = ps / pow(rs, gam);
+    kg = pow(K, ig);
+    pc = ps;
+    for (int n = 0; n < g.ng; ++n) {
+      double h = pow(pc, a) - a * grav * dz / kg;
+      double pn = pow(h, ia);
+      double rn = pow(pn / K, ig);
+      pp[ie + n + 1] = (float)(pn - b.pb[ie + n + 1]);
+      rr[ie + n + 1] = (float)(rn - b.rb[ie + n + 1]);
+      pc = pn;
+    }
+  }
+  __syncthreads();
+
+  for (int idx = tid; idx < C * nc1; idx += nt) {
+    int c = idx / nc1, i = idx - c * nc1;
+    int64_t col = col0 + c;
+    if (col >= ncol) continue;
+    int64_t off = col * nc1 + i;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) b.w[v * sv + off] = sw[(c * NV + v) * nc1 + i];
+  }
+
+  const int nf = g.nx1 + 1;
+  const int ptype = (p.r1_shock) ? p.r1_type : interp2_of(p.r1_type);
+  for (int idx = tid; idx < C * nf; idx += nt) {
+    int c = idx / nf, f = g.il + (idx - c * nf);
+    int64_t col = col0 + c;
+    if (col >= ncol) continue;
+    int j = (int)(col % g.nc2), k = (int)(col / g.nc2);
+    if (j < g.jl || j > g.ju || k < g.kl || k > g.ku) continue;
+    const float* base = sw + (size_t)c * NV * nc1;
+    float L[NV], R[NV], F[NV];
+    float pl, pr;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      float q[6];
+#pragma unroll
+      for (int t = 0; t < 6; ++t) {
+        int cell = min(max(f - 3 + t, 0), nc1 - 1);
+        q[t] = base[v * nc1 + cell];
+        if (v == IDN) q[t] += b.rbf[cell];  // density reconstructed as a full field
+      }
+      if (v == IPR) {
+        face_states<float>(ptype, p.r1_scale != 0, q, pl, pr);
+        pl += b.offL[f];
+        pr += b.offR[f];
+      } else if (v < 5) {
+        int typ = (p.r1_shock || v == IDN) ? p.r1_type : interp2_of(p.r1_type);
+        face_states<float>(typ, p.r1_scale != 0, q, L[v], R[v]);
+      } else {
+        face_states<float>(p.rs_type, p.rs_scale != 0, q, L[v], R[v]);
+        L[v] = L[v] < 0.f ? 0.f : L[v];
+        R[v] = R[v] < 0.f ? 0.f : R[v];
+      }
+    }
+    if (p.grav1 != 0.) {
+      if (f == g.il) {
+        pl = pr;
+        L[IDN] = R[IDN];
+      }
+      if (f == g.iu + 1) {
+        pr = pl;
+        R[IDN] = L[IDN];
+      }
+    }
+    const float pfv = (float)b.pf[f];
+    L[IPR] = pfv + pl;
+    R[IPR] = pfv + pr;
+    if (p.disable1) {
+#pragma unroll
+      for (int v = 0; v < 5; ++v) F[v] = 0.f;
+    } else {
+      riemann_flux_split(p.riemann, L, R, pl, pr, pfv, IVX, gamma, F);
+    }
+#pragma unroll
+    for (int n = 0; n < NS; ++n) F[5 + n] = F[IDN] > 0.f ? F[IDN] * L[5 + n] : F[IDN] * R[5 + n];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) sf[(c * NV + v) * nc1 + f] = F[v];
+  }
+  __syncthreads();
+
+  const float A1 = (float)g.A1;
+  for (int idx = tid; idx < C * g.nx1; idx += nt) {
+    int c = idx / g.nx1, i = g.il + (idx - c * g.nx1);
+    int64_t col = col0 + c;
+    if (col >= ncol) continue;
+    int j = (int)(col % g.nc2), k = (int)(col / g.nc2);
+    if (j < g.jl || j > g.ju || k < g.kl || k > g.ku) continue;
+    int64_t off = col * nc1 + i;
+    float d[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      const float* fv = sf + (c * NV + v) * nc1;
+      d[v] = A1 * fv[i + 1] - A1 * fv[i];
+    }
+    if (last) {
+      float wc[5];
+#pragma unroll
+      for (int v = 0; v < 5; ++v) wc[v] = sw[(c * NV + v) * nc1 + i];
+      finalize32<NS>(g, p, b, off, i, d, wc);
+    } else {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) b.D[v * sv + off] = d[v];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// x2 / x3 marching sweeps (reference constant along the sweep)
+// ---------------------------------------------------------------------------
+template <int NS, int AX>
+__global__ void __launch_bounds__(128) k_march32(Geo g, Phys p, StageBufs32 b, int seglen,
+                                                 int first, int last) {
+  constexpr int NV = 5 + NS;
+  const int ni = g.iu - g.il + 1;
+  int lo, hi, olo, ohi;
+  int64_t st, ost;
+  if (AX == 2) {
+    lo = g.jl, hi = g.ju, st = g.s2, olo = g.kl, ohi = g.ku, ost = g.s3;
+  } else {
+    lo = g.kl, hi = g.ku, st = g.s3, olo = g.jl, ohi = g.ju, ost = g.s2;
+  }
+  const int no = ohi - olo + 1;
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= (int64_t)ni * no) return;
+  const int i = g.il + (int)(tid % ni);
+  const int o = olo + (int)(tid / ni);
+  const int f0 = lo + blockIdx.y * seglen;
+  if (f0 > hi) return;
+  const int f1 = min(f0 + seglen, hi + 1);
+  const int64_t base = i + o * ost;
+  const int64_t sv = g.sv;
+  const int ivx = AX == 2 ? IVY : IVZ;
+  const float A = (float)(AX == 2 ? g.A2 : g.A3);
+  const int disabled = AX == 2 ? p.disable2 : p.disable3;
+  const int ncax = AX == 2 ? g.nc2 : g.nc3;
+  const float rref = b.rbf[i], pref = b.pbf[i];
+  const float gamma = (float)p.gammad;
+
+  float q[NV][6];
+  auto load = [&](int cell, int slot) {
+    cell = min(max(cell, 0), ncax - 1);
+    int64_t off = base + cell * st;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) q[v][slot] = b.w[v * sv + off];
+#pragma unroll
+    for (int n = 0; n < NS; ++n) q[5 + n][slot] = b.R[n * sv + off];
+  };
+#pragma unroll
+  for (int t = 0; t < 5; ++t) load(f0 - 3 + t, t);
+
+  float Fp[NV];
+  for (int f = f0; f <= f1; ++f) {
+    load(f + 2, 5);
+    float L[NV], R[NV], F[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      if (v < 5) {
+        int typ = (p.r23_shock || v == IDN) ? p.r23_type : interp2_of(p.r23_type);
+        face_states<float>(typ, p.r23_scale != 0, q[v], L[v], R[v]);
+      } else {
+        face_states<float>(p.rs_type, p.rs_scale != 0, q[v], L[v], R[v]);
+        L[v] = L[v] < 0.f ? 0.f : L[v];
+        R[v] = R[v] < 0.f ? 0.f : R[v];
+      }
+    }
+    float pl = L[IPR], pr = R[IPR];
+    L[IDN] += rref;
+    R[IDN] += rref;
+    L[IPR] += pref;
+    R[IPR] += pref;
+    if (disabled) {
+#pragma unroll
+      for (int v = 0; v < 5; ++v) F[v] = 0.f;
+    } else {
+      riemann_flux_split(p.riemann, L, R, pl, pr, pref, ivx, gamma, F);
+    }
+#pragma unroll
+    for (int n = 0; n < NS; ++n) F[5 + n] = F[IDN] > 0.f ? F[IDN] * L[5 + n] : F[IDN] * R[5 + n];
+    if (f > f0) {
+      const int64_t off = base + (int64_t)(f - 1) * st;
+      float d[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        d[v] = A * F[v] - A * Fp[v];
+        if (!first) d[v] = b.D[v * sv + off] + d[v];
+      }
+      if (last) {
+        float wc[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) wc[v] = q[v][2];
+        finalize32<NS>(g, p, b, off, i, d, wc);
+      } else {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) b.D[v * sv + off] = d[v];
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      Fp[v] = F[v];
+#pragma unroll
+      for (int t = 0; t < 5; ++t) q[v][t] = q[v][t + 1];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// boundary fills of perturbation arrays: as k_bc, plus the x1 offset of the
+// reference between the source and the ghost layer (rho, and E or p)
+// ---------------------------------------------------------------------------
+struct AxisBC32 {
+  int n, ng, lo_type, hi_type;
+};
+
+__device__ __forceinline__ int bc_map32(const AxisBC32& a, int i, bool& flip) {
+  flip = false;
+  if (a.n == 1) return i;
+  if (i < a.ng) {
+    switch (a.lo_type) {
+      case SNAPB_BC_REFLECTING: flip = true; return 2 * a.ng - 1 - i;
+      case SNAPB_BC_PERIODIC: return a.n - 2 * a.ng + i;
+      case SNAPB_BC_OUTFLOW: return a.ng;
+      default: return i;
+    }
+  }
+  if (i >= a.n - a.ng) {
+    switch (a.hi_type) {
+      case SNAPB_BC_REFLECTING: flip = true; return 2 * (a.n - a.ng) - 1 - i;
+      case SNAPB_BC_PERIODIC: return i - a.n + 2 * a.ng;
+      case SNAPB_BC_OUTFLOW: return a.n - a.ng - 1;
+      default: return i;
+    }
+  }
+  return i;
+}
+
+__global__ void k_bc32(int nc1, int nc2, int nc3, int64_t sv, AxisBC32 a1, AxisBC32 a2,
+                       AxisBC32 a3, float* var, int nv, int kind, const double* rb,
+                       const double* pb, double igm1) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= sv) return;
+  int i = (int)(t % nc1);
+  int j = (int)((t / nc1) % nc2);
+  int k = (int)(t / ((int64_t)nc1 * nc2));
+  bool f1, f2, f3;
+  int si = bc_map32(a1, i, f1), sj = bc_map32(a2, j, f2), sk = bc_map32(a3, k, f3);
+  if (si == i && sj == j && sk == k) return;
+  int64_t src = ((int64_t)sk * nc2 + sj) * nc1 + si;
+  bool flip = kind != SNAPB_SCALAR;
+  for (int v = 0; v < nv; ++v) {
+    double x = var[v * sv + src];
+    if (flip && ((v == IVX && f1) || (v == IVY && f2) || (v == IVZ && f3))) x = -x;
+    if (kind != SNAPB_SCALAR && si != i) {
+      if (v == IDN) x += rb[si] - rb[i];
+      if (v == IPR) x += (pb[si] - pb[i]) * (kind == SNAPB_CONSERVED ? igm1 : 1.0);
+    }
+    var[v * sv + t] = (float)x;
+  }
+}
+
+// conversions between the FP64 state and the FP32 perturbation
+__global__ void k_to_pert(int64_t n, int nc1, int kind, double igm1, const double* in,
+                          const double* rb, const double* pb, float* out) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  int i = (int)(t % nc1);
+  out[IDN * n + t] = (float)(in[IDN * n + t] - rb[i]);
+  out[IVX * n + t] = (float)in[IVX * n + t];
+  out[IVY * n + t] = (float)in[IVY * n + t];
+  out[IVZ * n + t] = (float)in[IVZ * n + t];
+  double pref = kind == SNAPB_CONSERVED ? pb[i] * igm1 : pb[i];
+  out[IPR * n + t] = (float)(in[IPR * n + t] - pref);
+}
+
+__global__ void k_from_pert(int64_t n, int nc1, int kind, double igm1, const float* in,
+                            const double* rb, const double* pb, double* out) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  int i = (int)(t % nc1);
+  out[IDN * n + t] = (double)in[IDN * n + t] + rb[i];
+  out[IVX * n + t] = in[IVX * n + t];
+  out[IVY * n + t] = in[IVY * n + t];
+  out[IVZ * n + t] = in[IVZ * n + t];
+  double pref = kind == SNAPB_CONSERVED ? pb[i] * igm1 : pb[i];
+  out[IPR * n + t] = (double)in[IPR * n + t] + pref;
+}
+
+// CFL limit from w' (full state formed in FP64)
+__device__ __forceinline__ double warp_min32(double x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x = fmin(x, __shfl_xor_sync(0xffffffffu, x, o));
+  return x;
+}
+
+__global__ void k_cfl32(Geo g, double gammad, int use1, int use2, int use3, const float* w,
+                        const double* rb, const double* pb, unsigned long long* slots) {
+  const int ni = g.iu - g.il + 1, nj = g.ju - g.jl + 1, nk = g.ku - g.kl + 1;
+  const int64_t n = (int64_t)ni * nj * nk;
+  double m1 = 1.7e308, m2 = 1.7e308, m3 = 1.7e308;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    int i = g.il + (int)(t % ni);
+    int j = g.jl + (int)((t / ni) % nj);
+    int k = g.kl + (int)(t / ((int64_t)ni * nj));
+    int64_t o = (int64_t)k * g.s3 + (int64_t)j * g.s2 + i;
+    double rho = rb[i] + w[IDN * g.sv + o], pr = pb[i] + w[IPR * g.sv + o];
+    double cs = sqrt(gammad * pr / rho);
+    if (use1) m1 = fmin(m1, g.dx1 / (fabs((double)w[IVX * g.sv + o]) + cs));
+    if (use2) m2 = fmin(m2, g.dx2 / (fabs((double)w[IVY * g.sv + o]) + cs));
+    if (use3) m3 = fmin(m3, g.dx3 / (fabs((double)w[IVZ * g.sv + o]) + cs));
+  }
+  __shared__ double red[3][32];
+  m1 = warp_min32(m1);
+  m2 = warp_min32(m2);
+  m3 = warp_min32(m3);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) {
+    red[0][wid] = m1;
+    red[1][wid] = m2;
+    red[2][wid] = m3;
+  }
+  __syncthreads();
+  if (wid == 0) {
+    int nw = blockDim.x >> 5;
+    m1 = lane < nw ? red[0][lane] : 1.7e308;
+    m2 = lane < nw ? red[1][lane] : 1.7e308;
+    m3 = lane < nw ? red[2][lane] : 1.7e308;
+    m1 = warp_min32(m1);
+    m2 = warp_min32(m2);
+    m3 = warp_min32(m3);
+    if (lane == 0) {
+      atomicMin(&slots[0], (unsigned long long)__double_as_longlong(m1));
+      atomicMin(&slots[1], (unsigned long long)__double_as_longlong(m2));
+      atomicMin(&slots[2], (unsigned long long)__double_as_longlong(m3));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// launchers (called from capi32.cu)
+// ---------------------------------------------------------------------------
+cudaError_t launch_ref32(const Geo& g, const Phys& p, const double* rb, const double* pb,
+                         double* rbw, double* pbw, const StageBufs32& b, cudaStream_t st) {
+  int n = g.nc1 + 1;
+  k_ref32<<<(n + 127) / 128, 128, 0, st>>>(g, p, rb, pb, rbw, pbw, b);
+  k_ref32_residual<<<(n + 127) / 128, 128, 0, st>>>(g, p, b);
+  return cudaGetLastError();
+}
+
+int x1_columns_per_cta32(const Geo& g, int nvt) {
+  size_t per = x1_smem32_per_column(g, nvt);
+  int c = (int)std::max<size_t>(1, (96 * 1024) / per);
+  return std::min(c, 16);
+}
+
+template <int NS>
+static cudaError_t launch_x1_32t(const Geo& g, const Phys& p, const StageBufs32& b, bool last,
+                                 cudaStream_t st) {
+  const int nvt = 5 + NS;
+  int C = x1_columns_per_cta32(g, nvt);
+  size_t smem = (size_t)C * x1_smem32_per_column(g, nvt);
+  if (smem > 200 * 1024) return cudaErrorInvalidConfiguration;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(k_x1_32<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_set = true;
+  }
+  int64_t ncol = (int64_t)g.nc2 * g.nc3;
+  k_x1_32<NS><<<(unsigned)((ncol + C - 1) / C), 256, smem, st>>>(g, p, b, C, last ? 1 : 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_x1_32(const Geo& g, const Phys& p, const StageBufs32& b, bool last,
+                         cudaStream_t st) {
+  switch (p.nscalar) {
+    case 0: return launch_x1_32t<0>(g, p, b, last, st);
+    case 1: return launch_x1_32t<1>(g, p, b, last, st);
+    case 2: return launch_x1_32t<2>(g, p, b, last, st);
+    case 3: return launch_x1_32t<3>(g, p, b, last, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <int NS, int AX>
+static cudaError_t launch_march32_t(const Geo& g, const Phys& p, const StageBufs32& b,
+                                    bool first, bool last, cudaStream_t st) {
+  int ni = g.iu - g.il + 1;
+  int no = AX == 2 ? g.ku - g.kl + 1 : g.ju - g.jl + 1;
+  int n = AX == 2 ? g.nx2 : g.nx3;
+  int seglen = 32;
+  int64_t threads = (int64_t)ni * no;
+  while (seglen > 8 && threads * ((n + seglen - 1) / seglen) < 148LL * 1024 * 2) seglen /= 2;
+  dim3 grid((unsigned)((threads + 127) / 128), (unsigned)((n + seglen - 1) / seglen));
+  k_march32<NS, AX><<<grid, 128, 0, st>>>(g, p, b, seglen, first ? 1 : 0, last ? 1 : 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_march32(int axis, const Geo& g, const Phys& p, const StageBufs32& b,
+                           bool first, bool last, cudaStream_t st) {
+#define SNAPB_MARCH32(NS)                                                  \
+  case NS:                                                                 \
+    return axis == 2 ? launch_march32_t<NS, 2>(g, p, b, first, last, st)  \
+                     : launch_march32_t<NS, 3>(g, p, b, first, last, st);
+  switch (p.nscalar) {
+    SNAPB_MARCH32(0)
+    SNAPB_MARCH32(1)
+    SNAPB_MARCH32(2)
+    SNAPB_MARCH32(3)
+  }
+#undef SNAPB_MARCH32
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_bc32(const Geo& g, const snapb_hydro_config& c, float* var, int nv, int kind,
+                        const double* rb, const double* pb, cudaStream_t st) {
+  AxisBC32 a1{g.nc1, g.ng, c.bc[0], c.bc[1]};
+  AxisBC32 a2{g.nc2, g.ng, c.bc[2], c.bc[3]};
+  AxisBC32 a3{g.nc3, g.ng, c.bc[4], c.bc[5]};
+  k_bc32<<<(unsigned)((g.sv + 255) / 256), 256, 0, st>>>(g.nc1, g.nc2, g.nc3, g.sv, a1, a2, a3,
+                                                         var, nv, kind, rb, pb,
+                                                         1.0 / (c.gammad - 1.0));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_to_pert(const Geo& g, const Phys& p, int kind, const double* in,
+                           const double* rb, const double* pb, float* out, cudaStream_t st) {
+  k_to_pert<<<(unsigned)((g.sv + 255) / 256), 256, 0, st>>>(g.sv, g.nc1, kind,
+                                                            1.0 / (p.gammad - 1.0), in, rb, pb,
+                                                            out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_from_pert(const Geo& g, const Phys& p, int kind, const float* in,
+                             const double* rb, const double* pb, double* out, cudaStream_t st) {
+  k_from_pert<<<(unsigned)((g.sv + 255) / 256), 256, 0, st>>>(g.sv, g.nc1, kind,
+                                                              1.0 / (p.gammad - 1.0), in, rb, pb,
+                                                              out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cfl32(const Geo& g, const Phys& p, const float* w, const double* rb,
+                         const double* pb, unsigned long long* slots, cudaStream_t st) {
+  int scheme = p.implicit_scheme;
+  int use1 = g.nc1 > 1, use2 = g.nc2 > 1, use3 = g.nc3 > 1;
+  if (scheme != 0) {
+    use1 = use1 && (!(scheme & 1) || (g.nc3 == 1 && g.nc2 == 1));
+    use2 = use2 && !((scheme >> 1) & 1);
+    use3 = use3 && !((scheme >> 2) & 1);
+  }
+  int64_t n = (int64_t)(g.iu - g.il + 1) * (g.ju - g.jl + 1) * (g.ku - g.kl + 1);
+  int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
+  k_cfl32<<<blocks, 256, 0, st>>>(g, p.gammad, use1, use2, use3, w, rb, pb, slots);
+  return cudaGetLastError();
+}
+
+}  // namespace snapb

@@ -267,11 +267,72 @@ __device__ __forceinline__ int64_t column_base(const Geo& g, int64_t col) {
   return (int64_t)k * g.s3 + (int64_t)j * g.s2 + g.il;
 }
 
+// ---- state access, FP64 plain form and FP32 perturbation form ----
+// full primitive of variable v at offset off, x1 index xi
+__device__ __forceinline__ double vic_w(const StageBufs& b, int64_t sv, int v, int64_t off,
+                                        int xi) {
+  return b.w[v * sv + off];
+}
+__device__ __forceinline__ double vic_w(const StageBufs32& b, int64_t sv, int v, int64_t off,
+                                        int xi) {
+  double x = (double)b.w[v * sv + off];
+  if (v == IDN) x += b.rb[xi];
+  if (v == IPR) x += b.pb[xi];
+  return x;
+}
+__device__ __forceinline__ double vic_d(const StageBufs& b, int64_t idx) { return b.D[idx]; }
+__device__ __forceinline__ double vic_d(const StageBufs32& b, int64_t idx) {
+  return (double)b.D[idx];
+}
+__device__ __forceinline__ void vic_set_d(const StageBufs& b, int64_t idx, double x) {
+  b.D[idx] = x;
+}
+__device__ __forceinline__ void vic_set_d(const StageBufs32& b, int64_t idx, double x) {
+  b.D[idx] = (float)x;
+}
+// RK combination of one stored value (u' for the FP32 form: the reference
+// part of u is constant in time, so the combination is the same)
+__device__ __forceinline__ double vic_rk(double* q, double* q0, int64_t o, int stage, double w0,
+                                         double w1, double w2, double d) {
+  double qo = q[o];
+  double q0v;
+  if (stage == 0) {
+    q0v = qo;
+    q0[o] = qo;
+  } else {
+    q0v = q0[o];
+  }
+  double qn = w0 * q0v + w1 * qo + w2 * d;
+  q[o] = qn;
+  return qn;
+}
+__device__ __forceinline__ double vic_rk(float* q, float* q0, int64_t o, int stage, double w0,
+                                         double w1, double w2, double d) {
+  double qo = q[o];
+  double q0v;
+  if (stage == 0) {
+    q0v = qo;
+    q0[o] = (float)qo;
+  } else {
+    q0v = q0[o];
+  }
+  float qn = (float)(w0 * q0v + w1 * qo + w2 * d);
+  q[o] = qn;
+  return qn;
+}
+// full density of a stored conserved perturbation
+__device__ __forceinline__ double vic_full_rho(const StageBufs&, double u_rho, int) {
+  return u_rho;
+}
+__device__ __forceinline__ double vic_full_rho(const StageBufs32& b, double u_rho, int xi) {
+  return u_rho + b.rb[xi];
+}
+
 // (1) assembly: every (column, t) in parallel.  The tile's cells are staged
 // through shared memory with loads along x1 (coalesced), the entries are
 // written with the column index fastest (coalesced).
-template <int N>
-__global__ void __launch_bounds__(256) k_vic_assemble(Geo g, Phys p, StageBufs b) {
+template <int N, class B>
+__global__ void __launch_bounds__(256) k_vic_assemble(Geo g, Phys p, B b) {
   constexpr int E1 = VicDims<N>::E1;
   const int nl = g.nx1;
   const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
@@ -287,7 +348,8 @@ __global__ void __launch_bounds__(256) k_vic_assemble(Geo g, Phys p, StageBufs b
     int cell = t0 - 1 + s;  // relative to il; valid range [-1, nl]
     int64_t col = col0 + c;
     double x = 0.;
-    if (col < ncol && cell >= -1 && cell <= nl) x = b.w[v * sv + column_base(g, col) + cell];
+    if (col < ncol && cell >= -1 && cell <= nl)
+      x = vic_w(b, sv, v, column_base(g, col) + cell, g.il + cell);
     ws[v][c][s] = x;
   }
   for (int idx = tid; idx < N * kTC * kTLA; idx += blockDim.x) {
@@ -296,7 +358,7 @@ __global__ void __launch_bounds__(256) k_vic_assemble(Geo g, Phys p, StageBufs b
     int cell = t0 + s;
     int64_t col = col0 + c;
     double x = 0.;
-    if (col < ncol && cell < nl) x = b.D[sel<N>(r) * sv + column_base(g, col) + cell];
+    if (col < ncol && cell < nl) x = vic_d(b, sel<N>(r) * sv + column_base(g, col) + cell);
     ds[r][c][s] = x;
   }
   __syncthreads();
@@ -339,8 +401,8 @@ __global__ void __launch_bounds__(256) k_vic_assemble(Geo g, Phys p, StageBufs b
 }
 
 // (2) block-Thomas sweep, one thread per column, every access coalesced.
-template <int N>
-__global__ void __launch_bounds__(128) k_vic_sweep(Geo g, Phys p, StageBufs b) {
+template <int N, class B>
+__global__ void __launch_bounds__(128) k_vic_sweep(Geo g, Phys p, B b) {
   constexpr int E1 = VicDims<N>::E1, ES = VicDims<N>::ES;
   const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
   const int64_t col = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -469,8 +531,8 @@ __global__ void __launch_bounds__(128) k_vic_sweep(Geo g, Phys p, StageBufs b) {
 // (3) redistribution + RK combination (or du), tiles of 32 columns x 32
 // layers: delta is transposed through shared memory so that the state
 // arrays are read and written along x1.
-template <int N, int NS>
-__global__ void __launch_bounds__(256) k_vic_finish(Geo g, Phys p, StageBufs b) {
+template <int N, int NS, class B>
+__global__ void __launch_bounds__(256) k_vic_finish(Geo g, Phys p, B b) {
   constexpr int E1 = VicDims<N>::E1, ES = VicDims<N>::ES;
   const int nl = g.nx1;
   const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
@@ -500,16 +562,17 @@ __global__ void __launch_bounds__(256) k_vic_finish(Geo g, Phys p, StageBufs b) 
     int i = i0 + s;
     if (col >= ncol || i >= nl) continue;
     const int64_t off = column_base(g, col) + i;
-    double rho = b.w[IDN * sv + off];
+    const int xi = g.il + i;
+    double rho = vic_w(b, sv, IDN, off, xi);
     double ai = rho * g.vol;
-    double et = b.D[IDN * sv + off];
+    double et = vic_d(b, IDN * sv + off);
     double fix = dl[0][c][s] - et;
     double du[5];
     du[IDN] = et + fix * 1. + rho * ai * zs[1][c] / zs[0][c];
     if constexpr (N == 3) {
       du[IVX] = dl[1][c][s];
-      du[IVY] = b.D[IVY * sv + off];
-      du[IVZ] = b.D[IVZ * sv + off];
+      du[IVY] = vic_d(b, IVY * sv + off);
+      du[IVZ] = vic_d(b, IVZ * sv + off);
       du[IPR] = dl[2][c][s];
     } else {
 #pragma unroll
@@ -518,66 +581,51 @@ __global__ void __launch_bounds__(256) k_vic_finish(Geo g, Phys p, StageBufs b) 
     if (b.M) b.M[IDN * sv + off] = fix;
     if (b.vic_du_only) {
 #pragma unroll
-      for (int v = 0; v < 5; ++v) b.D[v * sv + off] = du[v];
+      for (int v = 0; v < 5; ++v) vic_set_d(b, v * sv + off, du[v]);
       continue;
     }
     double unew_rho = 0.;
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
-      int64_t o = v * sv + off;
-      double uo = b.u[o];
-      double u0v;
-      if (b.stage == 0) {
-        u0v = uo;
-        b.u0[o] = uo;
-      } else {
-        u0v = b.u0[o];
-      }
-      double un = b.wgt0 * u0v + b.wgt1 * uo + b.wgt2 * du[v];
-      b.u[o] = un;
-      if (v == IDN) unew_rho = un;
+      double un = vic_rk(b.u, b.u0, v * sv + off, b.stage, b.wgt0, b.wgt1, b.wgt2, du[v]);
+      if (v == IDN) unew_rho = vic_full_rho(b, un, xi);
     }
 #pragma unroll
     for (int n = 0; n < NS; ++n) {
       int64_t o = n * sv + off;
-      double ds = b.D[(5 + n) * sv + off] + fix * b.r[o];
-      double so = b.s[o];
-      double s0v;
-      if (b.stage == 0) {
-        s0v = so;
-        b.s0[o] = so;
-      } else {
-        s0v = b.s0[o];
-      }
-      double sn = b.wgt0 * s0v + b.wgt1 * so + b.wgt2 * ds;
-      b.s[o] = sn;
+      double ds = vic_d(b, (5 + n) * sv + off) + fix * (double)b.r[o];
+      double sn = vic_rk(b.s, b.s0, o, b.stage, b.wgt0, b.wgt1, b.wgt2, ds);
       b.r[o] = sn / unew_rho;
     }
   }
 }
 
-template <int N>
-static cudaError_t launch_vic_n(const Geo& g, const Phys& p, const StageBufs& b,
-                                cudaStream_t st) {
+template <int N, class B>
+static cudaError_t launch_vic_n(const Geo& g, const Phys& p, const B& b, cudaStream_t st) {
   const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
   const int nl = g.nx1;
   dim3 ga((unsigned)((ncol + kTC - 1) / kTC), (unsigned)((nl + 2 + kTLA - 1) / kTLA));
-  k_vic_assemble<N><<<ga, 256, 0, st>>>(g, p, b);
+  k_vic_assemble<N, B><<<ga, 256, 0, st>>>(g, p, b);
   // small column counts: narrower CTAs spread the sequential sweeps over more SMs
   int bs = ncol >= 148 * 128 ? 128 : (ncol >= 148 * 64 ? 64 : 32);
-  k_vic_sweep<N><<<(unsigned)((ncol + bs - 1) / bs), bs, 0, st>>>(g, p, b);
+  k_vic_sweep<N, B><<<(unsigned)((ncol + bs - 1) / bs), bs, 0, st>>>(g, p, b);
   dim3 gf((unsigned)((ncol + kTC - 1) / kTC), (unsigned)((nl + kTL - 1) / kTL));
   switch (p.nscalar) {
-    case 0: k_vic_finish<N, 0><<<gf, 256, 0, st>>>(g, p, b); break;
-    case 1: k_vic_finish<N, 1><<<gf, 256, 0, st>>>(g, p, b); break;
-    case 2: k_vic_finish<N, 2><<<gf, 256, 0, st>>>(g, p, b); break;
-    case 3: k_vic_finish<N, 3><<<gf, 256, 0, st>>>(g, p, b); break;
+    case 0: k_vic_finish<N, 0, B><<<gf, 256, 0, st>>>(g, p, b); break;
+    case 1: k_vic_finish<N, 1, B><<<gf, 256, 0, st>>>(g, p, b); break;
+    case 2: k_vic_finish<N, 2, B><<<gf, 256, 0, st>>>(g, p, b); break;
+    case 3: k_vic_finish<N, 3, B><<<gf, 256, 0, st>>>(g, p, b); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
 }
 
 cudaError_t launch_vic(const Geo& g, const Phys& p, const StageBufs& b, cudaStream_t st) {
+  if (vic_n(p) == 5) return launch_vic_n<5>(g, p, b, st);
+  return launch_vic_n<3>(g, p, b, st);
+}
+
+cudaError_t launch_vic32(const Geo& g, const Phys& p, const StageBufs32& b, cudaStream_t st) {
   if (vic_n(p) == 5) return launch_vic_n<5>(g, p, b, st);
   return launch_vic_n<3>(g, p, b, st);
 }

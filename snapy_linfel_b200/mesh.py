@@ -152,3 +152,141 @@ class MeshBlock:
     def totals(self):
         """Domain totals of the conserved variables (mass0, ..., energy)."""
         return self.interior(self.hydro_u).sum(dim=(1, 2, 3))
+
+
+class MeshBlockF32:
+    """The FP32 perturbation form of MeshBlock.
+
+    hydro_u / hydro_w / scalar_* are FP32 perturbations about an FP64
+    reference profile (rho_bar(x1), p_bar(x1)); by default the reference is
+    the horizontal mean of the initial state.  ``state64()`` returns the FP64
+    conserved state.  Same call sequence as MeshBlock.
+    """
+
+    def __init__(self, options: MeshBlockOptions | HydroConfig, device=None):
+        import torch
+
+        if isinstance(options, HydroConfig):
+            options = MeshBlockOptions(options)
+        self.options = options
+        self.cfg = options.hydro
+        self.device = torch.device(device if device is not None else "cuda")
+        self.lib = _lib.lib()
+        c = self.cfg
+        nbytes = self.lib.snapb_workspace_size_f32(ctypes.byref(c))
+        if nbytes == 0:
+            raise _lib.SnapbError("configuration not supported by the FP32 form: " +
+                                  self.lib.snapb_last_error().decode())
+        f32 = dict(dtype=torch.float32, device=self.device)
+        f64 = dict(dtype=torch.float64, device=self.device)
+        self.hydro_u = torch.zeros(c.shape, **f32)
+        self.hydro_u0 = torch.zeros(c.shape, **f32)
+        self.hydro_w = torch.zeros(c.shape, **f32)
+        ns = c.nscalar
+        self.scalar_s = torch.zeros(c.scalar_shape, **f32) if ns else None
+        self.scalar_s0 = torch.zeros(c.scalar_shape, **f32) if ns else None
+        self.scalar_r = torch.zeros(c.scalar_shape, **f32) if ns else None
+        self.workspace = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        self.ref_rho = torch.zeros(c.nc1, **f64)
+        self.ref_p = torch.zeros(c.nc1, **f64)
+        self.dt_raw = torch.zeros(1, **f64)
+        self.dt = torch.zeros(1, **f64)
+        self.cycle = 0
+        self.current_redo = 0
+
+    def _call(self, name, *args):
+        _lib.check(getattr(self.lib, name)(*args), name)
+
+    def _ws(self):
+        return _lib.ptr(self.workspace), ctypes.c_size_t(self.workspace.numel())
+
+    def initialize(self, hydro_w, scalar_r=None, reference="mean"):
+        """reference: "mean" (horizontal mean of the initial state at each x1
+        level, ghosts included), None (zero reference: plain FP32), or a pair
+        (rho_bar, p_bar) of [nc1] arrays."""
+        import torch
+
+        c = self.cfg
+        st = _lib.stream_ptr()
+        w64 = torch.as_tensor(hydro_w, dtype=torch.float64).to(self.device).contiguous()
+        self._call("snapb_bc_apply", ctypes.byref(c), _lib.ptr(w64), c.nvar, PRIMITIVE, st)
+        it = self.cfg.interior()
+        ws, nb = self._ws()
+        if reference is None:
+            self.ref_rho.zero_()
+            self.ref_p.zero_()
+            self._call("snapb_reference_f32", ctypes.byref(c), None, None, ws, nb, st)
+        else:
+            if isinstance(reference, str) and reference == "mean":
+                ref_rho = w64[0][it[0], it[1], :].mean(dim=(0, 1))
+                ref_p = w64[4][it[0], it[1], :].mean(dim=(0, 1))
+            else:
+                ref_rho, ref_p = reference
+            self.ref_rho.copy_(torch.as_tensor(ref_rho, dtype=torch.float64))
+            self.ref_p.copy_(torch.as_tensor(ref_p, dtype=torch.float64))
+            self._call("snapb_reference_f32", ctypes.byref(c), _lib.ptr(self.ref_rho),
+                       _lib.ptr(self.ref_p), ws, nb, st)
+        u64 = torch.empty_like(w64)
+        self._call("snapb_prim2cons", ctypes.byref(c), _lib.ptr(w64), _lib.ptr(u64), st)
+        s64 = None
+        if c.nscalar:
+            r64 = torch.as_tensor(scalar_r, dtype=torch.float64).to(self.device).contiguous()
+            self._call("snapb_bc_apply", ctypes.byref(c), _lib.ptr(r64), c.nscalar, SCALAR, st)
+            s64 = (w64[0:1] * r64).contiguous()
+            self._call("snapb_bc_apply", ctypes.byref(c), _lib.ptr(s64), c.nscalar, SCALAR, st)
+            self.scalar_s.copy_(s64)
+            self.scalar_r.copy_(r64)
+        self._call("snapb_bc_apply", ctypes.byref(c), _lib.ptr(u64), c.nvar, CONSERVED, st)
+        self._call("snapb_to_perturbation", ctypes.byref(c), CONSERVED, _lib.ptr(u64),
+                   _lib.ptr(self.hydro_u), ws, nb, st)
+        self._call("snapb_to_perturbation", ctypes.byref(c), PRIMITIVE, _lib.ptr(w64),
+                   _lib.ptr(self.hydro_w), ws, nb, st)
+        return 0.0
+
+    def max_time_step(self):
+        c = self.cfg
+        st = _lib.stream_ptr()
+        ws, nb = self._ws()
+        self._call("snapb_max_time_step_f32", ctypes.byref(c), _lib.ptr(self.hydro_w),
+                   _lib.ptr(self.dt_raw), ws, nb, st)
+        self._call("snapb_scale_dt", _lib.ptr(self.dt_raw),
+                   ctypes.c_double(self.options.integration.cfl), self.current_redo,
+                   _lib.ptr(self.dt), st)
+        return self.dt
+
+    def set_dt(self, dt: float):
+        self.dt.fill_(float(dt))
+        return self.dt
+
+    def forward(self, stage: int, dt=None):
+        if dt is not None and dt is not self.dt:
+            self.set_dt(dt)
+        c = self.cfg
+        ws, nb = self._ws()
+        self._call("snapb_stage_f32", ctypes.byref(c), int(stage), _lib.ptr(self.dt),
+                   _lib.ptr(self.hydro_u), _lib.ptr(self.hydro_u0), _lib.ptr(self.hydro_w),
+                   _lib.ptr(self.scalar_s), _lib.ptr(self.scalar_s0), _lib.ptr(self.scalar_r),
+                   ws, nb, _lib.stream_ptr())
+
+    def step(self, dt=None):
+        if dt is None:
+            self.max_time_step()
+        else:
+            self.set_dt(dt)
+        for s in range(3):
+            self.forward(s)
+        self.cycle += 1
+
+    def state64(self):
+        """FP64 conserved state u = u_bar + u'."""
+        import torch
+
+        c = self.cfg
+        out = torch.empty(c.shape, dtype=torch.float64, device=self.device)
+        ws, nb = self._ws()
+        self._call("snapb_from_perturbation", ctypes.byref(c), CONSERVED, _lib.ptr(self.hydro_u),
+                   _lib.ptr(out), ws, nb, _lib.stream_ptr())
+        return out
+
+    def interior(self, t):
+        return t[(slice(None),) + self.cfg.interior()]
