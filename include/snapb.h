@@ -257,6 +257,47 @@ int snapb_max_time_step_f32(const snapb_hydro_config* cfg, const float* w,
                             double* dt_out, void* workspace,
                             size_t workspace_bytes, void* stream);
 
+/* ---- adjoint (reverse mode) of the FP64 stage ----
+ * No counterpart in the reference, which has no adjoint: these are the
+ * `*_adjoint` entry points of the hydro step.  dt is a constant of the
+ * adjoint (the CFL choice is not differentiated); every switch of the
+ * forward path (Riemann wave selections, upwinding, clamps) is differentiated
+ * on the branch the forward pass takes at the given state.  Supported: all
+ * reconstructions and hydro Riemann solvers, gravity with non_hydrostatic
+ * = 1, implicit schemes 0 / 1 / 9, passive scalars, reflecting / periodic /
+ * outflow boundaries; diffusion is rejected with SNAPB_ERR_ARG.
+ *
+ * The workspace is separate from (and larger than) the forward one. */
+size_t snapb_adjoint_workspace_size(const snapb_hydro_config* cfg);
+
+/* Reverse of snapb_stage: u, s are the stage-START state (ghosts filled, as
+ * snapb_stage received them); gu_out, gs_out the cotangents of the stage's
+ * output (full arrays, after its boundary fill).  Writes gu, gs (full arrays,
+ * ghost entries included: cotangents of the input arrays, the wgt1 term of
+ * the RK combination included) and ADDS wgt0 * BC^T(gu_out) to gu0, gs0 on
+ * the interior (the step-start state; at stage 0 u0 is u, so the caller adds
+ * gu0 to gu after the stage-0 reverse).  gs_out, gs, gs0 may be null when
+ * nscalar = 0.  The scalar mass-fix term uses s / rho of the stage input as
+ * the mixing ratio, which equals the forward's scalar_r after any stage. */
+int snapb_stage_adjoint(const snapb_hydro_config* cfg, int stage, const double* dt,
+                        const double* u, const double* s, const double* gu_out,
+                        const double* gs_out, double* gu, double* gs, double* gu0,
+                        double* gs0, void* workspace, size_t workspace_bytes,
+                        void* stream);
+
+/* Reverse of snapb_hydro_forward (du including the implicit correction):
+ * g_u = (d du / d u)^T g_du over the full array; g_du is read on the
+ * interior. */
+int snapb_hydro_forward_adjoint(const snapb_hydro_config* cfg, const double* dt,
+                                const double* u, const double* g_du, double* g_u,
+                                void* workspace, size_t workspace_bytes, void* stream);
+
+/* Reverse of snapb_bc_apply (out of place): interior cells gather the
+ * cotangents of their ghost images (sign flips of reflecting normals for
+ * kind != SNAPB_SCALAR), ghost entries of g_out are zero. */
+int snapb_bc_adjoint(const snapb_hydro_config* cfg, const double* g_in, double* g_out, int nv,
+                     int kind, void* stream);
+
 /* ---- diagnostics: per-kernel device time ----
  * While enabled, snapb_stage and snapb_hydro_forward record a CUDA event pair
  * around every kernel they launch.  snapb_timing_query synchronizes those

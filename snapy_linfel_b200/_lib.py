@@ -60,6 +60,10 @@ def lib():
         "snapb_stage_f32": (i, [cp, i, vp, vp, vp, vp, vp, vp, vp, vp, sz, vp]),
         "snapb_bc_apply_f32": (i, [cp, vp, i, i, vp, sz, vp]),
         "snapb_max_time_step_f32": (i, [cp, vp, vp, vp, sz, vp]),
+        "snapb_adjoint_workspace_size": (sz, [cp]),
+        "snapb_stage_adjoint": (i, [cp, i, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, sz, vp]),
+        "snapb_hydro_forward_adjoint": (i, [cp, vp, vp, vp, vp, vp, sz, vp]),
+        "snapb_bc_adjoint": (i, [cp, vp, vp, i, i, vp]),
         "snapb_timing_enable": (i, [i]),
         "snapb_timing_query": (i, [i, ctypes.POINTER(d), ctypes.POINTER(i)]),
     }
@@ -75,11 +79,13 @@ def exported_symbols():
     """Names of the entry points this binding declares (all in snapb.h)."""
     return ["snapb_abi_version", "snapb_last_error", "snapb_workspace_size", "snapb_cons2prim",
             "snapb_prim2cons", "snapb_reconstruct", "snapb_riemann", "snapb_hydro_forward",
-            "snapb_implicit_correction", "snapb_implicit_correction_noalloc", "snapb_stage", "snapb_bc_apply", "snapb_max_time_step", "snapb_scale_dt",
+            "snapb_implicit_correction", "snapb_implicit_correction_noalloc", "snapb_stage",
+            "snapb_bc_apply", "snapb_max_time_step", "snapb_scale_dt",
             "snapb_check_positive", "snapb_timing_enable", "snapb_timing_query",
             "snapb_workspace_size_f32", "snapb_reference_f32", "snapb_to_perturbation",
             "snapb_from_perturbation", "snapb_stage_f32", "snapb_bc_apply_f32",
-            "snapb_max_time_step_f32"]
+            "snapb_max_time_step_f32", "snapb_adjoint_workspace_size", "snapb_stage_adjoint",
+            "snapb_hydro_forward_adjoint", "snapb_bc_adjoint"]
 
 
 KERNELS = {"x1_sweep": 0, "diffusion": 1, "x2_sweep": 2, "x3_sweep": 3, "finalize": 4,

@@ -15,6 +15,13 @@
 
 namespace snapb {
 
+// the double overloads stay visible next to the Dual ones below
+using ::fabs;
+using ::fmax;
+using ::fmin;
+using ::pow;
+using ::sqrt;
+
 struct Dual {
   double v, d;
   __host__ __device__ Dual() : v(0.), d(0.) {}
@@ -68,5 +75,11 @@ __device__ __forceinline__ Dual sqrt(const Dual& a) {
 }
 __device__ __forceinline__ Dual fabs(const Dual& a) { return a.v < 0. ? -a : a; }
 __device__ __forceinline__ Dual fmax(const Dual& a, const Dual& b) { return a.v >= b.v ? a : b; }
+__device__ __forceinline__ Dual fmin(const Dual& a, const Dual& b) { return a.v <= b.v ? a : b; }
+// x^e for a constant exponent (x > 0 wherever it is used: pressures, densities)
+__device__ __forceinline__ Dual pow(const Dual& x, double e) {
+  double y = ::pow(x.v, e);
+  return Dual(y, e * y / x.v * x.d);
+}
 
 }  // namespace snapb
