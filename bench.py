@@ -326,6 +326,90 @@ def run_fp32_form(args, opts, state, mb64, cells, stream, barrier, world):
             "e2e": {"value": e2e, "unit": UNIT}, "h2d": nbytes, "d2h": nbytes}
 
 
+def run_adjoint_timing(args, opts, state, cells, stream, barrier):
+    """FP64 adjoint cost on the same workload: one RK3 step forward vs the
+    reverse of that step (three stage reverses from the kept stage inputs),
+    and the checkpointed rollout's backward (segment re-run + reverses)."""
+    import torch
+
+    from snapy_linfel_b200 import _lib
+    from snapy_linfel_b200.adjoint import StepRunner, rollout
+    from snapy_linfel_b200.mesh import MeshBlock
+
+    w, r = state
+    mb = MeshBlock(opts, device="cuda")
+    mb.initialize(w, r)
+    dt = mb.max_time_step().clone()
+    u0 = mb.hydro_u.clone()
+    s0 = mb.scalar_s.clone() if opts.hydro.nscalar else None
+    del mb
+    runner = StepRunner(opts, device="cuda")
+    adj = runner.adjoint()
+    nsteps = max(1, min(args.steps, args.adj_steps))
+    runner.load(u0, s0)
+    for _ in range(2):  # warm-up
+        runner.step(dt)
+    runner.load(u0, s0)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(nsteps):
+        runner.step(dt)
+    e1.record(stream)
+    barrier()
+    fwd_ms = e0.elapsed_time(e1) / nsteps
+    runner.load(u0, s0)
+    kept = [runner.step(dt, keep=True) for _ in range(nsteps)]
+    g = torch.ones_like(u0) * 1e-3
+    gs = torch.ones_like(s0) * 1e-3 if s0 is not None else None
+    # warm-up reverse
+    gu0 = torch.zeros_like(g)
+    gs0 = torch.zeros_like(gs) if gs is not None else None
+    adj.stage(2, dt, kept[-1][2][0], kept[-1][2][1], g, gs, gu0, gs0)
+    barrier()
+    _lib.timing_enable(True)
+    e0.record(stream)
+    gg, ggs = g, gs
+    for n in reversed(range(nsteps)):
+        gu0 = torch.zeros_like(g)
+        gs0 = torch.zeros_like(gs) if gs is not None else None
+        for st in (2, 1, 0):
+            gg, ggs = adj.stage(st, dt, kept[n][st][0], kept[n][st][1], gg, ggs, gu0, gs0)
+        gg = gg + gu0
+        if ggs is not None:
+            ggs = ggs + gs0
+    e1.record(stream)
+    barrier()
+    rev_ms = e0.elapsed_time(e1) / nsteps
+    kern = {k: round(v[0] / v[1], 4) for k, v in _lib.timing_query().items()}
+    _lib.timing_enable(False)
+    del kept
+    # the checkpointed rollout: forward + backward through torch.autograd
+    x = u0.clone().requires_grad_(True)
+    dts = dt.repeat(nsteps)
+    barrier()
+    e0.record(stream)
+    uT, _ = rollout(opts, x, s0, dts, checkpoint_every=nsteps, runner=runner)
+    e1.record(stream)
+    barrier()
+    roll_fwd_ms = e0.elapsed_time(e1) / nsteps
+    e0.record(stream)
+    uT.backward(torch.ones_like(uT) * 1e-3)
+    e1.record(stream)
+    barrier()
+    roll_bwd_ms = e0.elapsed_time(e1) / nsteps
+    del x, uT, runner, adj
+    torch.cuda.empty_cache()
+    return {"steps": nsteps, "forward_ms_per_step": fwd_ms, "reverse_ms_per_step": rev_ms,
+            "adjoint_over_forward": rev_ms / fwd_ms,
+            "checkpointed": {"forward_ms_per_step": roll_fwd_ms,
+                             "backward_ms_per_step": roll_bwd_ms,
+                             "backward_over_forward": roll_bwd_ms / roll_fwd_ms,
+                             "checkpoint_every": nsteps},
+            "reverse_kernel_ms_per_stage": kern, "dtype": "f64",
+            "value": cells * 3 / (rev_ms / 1e3) / 1e6, "unit": "Mcell-updates/s (reverse)"}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -423,6 +507,11 @@ def run_ours(args):
             f32["ms"] = t.item()
         f32["value"] = world * cells * 3 * args.steps / (f32["ms"] / 1e3) / 1e6
 
+    adj = None
+    if not args.no_adjoint:
+        adj = run_adjoint_timing(args, opts, workload_state(args.workload), cells, stream,
+                                 barrier)
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         try:
@@ -472,6 +561,7 @@ def run_ours(args):
                                     "algorithmic_bytes_per_cell_update":
                                         algo_bytes_per_cell_update(cfg)},
             "kernel_ms_per_launch_fp64": kern_ms,
+            "adjoint": adj,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e if not isinstance(e2e, dict) else e2e["value"], "unit": UNIT,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
@@ -494,6 +584,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--acc-steps", type=int, default=5)
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adj-steps", type=int, default=2)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

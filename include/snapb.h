@@ -299,8 +299,9 @@ int snapb_bc_adjoint(const snapb_hydro_config* cfg, const double* g_in, double* 
                      int kind, void* stream);
 
 /* ---- diagnostics: per-kernel device time ----
- * While enabled, snapb_stage and snapb_hydro_forward record a CUDA event pair
- * around every kernel they launch.  snapb_timing_query synchronizes those
+ * While enabled, snapb_stage, snapb_hydro_forward, snapb_stage_f32 and the
+ * adjoint entry points record a CUDA event pair around every kernel (or
+ * kernel group) they launch.  snapb_timing_query synchronizes those
  * events and returns the summed device milliseconds and the launch count of
  * one kernel kind.  Enabling clears the record.  (Plays the role of the
  * reference's verbose phase timers, src/hydro/hydro_forward.cpp:26-31.) */
@@ -312,7 +313,12 @@ enum {
   SNAPB_K_FINAL = 4,
   SNAPB_K_VIC = 5,  /* implicit column solve */
   SNAPB_K_BC = 6,   /* boundary fills */
-  SNAPB_K_COUNT = 7
+  SNAPB_K_ADJ_COMBINE = 7,   /* adjoint: BC^T and RK weights */
+  SNAPB_K_ADJ_RECOMPUTE = 8, /* adjoint: forward recompute of w, r, du */
+  SNAPB_K_ADJ_VIC = 9,       /* adjoint: implicit solve reverse */
+  SNAPB_K_ADJ_X23 = 10,      /* adjoint: x2 / x3 face reverses */
+  SNAPB_K_ADJ_X1 = 11,       /* adjoint: x1 faces, gravity, U->W reverse */
+  SNAPB_K_COUNT = 12
 };
 int snapb_timing_enable(int on);
 int snapb_timing_query(int kernel, double* total_ms, int* launches);

@@ -89,7 +89,8 @@ def exported_symbols():
 
 
 KERNELS = {"x1_sweep": 0, "diffusion": 1, "x2_sweep": 2, "x3_sweep": 3, "finalize": 4,
-           "implicit_vic": 5, "boundary": 6}
+           "implicit_vic": 5, "boundary": 6, "adj_combine": 7, "adj_recompute": 8,
+           "adj_vic": 9, "adj_x2x3": 10, "adj_x1": 11}
 
 
 def timing_enable(on: bool = True):

@@ -1293,6 +1293,7 @@ static cudaError_t launch_sweeps_adj_ns(const Geo& g, const Phys& p, const AdjBu
   const int ni = g.iu - g.il + 1;
   for (int ax = 3; ax >= 2; --ax) {
     if ((ax == 3 && !a3) || (ax == 2 && !a2)) continue;
+    ScopedTimer tm(SNAPB_K_ADJ_X23, st);
     int nax = ax == 2 ? g.nx2 : g.nx3;
     int no = ax == 2 ? (g.ku - g.kl + 1) : (g.ju - g.jl + 1);
     int64_t lines = (int64_t)ni * no;
@@ -1310,6 +1311,7 @@ static cudaError_t launch_sweeps_adj_ns(const Geo& g, const Phys& p, const AdjBu
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
+  ScopedTimer tm(SNAPB_K_ADJ_X1, st);
   if (a1) {
     const int nv = 5 + NS;
     size_t per = (size_t)2 * nv * g.nc1 * sizeof(double);
@@ -1426,18 +1428,24 @@ int reverse_core(const snapb_hydro_config* c, const Geo& g, Phys p, const double
   b.write_du = 1;
   const bool a1 = g.nc1 > 1, a2 = g.nc2 > 1, a3 = g.nc3 > 1;
   const int last_axis = a3 ? 3 : (a2 ? 2 : 1);
-  cudaError_t e = a1 ? launch_x1(g, p, b, last_axis == 1, st) : launch_c2p_only(g, p, b, st);
-  if (e != cudaSuccess) return cuda_rc(e, who);
-  if (p.implicit_scheme != 0) {
-    if (a2 && (e = launch_march(2, g, p, b, !a1, last_axis == 2, st)) != cudaSuccess)
-      return cuda_rc(e, who);
-    if (a3 && (e = launch_march(3, g, p, b, !a1 && !a2, true, st)) != cudaSuccess)
-      return cuda_rc(e, who);
+  cudaError_t e;
+  {
+    ScopedTimer t(SNAPB_K_ADJ_RECOMPUTE, st);
+    e = a1 ? launch_x1(g, p, b, last_axis == 1, st) : launch_c2p_only(g, p, b, st);
+    if (e != cudaSuccess) return cuda_rc(e, who);
+    if (p.implicit_scheme != 0) {
+      if (a2 && (e = launch_march(2, g, p, b, !a1, last_axis == 2, st)) != cudaSuccess)
+        return cuda_rc(e, who);
+      if (a3 && (e = launch_march(3, g, p, b, !a1 && !a2, true, st)) != cudaSuccess)
+        return cuda_rc(e, who);
+    }
+    e = cudaMemsetAsync(ab.GW, 0, (size_t)(5 + p.nscalar) * g.sv * sizeof(double), st);
+    if (e != cudaSuccess) return cuda_rc(e, who);
   }
-  e = cudaMemsetAsync(ab.GW, 0, (size_t)(5 + p.nscalar) * g.sv * sizeof(double), st);
-  if (e != cudaSuccess) return cuda_rc(e, who);
-  if (p.implicit_scheme != 0 && (e = launch_vic_adj(g, p, ab, st)) != cudaSuccess)
-    return cuda_rc(e, who);
+  if (p.implicit_scheme != 0) {
+    ScopedTimer t(SNAPB_K_ADJ_VIC, st);
+    if ((e = launch_vic_adj(g, p, ab, st)) != cudaSuccess) return cuda_rc(e, who);
+  }
   if ((e = launch_sweeps_adj(g, p, ab, st)) != cudaSuccess) return cuda_rc(e, who);
   return SNAPB_OK;
 }
@@ -1493,8 +1501,12 @@ int snapb_stage_adjoint(const snapb_hydro_config* cfg, int stage, const double* 
   rk3_weights(stage, ca.w0, ca.w1, ca.w2);
   ca.ns = cfg->nscalar;
   axes(g, *cfg, ca.a1, ca.a2, ca.a3);
-  k_adj_combine<<<(unsigned)((g.sv + 255) / 256), 256, 0, st>>>(g, ca);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e;
+  {
+    ScopedTimer t(SNAPB_K_ADJ_COMBINE, st);
+    k_adj_combine<<<(unsigned)((g.sv + 255) / 256), 256, 0, st>>>(g, ca);
+    e = cudaGetLastError();
+  }
   if (e != cudaSuccess) return cuda_rc(e, "stage_adjoint combine");
   return reverse_core(cfg, g, p, dt, u, s, ab, st, "stage_adjoint");
 }

@@ -95,22 +95,7 @@ struct TimedLaunch {
 bool g_timing = false;
 std::vector<TimedLaunch> g_launches;
 
-struct KernelTimer {
-  int kind;
-  cudaStream_t st;
-  cudaEvent_t a = nullptr, b = nullptr;
-  KernelTimer(int k, cudaStream_t s) : kind(k), st(s) {
-    if (!g_timing) return;
-    cudaEventCreate(&a);
-    cudaEventCreate(&b);
-    cudaEventRecord(a, st);
-  }
-  ~KernelTimer() {
-    if (!g_timing || !a) return;
-    cudaEventRecord(b, st);
-    g_launches.push_back({kind, a, b});
-  }
-};
+using KernelTimer = snapb::ScopedTimer;
 
 void clear_timings() {
   for (auto& l : g_launches) {
@@ -222,6 +207,17 @@ int run_stage(const snapb_hydro_config* c, int stage, const double* dt, double* 
 }  // namespace
 
 namespace snapb {
+ScopedTimer::ScopedTimer(int k, cudaStream_t s) : kind(k), st(s) {
+  if (!g_timing) return;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  cudaEventRecord(a, st);
+}
+ScopedTimer::~ScopedTimer() {
+  if (!g_timing || !a) return;
+  cudaEventRecord(b, st);
+  g_launches.push_back({kind, a, b});
+}
 const char* internal_check_config(const snapb_hydro_config* c) { return check_config(c); }
 int internal_fail(int code, const std::string& msg) { return fail(code, msg); }
 }  // namespace snapb

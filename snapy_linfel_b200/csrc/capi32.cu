@@ -177,20 +177,28 @@ int snapb_stage_f32(const snapb_hydro_config* cfg, int stage, const double* dt, 
   cudaStream_t st = (cudaStream_t)stream;
   const bool a2 = g.nc2 > 1, a3 = g.nc3 > 1;
   int last = a3 ? 3 : (a2 ? 2 : 1);
-  cudaError_t e = launch_x1_32(g, p, b, last == 1, st);
+  cudaError_t e;
+  {
+    ScopedTimer t(SNAPB_K_X1, st);
+    e = launch_x1_32(g, p, b, last == 1, st);
+  }
   if (e != cudaSuccess) return cuda32(e, "stage_f32 x1");
   if (a2) {
+    ScopedTimer t(SNAPB_K_X2, st);
     e = launch_march32(2, g, p, b, false, last == 2, st);
     if (e != cudaSuccess) return cuda32(e, "stage_f32 x2");
   }
   if (a3) {
+    ScopedTimer t(SNAPB_K_X3, st);
     e = launch_march32(3, g, p, b, false, true, st);
     if (e != cudaSuccess) return cuda32(e, "stage_f32 x3");
   }
   if (p.implicit_scheme) {
+    ScopedTimer t(SNAPB_K_VIC, st);
     e = launch_vic32(g, p, b, st);
     if (e != cudaSuccess) return cuda32(e, "stage_f32 implicit");
   }
+  ScopedTimer t(SNAPB_K_BC, st);
   e = launch_bc32(g, *cfg, u, cfg->nvar, SNAPB_CONSERVED, b.rb, b.pb, st);
   if (e == cudaSuccess && p.nscalar > 0)
     e = launch_bc32(g, *cfg, s, p.nscalar, SNAPB_SCALAR, b.rb, b.pb, st);

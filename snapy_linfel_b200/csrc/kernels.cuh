@@ -100,6 +100,18 @@ cudaError_t launch_riemann(const Geo& g, const Phys& p, int solver, int dim, con
                            const double* wr, int nv, double* flx, double* fp, const double* vel,
                            cudaStream_t st);
 
+// CUDA-event pair around a kernel sequence while snapb_timing_enable is on
+// (kind: a SNAPB_K_* value); defined in capi.cu
+struct ScopedTimer {
+  int kind;
+  cudaStream_t st;
+  cudaEvent_t a = nullptr, b = nullptr;
+  ScopedTimer(int k, cudaStream_t s);
+  ~ScopedTimer();
+  ScopedTimer(const ScopedTimer&) = delete;
+  ScopedTimer& operator=(const ScopedTimer&) = delete;
+};
+
 // argument validation and last-error reporting shared with entry points that
 // live outside capi.cu
 const char* internal_check_config(const snapb_hydro_config* c);
