@@ -257,6 +257,52 @@ int snapb_max_time_step_f32(const snapb_hydro_config* cfg, const float* w,
                             double* dt_out, void* workspace,
                             size_t workspace_bytes, void* stream);
 
+/* ---- batched ensembles (FP32 perturbation form) ----
+ * No counterpart in the reference, which advances one MeshBlock per call:
+ * many independent blocks of uneven sizes (same physics, same active axes)
+ * advance together.  Each sweep of a stage is one persistent launch over all
+ * members whose CTAs pull (member, tile) work items from a device counter.
+ * Each member's state is the FP32 perturbation form of snapb_stage_f32, with
+ * its own FP32 workspace on which snapb_reference_f32 has run.  The plan
+ * (host object) is created once, then bound to a device workspace of
+ * snapb_ensemble_workspace_size bytes; every call is stream ordered and
+ * graph-capturable (dt per member stays on the device).  Diffusion and
+ * non_hydrostatic < 1 are not batched. */
+typedef struct snapb_member_f32 {
+  snapb_hydro_config cfg;
+  float *u, *u0, *w, *s, *s0, *r; /* as snapb_stage_f32 */
+  void* workspace;                /* the member's FP32 workspace */
+  size_t workspace_bytes;
+} snapb_member_f32;
+
+/* tile shapes; 0 = default.  x1_columns: columns per x1 tile; march_segment:
+ * faces per x2/x3 segment; ctas_per_sm: persistent CTAs per SM; vic_block:
+ * columns per implicit-column tile (32, 64 or 128). */
+typedef struct snapb_ensemble_tuning {
+  int32_t x1_columns, march_segment, ctas_per_sm, vic_block;
+} snapb_ensemble_tuning;
+
+typedef struct snapb_ensemble snapb_ensemble; /* opaque host-side plan */
+
+int snapb_ensemble_create(const snapb_member_f32* members, int n,
+                          const snapb_ensemble_tuning* tune, snapb_ensemble** out);
+size_t snapb_ensemble_workspace_size(const snapb_ensemble* e);
+/* copies the member descriptors and work-queue tables into the workspace */
+int snapb_ensemble_bind(snapb_ensemble* e, void* workspace, size_t workspace_bytes,
+                        void* stream);
+/* re-plans with new tile shapes (within the bound workspace) and re-uploads */
+int snapb_ensemble_set_tuning(snapb_ensemble* e, const snapb_ensemble_tuning* tune,
+                              void* stream);
+/* device array [n]: the members' dt, written by snapb_ensemble_max_time_step_f32
+ * (or by the caller) and read by every stage */
+const double* snapb_ensemble_dt(const snapb_ensemble* e);
+/* dt_m = factor * CFL limit of member m's w (factor = cfl * 2^-redo) */
+int snapb_ensemble_max_time_step_f32(snapb_ensemble* e, double factor, void* stream);
+/* one RK stage of every member: x1, x2, x3 sweeps, implicit solve, boundary
+ * fills, each one persistent launch */
+int snapb_ensemble_stage_f32(snapb_ensemble* e, int stage, void* stream);
+void snapb_ensemble_destroy(snapb_ensemble* e);
+
 /* ---- adjoint (reverse mode) of the FP64 stage ----
  * No counterpart in the reference, which has no adjoint: these are the
  * `*_adjoint` entry points of the hydro step.  dt is a constant of the

@@ -122,6 +122,11 @@ int cuda32(cudaError_t e, const char* where) {
 
 }  // namespace
 
+namespace snapb {
+StageBufs32 bufs32_of(const snapb_hydro_config& c, void* ws) { return bufs32(c, ws); }
+size_t workspace_size_f32_of(const snapb_hydro_config& c) { return layout32(c).total; }
+}  // namespace snapb
+
 extern "C" {
 
 size_t snapb_workspace_size_f32(const snapb_hydro_config* cfg) {

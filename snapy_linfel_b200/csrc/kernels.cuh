@@ -59,6 +59,71 @@ struct StageBufs32 {
   int vic_du_only;
 };
 
+// ---------------------------------------------------------------------------
+// Batched ensembles: many independent blocks of uneven sizes advanced by one
+// persistent launch per sweep, each CTA pulling (member, tile) work items from
+// a device counter.
+// ---------------------------------------------------------------------------
+
+// One ensemble member (FP32 perturbation form), resident in device memory.
+// The stage-dependent fields of b (stage, weights) are set by each launch.
+struct Member32 {
+  Geo g;
+  StageBufs32 b;
+  int bc[6];
+  int x1_cols;           // columns per x1 tile
+  int seglen2, nseg2;    // x2 march: faces per segment, segments
+  int seglen3, nseg3;    // x3 march
+  int vic_cols;          // columns per implicit-column tile
+  int pad;
+};
+
+// Work items of one persistent launch: item k belongs to member m when
+// prefix[m] <= k < prefix[m + 1]; `counter` is zero when the launch starts.
+struct WorkQueue {
+  const int64_t* prefix;  // [M + 1]
+  int M;
+  unsigned long long* counter;
+};
+
+// Next (member, tile) for the whole CTA; false when the queue is drained.
+// Every thread of the CTA must call it.
+__device__ __forceinline__ bool queue_next(const WorkQueue& q, int& m, int64_t& tile) {
+  __shared__ unsigned long long s_item;
+  __syncthreads();
+  if (threadIdx.x == 0) s_item = atomicAdd(q.counter, 1ULL);
+  __syncthreads();
+  const int64_t item = (int64_t)s_item;
+  if (item >= q.prefix[q.M]) return false;
+  int lo = 0, hi = q.M - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (q.prefix[mid] <= item) lo = mid;
+    else hi = mid - 1;
+  }
+  m = lo;
+  tile = item - q.prefix[lo];
+  return true;
+}
+
+// persistent launchers of the batched FP32 stage (grid = persistent CTAs)
+cudaError_t launch_x1_32_batch(const Member32* mem, const Phys& p, const WorkQueue& q,
+                               int stage, bool last, int grid, size_t smem, cudaStream_t st);
+cudaError_t launch_march32_batch(int axis, const Member32* mem, const Phys& p,
+                                 const WorkQueue& q, int stage, bool first, bool last, int grid,
+                                 cudaStream_t st);
+cudaError_t launch_vic_column_batch(const Member32* mem, const Phys& p, const WorkQueue& q,
+                                    int stage, int grid, int block, cudaStream_t st);
+cudaError_t launch_vic_finish_batch(const Member32* mem, const Phys& p, const WorkQueue& q,
+                                    int stage, int grid, cudaStream_t st);
+cudaError_t launch_bc32_batch(const Member32* mem, const Phys& p, const WorkQueue& q, int kind,
+                              double igm1, int grid, cudaStream_t st);
+size_t x1_smem32_per_column(const Geo& g, int nvt);
+StageBufs32 bufs32_of(const snapb_hydro_config& c, void* ws);
+size_t workspace_size_f32_of(const snapb_hydro_config& c);
+constexpr int kVicFinishCols = 32;    // columns per implicit-finish tile
+constexpr int kVicFinishLayers = 32;  // layers per implicit-finish tile
+
 // RK3 (Shu-Osher) stage weights: u = wgt0*u0 + wgt1*u + wgt2*du
 inline void rk3_weights(int stage, double& a, double& b, double& c) {
   static const double W[3][3] = {{1., 0., 1.}, {3. / 4., 1. / 4., 1. / 4.},

@@ -157,15 +157,16 @@ size_t x1_smem32_per_column(const Geo& g, int nvt) {
   return (size_t)(2 * nvt) * g.nc1 * sizeof(float);
 }
 
+// One tile: columns col0 .. col0+C-1 of the block, smf = 2 * NV * nc1 * C floats.
+// Every thread of the CTA calls it (it synchronises the CTA).
 template <int NS>
-__global__ void __launch_bounds__(256) k_x1_32(Geo g, Phys p, StageBufs32 b, int C, int last) {
+__device__ __forceinline__ void x1_32_tile(const Geo& g, const Phys& p, const StageBufs32& b,
+                                           int C, int last, int64_t col0, float* smf) {
   constexpr int NV = 5 + NS;
-  extern __shared__ float smf[];
   const int nc1 = g.nc1;
   float* sw = smf;
   float* sf = sw + (size_t)C * NV * nc1;
   const int64_t ncol = (int64_t)g.nc2 * g.nc3;
-  const int64_t col0 = (int64_t)blockIdx.x * C;
   const int tid = threadIdx.x, nt = blockDim.x;
   const int64_t sv = g.sv;
   const float gm1 = (float)(p.gammad - 1.);
@@ -320,12 +321,21 @@ __global__ void __launch_bounds__(256) k_x1_32(Geo g, Phys p, StageBufs32 b, int
   }
 }
 
+template <int NS>
+__global__ void __launch_bounds__(256) k_x1_32(Geo g, Phys p, StageBufs32 b, int C, int last) {
+  extern __shared__ float smf[];
+  x1_32_tile<NS>(g, p, b, C, last, (int64_t)blockIdx.x * C, smf);
+}
+
 // ---------------------------------------------------------------------------
 // x2 / x3 marching sweeps (reference constant along the sweep)
 // ---------------------------------------------------------------------------
+// One thread's work: line tid (x1 cell x other horizontal index) and face
+// segment seg of the sweep axis.
 template <int NS, int AX>
-__global__ void __launch_bounds__(128) k_march32(Geo g, Phys p, StageBufs32 b, int seglen,
-                                                 int first, int last) {
+__device__ __forceinline__ void march32_line(const Geo& g, const Phys& p, const StageBufs32& b,
+                                             int seglen, int first, int last, int64_t tid,
+                                             int seg) {
   constexpr int NV = 5 + NS;
   const int ni = g.iu - g.il + 1;
   int lo, hi, olo, ohi;
@@ -336,11 +346,10 @@ __global__ void __launch_bounds__(128) k_march32(Geo g, Phys p, StageBufs32 b, i
     lo = g.kl, hi = g.ku, st = g.s3, olo = g.jl, ohi = g.ju, ost = g.s2;
   }
   const int no = ohi - olo + 1;
-  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (tid >= (int64_t)ni * no) return;
   const int i = g.il + (int)(tid % ni);
   const int o = olo + (int)(tid / ni);
-  const int f0 = lo + blockIdx.y * seglen;
+  const int f0 = lo + seg * seglen;
   if (f0 > hi) return;
   const int f1 = min(f0 + seglen, hi + 1);
   const int64_t base = i + o * ost;
@@ -419,6 +428,13 @@ __global__ void __launch_bounds__(128) k_march32(Geo g, Phys p, StageBufs32 b, i
   }
 }
 
+template <int NS, int AX>
+__global__ void __launch_bounds__(128) k_march32(Geo g, Phys p, StageBufs32 b, int seglen,
+                                                 int first, int last) {
+  march32_line<NS, AX>(g, p, b, seglen, first, last,
+                       (int64_t)blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y);
+}
+
 // ---------------------------------------------------------------------------
 // boundary fills of perturbation arrays: as k_bc, plus the x1 offset of the
 // reference between the source and the ghost layer (rho, and E or p)
@@ -449,10 +465,10 @@ __device__ __forceinline__ int bc_map32(const AxisBC32& a, int i, bool& flip) {
   return i;
 }
 
-__global__ void k_bc32(int nc1, int nc2, int nc3, int64_t sv, AxisBC32 a1, AxisBC32 a2,
-                       AxisBC32 a3, float* var, int nv, int kind, const double* rb,
-                       const double* pb, double igm1) {
-  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void bc32_cell(int nc1, int nc2, int nc3, int64_t sv, AxisBC32 a1,
+                                          AxisBC32 a2, AxisBC32 a3, float* var, int nv,
+                                          int kind, const double* rb, const double* pb,
+                                          double igm1, int64_t t) {
   if (t >= sv) return;
   int i = (int)(t % nc1);
   int j = (int)((t / nc1) % nc2);
@@ -471,6 +487,13 @@ __global__ void k_bc32(int nc1, int nc2, int nc3, int64_t sv, AxisBC32 a1, AxisB
     }
     var[v * sv + t] = (float)x;
   }
+}
+
+__global__ void k_bc32(int nc1, int nc2, int nc3, int64_t sv, AxisBC32 a1, AxisBC32 a2,
+                       AxisBC32 a3, float* var, int nv, int kind, const double* rb,
+                       const double* pb, double igm1) {
+  bc32_cell(nc1, nc2, nc3, sv, a1, a2, a3, var, nv, kind, rb, pb, igm1,
+            (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // conversions between the FP64 state and the FP32 perturbation
@@ -549,6 +572,120 @@ __global__ void k_cfl32(Geo g, double gammad, int use1, int use2, int use3, cons
       atomicMin(&slots[2], (unsigned long long)__double_as_longlong(m3));
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// persistent batched kernels: every CTA pulls (member, tile) items
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void set_stage32(StageBufs32& b, int stage) {
+  double w0 = 1., w1 = 0., w2 = 1.;
+  if (stage == 1) w0 = 3. / 4., w1 = 1. / 4., w2 = 1. / 4.;
+  if (stage == 2) w0 = 1. / 3., w1 = 2. / 3., w2 = 2. / 3.;
+  b.stage = stage;
+  b.wgt0 = w0;
+  b.wgt1 = w1;
+  b.wgt2 = w2;
+}
+
+template <int NS>
+__global__ void __launch_bounds__(256) k_x1_32_batch(const Member32* __restrict__ mem, Phys p,
+                                                     WorkQueue q, int stage, int last) {
+  extern __shared__ float smf[];
+  int m;
+  int64_t tile;
+  while (queue_next(q, m, tile)) {
+    const Geo g = mem[m].g;
+    StageBufs32 b = mem[m].b;
+    set_stage32(b, stage);
+    const int C = mem[m].x1_cols;
+    x1_32_tile<NS>(g, p, b, C, last, tile * C, smf);
+  }
+}
+
+template <int NS, int AX>
+__global__ void __launch_bounds__(128) k_march32_batch(const Member32* __restrict__ mem, Phys p,
+                                                       WorkQueue q, int stage, int first,
+                                                       int last) {
+  int m;
+  int64_t tile;
+  while (queue_next(q, m, tile)) {
+    const Geo g = mem[m].g;
+    StageBufs32 b = mem[m].b;
+    set_stage32(b, stage);
+    const int seglen = AX == 2 ? mem[m].seglen2 : mem[m].seglen3;
+    const int nseg = AX == 2 ? mem[m].nseg2 : mem[m].nseg3;
+    const int64_t blk = tile / nseg;
+    const int seg = (int)(tile - blk * nseg);
+    march32_line<NS, AX>(g, p, b, seglen, first, last, blk * blockDim.x + threadIdx.x, seg);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_bc32_batch(const Member32* __restrict__ mem, Phys p,
+                                                    WorkQueue q, int kind, double igm1) {
+  int m;
+  int64_t tile;
+  while (queue_next(q, m, tile)) {
+    const Geo& g = mem[m].g;
+    const Member32& mb = mem[m];
+    AxisBC32 a1{g.nc1, g.ng, mb.bc[0], mb.bc[1]};
+    AxisBC32 a2{g.nc2, g.ng, mb.bc[2], mb.bc[3]};
+    AxisBC32 a3{g.nc3, g.ng, mb.bc[4], mb.bc[5]};
+    float* var = kind == SNAPB_SCALAR ? mb.b.s : mb.b.u;
+    int nv = kind == SNAPB_SCALAR ? p.nscalar : 5;
+    bc32_cell(g.nc1, g.nc2, g.nc3, g.sv, a1, a2, a3, var, nv, kind, mb.b.rb, mb.b.pb, igm1,
+              tile * blockDim.x + threadIdx.x);
+  }
+}
+
+cudaError_t launch_x1_32_batch(const Member32* mem, const Phys& p, const WorkQueue& q,
+                               int stage, bool last, int grid, size_t smem, cudaStream_t st) {
+#define SNAPB_X1B(NS)                                                                         \
+  case NS: {                                                                                  \
+    static bool attr = false;                                                                 \
+    if (!attr) {                                                                              \
+      cudaFuncSetAttribute(k_x1_32_batch<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+                           200 * 1024);                                                       \
+      attr = true;                                                                            \
+    }                                                                                         \
+    k_x1_32_batch<NS><<<grid, 256, smem, st>>>(mem, p, q, stage, last ? 1 : 0);               \
+    break;                                                                                    \
+  }
+  switch (p.nscalar) {
+    SNAPB_X1B(0)
+    SNAPB_X1B(1)
+    SNAPB_X1B(2)
+    SNAPB_X1B(3)
+    default: return cudaErrorInvalidValue;
+  }
+#undef SNAPB_X1B
+  return cudaGetLastError();
+}
+
+cudaError_t launch_march32_batch(int axis, const Member32* mem, const Phys& p,
+                                 const WorkQueue& q, int stage, bool first, bool last, int grid,
+                                 cudaStream_t st) {
+#define SNAPB_MB(NS)                                                                         \
+  case NS:                                                                                   \
+    if (axis == 2)                                                                           \
+      k_march32_batch<NS, 2><<<grid, 128, 0, st>>>(mem, p, q, stage, first, last);           \
+    else                                                                                     \
+      k_march32_batch<NS, 3><<<grid, 128, 0, st>>>(mem, p, q, stage, first, last);           \
+    break;
+  switch (p.nscalar) {
+    SNAPB_MB(0)
+    SNAPB_MB(1)
+    SNAPB_MB(2)
+    SNAPB_MB(3)
+    default: return cudaErrorInvalidValue;
+  }
+#undef SNAPB_MB
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bc32_batch(const Member32* mem, const Phys& p, const WorkQueue& q, int kind,
+                              double igm1, int grid, cudaStream_t st) {
+  k_bc32_batch<<<grid, 256, 0, st>>>(mem, p, q, kind, igm1);
+  return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------

@@ -1,14 +1,15 @@
 // vic.cu — vertically implicit correction (VIC) of one RK stage, FP64.
 //
-// Three kernels per solve:
-//   k_vic_assemble  every (column, interface) in parallel: the Roe-averaged
-//                   |A| = R |Lambda| R^-1 once per interface (the reference
-//                   forms it twice, once per neighbouring cell) and the flux
-//                   Jacobian once per cell, staged through shared memory;
-//   k_vic_sweep     one thread per x1 column (x1 is the vertical axis): the
-//                   block-Thomas elimination with nothing but small block
-//                   algebra in its sequential chain, back substitution and
-//                   the MS-VIC column sums;
+// Two kernels per solve:
+//   k_vic_column    one thread per x1 column (x1 is the vertical axis): the
+//                   blocks are formed on the fly while the column is swept —
+//                   the Roe-averaged |A| = R |Lambda| R^-1 once per interface
+//                   (the reference forms it twice, once per neighbouring cell)
+//                   and the flux Jacobian once per cell, a layer ahead of the
+//                   elimination that consumes them — then the block-Thomas
+//                   elimination, back substitution and the MS-VIC column
+//                   sums.  Only the reduced blocks and the partial solutions
+//                   go through HBM;
 //   k_vic_finish    per cell: mass redistribution, scalar mass fix and the RK
 //                   combination (or du), with delta transposed through shared
 //                   memory.
@@ -34,16 +35,12 @@ namespace snapb {
 // ---------------------------------------------------------------------------
 // Scratch layout (doubles, column index fastest so that the threads of a warp,
 // one column each, read consecutive addresses):
-//   T [nl+2][E1][ncol]   per index t: |A| at the face between cells t-1 and t
-//                        (N*N), the flux Jacobian of cell t-1 (N*N), the
-//                        explicit du rows of cell t (N) and rho of cell t (1)
 //   S [nl][N*N+N][ncol]  the reduced blocks a'_i then the partial solutions
 //                        delta_i (back-substituted in place)
 //   Z [2][ncol]          per-column sums: sum (rho V)^2 and B_dry
 // ---------------------------------------------------------------------------
 template <int N>
 struct VicDims {
-  static constexpr int E1 = 2 * N * N + N + 1;
   static constexpr int ES = N * N + N;
 };
 
@@ -54,13 +51,12 @@ size_t vic_scratch_bytes(const Geo& g, const Phys& p) {
   int N = vic_n(p);
   int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
   int64_t nl = g.nx1;
-  int64_t e1 = 2 * N * N + N + 1, es = N * N + N;
-  return (size_t)((nl + 2) * e1 * ncol + nl * es * ncol + 2 * ncol) * sizeof(double);
+  int64_t es = N * N + N;
+  return (size_t)(nl * es * ncol + 2 * ncol) * sizeof(double);
 }
 
 constexpr int kTC = 32;  // columns per tile
 constexpr int kTL = 32;  // layers per tile (redistribution)
-constexpr int kTLA = 16;  // layers per tile (assembly; static shared memory <= 48 KB)
 
 // (k, j, il) offset of interior column `col`
 __device__ __forceinline__ int64_t column_base(const Geo& g, int64_t col) {
@@ -130,114 +126,46 @@ __device__ __forceinline__ double vic_full_rho(const StageBufs32& b, double u_rh
   return u_rho + b.rb[xi];
 }
 
-// (1) assembly: every (column, t) in parallel.  The tile's cells are staged
-// through shared memory with loads along x1 (coalesced), the entries are
-// written with the column index fastest (coalesced).
+// (1) one thread per column: blocks formed a layer ahead of the
+// block-Thomas elimination, back substitution and the column sums.  Loads of
+// a layer's w and du go 32 columns apart across a warp; the next layers of
+// each column sit in the same 32-byte sectors, which stay in L1.
 template <int N, class B>
-__global__ void __launch_bounds__(256) k_vic_assemble(Geo g, Phys p, B b) {
-  constexpr int E1 = VicDims<N>::E1;
-  const int nl = g.nx1;
+__device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B& b, int64_t col) {
+  constexpr int ES = VicDims<N>::ES;
   const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
-  const int64_t col0 = (int64_t)blockIdx.x * kTC;
-  const int t0 = blockIdx.y * kTLA;
-  const int64_t sv = g.sv;
-  __shared__ double ws[5][kTC][kTLA + 2];   // cells t0-1 .. t0+kTLA-1
-  __shared__ double ds[N][kTC][kTLA + 1];   // du rows of cells t0 .. t0+kTLA-1
-  const int tid = threadIdx.x;
-  for (int idx = tid; idx < 5 * kTC * (kTLA + 1); idx += blockDim.x) {
-    int s = idx % (kTLA + 1), rest = idx / (kTLA + 1);
-    int c = rest % kTC, v = rest / kTC;
-    int cell = t0 - 1 + s;  // relative to il; valid range [-1, nl]
-    int64_t col = col0 + c;
-    double x = 0.;
-    if (col < ncol && cell >= -1 && cell <= nl)
-      x = vic_w(b, sv, v, column_base(g, col) + cell, g.il + cell);
-    ws[v][c][s] = x;
-  }
-  for (int idx = tid; idx < N * kTC * kTLA; idx += blockDim.x) {
-    int s = idx % kTLA, rest = idx / kTLA;
-    int c = rest % kTC, r = rest / kTC;
-    int cell = t0 + s;
-    int64_t col = col0 + c;
-    double x = 0.;
-    if (col < ncol && cell < nl) x = vic_d(b, sel<N>(r) * sv + column_base(g, col) + cell);
-    ds[r][c][s] = x;
-  }
-  __syncthreads();
-  const double gm1c = p.gammad - 1.;
-  const double gm1f = 0.5 * (p.gammad + p.gammad) - 1.;
-  double* T = b.vic;
-  for (int idx = tid; idx < kTC * kTLA; idx += blockDim.x) {
-    int c = idx % kTC, s = idx / kTC;
-    int t = t0 + s;
-    int64_t col = col0 + c;
-    if (col >= ncol || t > nl + 1) continue;
-    double wl[5], wr[5];
-#pragma unroll
-    for (int v = 0; v < 5; ++v) {
-      wl[v] = ws[v][c][s];      // cell t-1
-      wr[v] = ws[v][c][s + 1];  // cell t
-    }
-    double* out = T + (int64_t)t * E1 * ncol + col;
-    double A[N][N], J[N][N];
-    if (t <= nl) {
-      absA_block<N>(gm1f, wl, wr, A);
-    } else {
-#pragma unroll
-      for (int r = 0; r < N; ++r)
-#pragma unroll
-        for (int q = 0; q < N; ++q) A[r][q] = 0.;
-    }
-    jac_block<N>(gm1c, wl, J);
-#pragma unroll
-    for (int r = 0; r < N; ++r)
-#pragma unroll
-      for (int q = 0; q < N; ++q) {
-        out[(r * N + q) * ncol] = A[r][q];
-        out[(N * N + r * N + q) * ncol] = J[r][q];
-      }
-#pragma unroll
-    for (int r = 0; r < N; ++r) out[(2 * N * N + r) * ncol] = t < nl ? ds[r][c][s] : 0.;
-    out[(2 * N * N + N) * ncol] = t < nl ? wr[IDN] : 0.;
-  }
-}
-
-// (2) block-Thomas sweep, one thread per column, every access coalesced.
-template <int N, class B>
-__global__ void __launch_bounds__(128) k_vic_sweep(Geo g, Phys p, B b) {
-  constexpr int E1 = VicDims<N>::E1, ES = VicDims<N>::ES;
-  const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
-  const int64_t col = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= ncol) return;
   const int nl = g.nx1;
-  const double* T = b.vic + col;
-  double* S = b.vic + (int64_t)(nl + 2) * E1 * ncol + col;
+  const int64_t sv = g.sv;
+  const int64_t cb = column_base(g, col);
+  double* S = b.vic + col;
   double* Z = S + (int64_t)nl * ES * ncol;
-  auto Tat = [&](int t, int e) { return T[((int64_t)t * E1 + e) * ncol]; };
   auto Sat = [&](int i, int e) -> double& { return S[((int64_t)i * ES + e) * ncol]; };
-
+  auto load_w = [&](int i, double* w) {
+#pragma unroll
+    for (int v = 0; v < 5; ++v) w[v] = vic_w(b, sv, v, cb + i, g.il + i);
+  };
+  const double gm1c = p.gammad - 1.;
+  const double gm1f = 0.5 * (p.gammad + p.gammad) - 1.;
   const double dt = *b.dt;
-  const double Aa = g.A1, hiv = 0.5 / g.vol, idt = 1. / dt, grav = p.grav1;
+  const double Aa = g.A1, hiv = 0.5 / g.vol, idt = 1. / dt, grav = p.grav1, V = g.vol;
+  double wc[5], wn[5];
   double Am[N][N], Jp[N][N], Jc[N][N], ap[N][N], dp[N];
-#pragma unroll
-  for (int r = 0; r < N; ++r)
-#pragma unroll
-    for (int q = 0; q < N; ++q) {
-      Am[r][q] = Tat(0, r * N + q);
-      Jp[r][q] = Tat(0, N * N + r * N + q);  // cell -1
-      Jc[r][q] = Tat(1, N * N + r * N + q);  // cell 0
-    }
+  load_w(-1, wn);
+  jac_block<N>(gm1c, wn, Jp);
+  load_w(0, wc);
+  absA_block<N>(gm1f, wn, wc, Am);
+  jac_block<N>(gm1c, wc, Jc);
+  double sum_a2 = 0.;
   for (int i = 0; i < nl; ++i) {
+    load_w(i + 1, wn);  // the ghost cell nl at the top
     double Ap[N][N], Jn[N][N], rhs[N];
+    absA_block<N>(gm1f, wc, wn, Ap);
+    jac_block<N>(gm1c, wn, Jn);
 #pragma unroll
-    for (int r = 0; r < N; ++r) {
-      rhs[r] = Tat(i, 2 * N * N + r) / dt;
-#pragma unroll
-      for (int q = 0; q < N; ++q) {
-        Ap[r][q] = Tat(i + 1, r * N + q);
-        Jn[r][q] = Tat(i + 2, N * N + r * N + q);  // cell i+1
-      }
-    }
+    for (int r = 0; r < N; ++r) rhs[r] = vic_d(b, sel<N>(r) * sv + cb + i) / dt;
+    double ai = wc[IDN] * V;
+    sum_a2 += ai * ai;
     double a[N][N], bb[N][N], c[N][N];
 #pragma unroll
     for (int r = 0; r < N; ++r)
@@ -299,11 +227,14 @@ __global__ void __launch_bounds__(128) k_vic_sweep(Geo g, Phys p, B b) {
         Jp[r][q] = Jc[r][q];
         Jc[r][q] = Jn[r][q];
       }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) wc[v] = wn[v];
   }
-  // back substitution: delta_i -= a'_i delta_{i+1}
+  // back substitution: delta_i -= a'_i delta_{i+1}; B_dry accumulated on the way
   double dn[N];
 #pragma unroll
   for (int r = 0; r < N; ++r) dn[r] = dp[r];
+  double b_dry = (vic_d(b, IDN * sv + cb + nl - 1) - dn[0]) * 1. * V;
   for (int i = nl - 2; i >= 0; --i) {
     double d[N];
 #pragma unroll
@@ -318,30 +249,29 @@ __global__ void __launch_bounds__(128) k_vic_sweep(Geo g, Phys p, B b) {
       dn[r] = d[r];
       Sat(i, N * N + r) = d[r];
     }
-  }
-  // column sums in ascending layer order (vic_backward_reduce)
-  double sum_a2 = 0., b_dry = 0.;
-  for (int i = 0; i < nl; ++i) {
-    double ai = Tat(i, 2 * N * N + N) * g.vol;
-    sum_a2 += ai * ai;
-    b_dry += (Tat(i, 2 * N * N) - Sat(i, N * N)) * 1. * g.vol;
+    b_dry += (vic_d(b, IDN * sv + cb + i) - d[0]) * 1. * V;
   }
   Z[0] = sum_a2;
   Z[ncol] = b_dry;
 }
 
+template <int N, class B>
+__global__ void __launch_bounds__(128) k_vic_column(Geo g, Phys p, B b) {
+  vic_column<N, B>(g, p, b, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 // (3) redistribution + RK combination (or du), tiles of 32 columns x 32
 // layers: delta is transposed through shared memory so that the state
 // arrays are read and written along x1.
+// one tile: columns col0 .. col0+kTC-1, layers i0 .. i0+kTL-1 (whole CTA)
 template <int N, int NS, class B>
-__global__ void __launch_bounds__(256) k_vic_finish(Geo g, Phys p, B b) {
-  constexpr int E1 = VicDims<N>::E1, ES = VicDims<N>::ES;
+__device__ __forceinline__ void vic_finish_tile(const Geo& g, const Phys& p, const B& b,
+                                                int64_t col0, int i0) {
+  constexpr int ES = VicDims<N>::ES;
   const int nl = g.nx1;
   const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
-  const int64_t col0 = (int64_t)blockIdx.x * kTC;
-  const int i0 = blockIdx.y * kTL;
   const int64_t sv = g.sv;
-  const double* S = b.vic + (int64_t)(nl + 2) * E1 * ncol;
+  const double* S = b.vic;
   const double* Z = S + (int64_t)nl * ES * ncol;
   __shared__ double dl[N][kTC][kTL + 1];
   __shared__ double zs[2][kTC];
@@ -402,15 +332,18 @@ __global__ void __launch_bounds__(256) k_vic_finish(Geo g, Phys p, B b) {
   }
 }
 
+template <int N, int NS, class B>
+__global__ void __launch_bounds__(256) k_vic_finish(Geo g, Phys p, B b) {
+  vic_finish_tile<N, NS, B>(g, p, b, (int64_t)blockIdx.x * kTC, (int)blockIdx.y * kTL);
+}
+
 template <int N, class B>
 static cudaError_t launch_vic_n(const Geo& g, const Phys& p, const B& b, cudaStream_t st) {
   const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
   const int nl = g.nx1;
-  dim3 ga((unsigned)((ncol + kTC - 1) / kTC), (unsigned)((nl + 2 + kTLA - 1) / kTLA));
-  k_vic_assemble<N, B><<<ga, 256, 0, st>>>(g, p, b);
   // small column counts: narrower CTAs spread the sequential sweeps over more SMs
   int bs = ncol >= 148 * 128 ? 128 : (ncol >= 148 * 64 ? 64 : 32);
-  k_vic_sweep<N, B><<<(unsigned)((ncol + bs - 1) / bs), bs, 0, st>>>(g, p, b);
+  k_vic_column<N, B><<<(unsigned)((ncol + bs - 1) / bs), bs, 0, st>>>(g, p, b);
   dim3 gf((unsigned)((ncol + kTC - 1) / kTC), (unsigned)((nl + kTL - 1) / kTL));
   switch (p.nscalar) {
     case 0: k_vic_finish<N, 0, B><<<gf, 256, 0, st>>>(g, p, b); break;
@@ -430,6 +363,81 @@ cudaError_t launch_vic(const Geo& g, const Phys& p, const StageBufs& b, cudaStre
 cudaError_t launch_vic32(const Geo& g, const Phys& p, const StageBufs32& b, cudaStream_t st) {
   if (vic_n(p) == 5) return launch_vic_n<5>(g, p, b, st);
   return launch_vic_n<3>(g, p, b, st);
+}
+
+// ---- persistent batched variants (ensemble members, FP32 form) ----
+__device__ __forceinline__ void set_stage_vic32(StageBufs32& b, int stage) {
+  double w0 = 1., w1 = 0., w2 = 1.;
+  if (stage == 1) w0 = 3. / 4., w1 = 1. / 4., w2 = 1. / 4.;
+  if (stage == 2) w0 = 1. / 3., w1 = 2. / 3., w2 = 2. / 3.;
+  b.stage = stage;
+  b.wgt0 = w0;
+  b.wgt1 = w1;
+  b.wgt2 = w2;
+}
+
+template <int N>
+__global__ void __launch_bounds__(128) k_vic_column_batch(const Member32* __restrict__ mem,
+                                                          Phys p, WorkQueue q, int stage) {
+  int m;
+  int64_t tile;
+  while (queue_next(q, m, tile)) {
+    const Geo g = mem[m].g;
+    StageBufs32 b = mem[m].b;
+    set_stage_vic32(b, stage);
+    const int64_t col = tile * mem[m].vic_cols + threadIdx.x;
+    if ((int)threadIdx.x < mem[m].vic_cols) vic_column<N, StageBufs32>(g, p, b, col);
+  }
+}
+
+template <int N, int NS>
+__global__ void __launch_bounds__(256) k_vic_finish_batch(const Member32* __restrict__ mem,
+                                                          Phys p, WorkQueue q, int stage) {
+  int m;
+  int64_t tile;
+  while (queue_next(q, m, tile)) {
+    const Geo g = mem[m].g;
+    StageBufs32 b = mem[m].b;
+    set_stage_vic32(b, stage);
+    const int nlb = (g.nx1 + kTL - 1) / kTL;
+    const int64_t cb = tile / nlb;
+    const int lb = (int)(tile - cb * nlb);
+    vic_finish_tile<N, NS, StageBufs32>(g, p, b, cb * kTC, lb * kTL);
+  }
+}
+
+cudaError_t launch_vic_column_batch(const Member32* mem, const Phys& p, const WorkQueue& q,
+                                    int stage, int grid, int block, cudaStream_t st) {
+  if (vic_n(p) == 5)
+    k_vic_column_batch<5><<<grid, block, 0, st>>>(mem, p, q, stage);
+  else
+    k_vic_column_batch<3><<<grid, block, 0, st>>>(mem, p, q, stage);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_vic_finish_batch(const Member32* mem, const Phys& p, const WorkQueue& q,
+                                    int stage, int grid, cudaStream_t st) {
+  static_assert(kTC == kVicFinishCols && kTL == kVicFinishLayers, "finish tile shape");
+#define SNAPB_VFB(N, NS) k_vic_finish_batch<N, NS><<<grid, 256, 0, st>>>(mem, p, q, stage)
+  if (vic_n(p) == 5) {
+    switch (p.nscalar) {
+      case 0: SNAPB_VFB(5, 0); break;
+      case 1: SNAPB_VFB(5, 1); break;
+      case 2: SNAPB_VFB(5, 2); break;
+      case 3: SNAPB_VFB(5, 3); break;
+      default: return cudaErrorInvalidValue;
+    }
+  } else {
+    switch (p.nscalar) {
+      case 0: SNAPB_VFB(3, 0); break;
+      case 1: SNAPB_VFB(3, 1); break;
+      case 2: SNAPB_VFB(3, 2); break;
+      case 3: SNAPB_VFB(3, 3); break;
+      default: return cudaErrorInvalidValue;
+    }
+  }
+#undef SNAPB_VFB
+  return cudaGetLastError();
 }
 
 }  // namespace snapb

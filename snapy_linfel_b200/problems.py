@@ -110,6 +110,15 @@ def ensemble(n=48, seed=2024, horiz=(64, 96, 128), vert=(64, 128)):
     return members
 
 
+def ensemble_members(n=48, seed=2024, horiz=(64, 96, 128), vert=(64, 128),
+                     riemann="lmars", implicit_scheme=1):
+    """(options, w, r) of every member of the seeded ensemble."""
+    out = []
+    for m in ensemble(n=n, seed=seed, horiz=horiz, vert=vert):
+        out.append(warm_bubble_3d(riemann=riemann, implicit_scheme=implicit_scheme, **m))
+    return out
+
+
 def gaussian_random_field(shape, dx, corr, sigma, seed):
     """Seeded Gaussian random field by FFT filtering of white noise."""
     rng = np.random.default_rng(seed)
