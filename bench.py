@@ -1,10 +1,21 @@
 """Benchmark of the hydro forward step (one JSON line on rank 0).
 
-Workload (default ``c5``): the large single 3-D domain of the benchmark
-configurations — 384 x 384 x 192 cells, H2-He ideal gas, WENO5 + Roe,
-vertically implicit solve (3x3 VIC), 2 passive tracers, doubly periodic,
-synthetic seeded initial state.  A "step" is one RK3 step (3 stages) of the
-whole domain; the unit counts interior cells x RK stages.
+Workload (default ``c3``): the batched ensemble of the benchmark
+configurations — 48 independent 3-D dry warm-bubble domains of seeded uneven
+sizes ({64,96,128}^2 x {64,128}, 48.2 M cells in all), WENO5 + LMARS,
+vertically implicit solve (3x3 VIC), doubly periodic, CFL 0.8.  The head
+value is the batched FP32 perturbation form (one persistent launch per sweep
+over all members, the step replayed from a CUDA graph, tile shapes picked by
+the autotuner); the plain FP64 form (member after member through
+snapb_stage) runs the same members beside it, and both are compared field by
+field over a few steps with the same dt.  A "step" is one RK3 step (3 stages)
+of every member; the unit counts interior cells x RK stages.  The line also
+carries the adjoint/forward time of the 2-D warm-bubble adjoint workload
+(512 x 256, WENO5 + HLLC, vertical implicit).
+
+Other workloads: ``c3s`` (the first 12 members, for profiling captures),
+``c5`` (384 x 384 x 192 H2-He single domain, WENO5 + Roe, 2 tracers; FP32
+form vs FP64 form and the adjoint on that domain), ``c5s``, ``c2``, ``c1``.
 
 Arms:
   --impl ours       (default) the CUDA path through the C ABI
@@ -35,6 +46,8 @@ UNIT = "Mcell-updates/s"
 
 
 WORKLOAD_DESC = {
+    "c3": "ensemble_48_warm_bubbles_3d_{64,96,128}^2x{64,128}_weno5_lmars_vic3",
+    "c3s": "ensemble_first_12_of_48_warm_bubbles_3d_weno5_lmars_vic3",
     "c5": "large_3d_h2he_384x384x192_weno5_roe_vic3_2tracers",
     "c5s": "large_3d_h2he_96x96x192_weno5_roe_vic3_2tracers",
     "c2": "straka_1024x128_weno5_lmars_vic3_diffusion",
@@ -159,25 +172,44 @@ def measured_peaks():
 # --------------------------------------------------------------------------
 # CPU arm / baseline (the checker's builds; only bench.py's baseline legs run them)
 # --------------------------------------------------------------------------
-def cpu_sample_run(kind: str, steps: int, warmup: int, threads: int | None = None,
-                   nx_h: int = 64):
-    """Time RK3 steps of a bounded sub-domain (nx_h x nx_h x 192) on the host."""
-    from oracle.pyoracle import Oracle
+def cpu_sample_problem(workload_name: str, nx_h: int = 64):
+    """A bounded sub-domain of a workload for the host-core timing."""
     from snapy_linfel_b200 import problems
+
+    if workload_name in ("c3", "c3s"):
+        m = problems.ensemble(n=1, seed=2024)[0]
+        m.update(nx3=nx_h, nx2=nx_h, nx1=64)
+        opts, w, _ = problems.warm_bubble_3d(**m)
+        return opts, w, None, (f"one {nx_h}x{nx_h}x64 member of the same ensemble "
+                               "(WENO5+LMARS+VIC3)")
+    opts, w, r = problems.large_3d(nx3=nx_h, nx2=nx_h, nx1=192)
+    return opts, w, r, (f"{nx_h}x{nx_h}x192 sub-domain of the same workload "
+                        "(WENO5+Roe+VIC3+2 tracers)")
+
+
+def cpu_sample_run(kind: str, steps: int, warmup: int, threads: int | None = None,
+                   nx_h: int = 64, workload_name: str = "c5"):
+    """Time RK3 steps of a bounded sub-domain of the workload on the host."""
+    from oracle.pyoracle import Oracle
     from snapy_linfel_b200.config import CONSERVED, PRIMITIVE, SCALAR
 
     orc = Oracle(kind)
     nthreads = threads or os.cpu_count() or 1
     orc.set_threads(nthreads)
-    opts, w, r = problems.large_3d(nx3=nx_h, nx2=nx_h, nx1=192)
+    opts, w, r, what = cpu_sample_problem(workload_name, nx_h)
     c = opts.hydro
     orc.bc_apply(c, w, PRIMITIVE)
-    orc.bc_apply(c, r, SCALAR)
     u = orc.prim2cons(c, w)
-    s = w[0:1] * r
     orc.bc_apply(c, u, CONSERVED)
-    orc.bc_apply(c, s, SCALAR)
-    u0, s0 = np.empty_like(u), np.empty_like(s)
+    u0 = np.empty_like(u)
+    s = s0 = None
+    if c.nscalar:
+        orc.bc_apply(c, r, SCALAR)
+        s = w[0:1] * r
+        orc.bc_apply(c, s, SCALAR)
+        s0 = np.empty_like(s)
+    else:
+        r = None
     blk = orc.block(c)
     times = []
     for n in range(warmup + steps):
@@ -190,8 +222,7 @@ def cpu_sample_run(kind: str, steps: int, warmup: int, threads: int | None = Non
     cells = interior_cells(c)
     per_step = statistics.median(times)
     value = cells * 3 / per_step / 1e6
-    sample = (f"{nx_h}x{nx_h}x192 sub-domain of the same workload (WENO5+Roe+VIC3+2 tracers), "
-              f"{steps} RK3 step(s), median wall time")
+    sample = f"{what}, {steps} RK3 step(s), median wall time"
     return value, per_step, nthreads, sample, orc.kind
 
 
@@ -203,7 +234,8 @@ def run_reference(args):
         return 0
     desc = WORKLOAD_DESC[args.workload]
     kind = "reference" if os.path.exists(lib_path("reference")) else "port"
-    value, per_step, cores, sample, _ = cpu_sample_run(kind, args.steps, args.warmup)
+    value, per_step, cores, sample, _ = cpu_sample_run(kind, args.steps, args.warmup,
+                                                       workload_name=args.workload)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -345,7 +377,7 @@ def run_adjoint_timing(args, opts, state, cells, stream, barrier):
     del mb
     runner = StepRunner(opts, device="cuda")
     adj = runner.adjoint()
-    nsteps = max(1, min(args.steps, args.adj_steps))
+    nsteps = max(1, min(args.steps, args.adj_steps)) if cells >= 1_000_000 else 10
     runner.load(u0, s0)
     for _ in range(2):  # warm-up
         runner.step(dt)
@@ -408,6 +440,226 @@ def run_adjoint_timing(args, opts, state, cells, stream, barrier):
                              "checkpoint_every": nsteps},
             "reverse_kernel_ms_per_stage": kern, "dtype": "f64",
             "value": cells * 3 / (rev_ms / 1e3) / 1e6, "unit": "Mcell-updates/s (reverse)"}
+
+
+def ensemble_launches_per_step(cfg) -> int:
+    """kernels of one batched step: CFL fill + reduce + final, then per stage
+    x1, x2, x3 sweeps, implicit column + finish, boundary fill(s)"""
+    per_stage = 3 + (2 if cfg.implicit_scheme else 0) + 1 + (1 if cfg.nscalar else 0)
+    return 3 + 3 * per_stage
+
+
+def perturbation_fields(u, cfg, rb, pb):
+    """rho' = rho - rho_bar, theta' = theta - theta_bar (p0 = 1e5 Pa) and the
+    vertical velocity of a conserved FP64 state, interior cells"""
+    it = cfg.interior()
+    gm1 = cfg.gammad - 1.0
+    kappa = gm1 / cfg.gammad
+    rho = u[0]
+    ke = 0.5 * (u[1] ** 2 + u[2] ** 2 + u[3] ** 2) / rho
+    p = gm1 * (u[4] - ke)
+    theta = p / (rho * cfg.rgas) * (1.0e5 / p) ** kappa
+    rbv, pbv = rb.view(1, 1, -1), pb.view(1, 1, -1)
+    theta_bar = pbv / (rbv * cfg.rgas) * (1.0e5 / pbv) ** kappa
+    return [(rho - rbv)[it], (theta - theta_bar)[it], (u[1] / rho)[it]]
+
+
+def run_ensemble(args):
+    import torch
+    import torch.distributed as dist
+
+    from snapy_linfel_b200 import _lib, problems
+    from snapy_linfel_b200.ensemble import Ensemble
+    from snapy_linfel_b200.mesh import MeshBlock
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    dev = f"cuda:{local}"
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_ms(ms):
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return t.item()
+
+    members = problems.ensemble_members(n=48, seed=2024)
+    if args.workload == "c3s":  # a quarter of the ensemble, for profiling captures
+        members = members[:12]
+    cfg0 = members[0][0].hydro
+    cells = sum(o.hydro.nx1 * o.hydro.nx2 * o.hydro.nx3 for o, _, _ in members)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    # ---- batched FP32: autotune, capture, replay ----
+    ens = Ensemble(members, device=dev)
+    init32 = ens.save()
+    tune = ens.tune(steps=1)
+    ens.restore(init32)
+    ens.capture()
+    for _ in range(args.warmup):
+        ens.step()
+    barrier()
+    with ClockSampler(local) as clk:
+        barrier()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            ens.step()
+        ev1.record(stream)
+        barrier()
+    ms32 = max_ms(ev0.elapsed_time(ev1))
+    value32 = world * cells * 3 * args.steps / (ms32 / 1e3) / 1e6
+    _lib.timing_enable(True)
+    for _ in range(2):
+        ens.step_eager()
+    torch.cuda.synchronize()
+    kern32 = _lib.timing_query()
+    _lib.timing_enable(False)
+    # end to end: every member's state from pinned host memory and back, per step
+    hus = [torch.empty(b.hydro_u.shape, dtype=torch.float32).pin_memory() for b in ens.blocks]
+    for h, b in zip(hus, ens.blocks):
+        h.copy_(b.hydro_u.cpu())
+    nbytes = sum(h.numel() * 4 for h in hus)
+    barrier()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        for h, b in zip(hus, ens.blocks):
+            b.hydro_u.copy_(h, non_blocking=True)
+        ens.step()
+        for h, b in zip(hus, ens.blocks):
+            h.copy_(b.hydro_u, non_blocking=True)
+    ev1.record(stream)
+    barrier()
+    e2e = world * cells * 3 * args.steps / (max_ms(ev0.elapsed_time(ev1)) / 1e3) / 1e6
+    del hus
+
+    # ---- plain FP64: member after member through snapb_stage ----
+    blocks = []
+    for opts, w, r in members:
+        mb = MeshBlock(opts, device=dev)
+        mb.initialize(w, r)
+        blocks.append(mb)
+    for _ in range(args.warmup):
+        for mb in blocks:
+            mb.step()
+    barrier()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        for mb in blocks:
+            mb.step()
+    ev1.record(stream)
+    barrier()
+    ms64 = max_ms(ev0.elapsed_time(ev1))
+    value64 = world * cells * 3 * args.steps / (ms64 / 1e3) / 1e6
+
+    # ---- accuracy: both forms from the same state with the same dt ----
+    ens.restore(init32)
+    for (opts, w, r), mb in zip(members, blocks):
+        mb.initialize(w, r)
+    for _ in range(args.acc_steps):
+        ens.max_time_step()
+        dts = ens.dts().clone()
+        for m, mb in enumerate(blocks):
+            mb.step(dts[m:m + 1])
+        for k in range(3):
+            ens.stage(k)
+    torch.cuda.synchronize()
+    names = ["rho", "mom1", "mom2", "mom3", "energy", "rho_prime", "theta_prime", "w_vertical"]
+    num = np.zeros(len(names))
+    den = np.zeros(len(names))
+    emax = np.zeros(len(names))
+    vmax = np.zeros(len(names))
+    for b32, b64 in zip(ens.blocks, blocks):
+        c = b64.cfg
+        it = c.interior()
+        a = b32.state64()
+        b = b64.hydro_u
+        fa = [a[v][it] for v in range(5)] + perturbation_fields(a, c, b32.ref_rho, b32.ref_p)
+        fb = [b[v][it] for v in range(5)] + perturbation_fields(b, c, b32.ref_rho, b32.ref_p)
+        for k, (x, y) in enumerate(zip(fa, fb)):
+            d = (x - y).abs()
+            num[k] += float(d.sum())
+            den[k] += float(y.abs().sum())
+            emax[k] = max(emax[k], float(d.max()))
+            vmax[k] = max(vmax[k], float(y.abs().max()))
+    acc = {"steps": args.acc_steps, "fields": names,
+           "rel_l1": [float(n / max(d, 1e-300)) for n, d in zip(num, den)],
+           "linf": [float(e / max(v, 1e-300)) for e, v in zip(emax, vmax)]}
+    del blocks
+    torch.cuda.empty_cache()
+
+    # ---- adjoint / forward time on the 2-D warm-bubble adjoint workload ----
+    adj = None
+    if not args.no_adjoint:
+        aopts, aw, _ = problems.adjoint_bubble()
+        adj = run_adjoint_timing(args, aopts, (aw, None), interior_cells(aopts.hydro), stream,
+                                 barrier)
+        adj["workload"] = "adjoint_bubble_2d_512x256_weno5_hllc_vic3"
+
+    # ---- roofline of the dominant batched kernel ----
+    peak, peak_src = measured_peaks()
+    roof = dominant_roofline(kern32, cfg0, cells, 4, peak, peak_src)
+    st32 = ms32 / 1e3 / (3 * args.steps)
+    bw32 = algo_bytes_per_cell_update(cfg0, 4) * cells / st32 / 1e9
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            from oracle.pyoracle import lib_path
+
+            kind = "reference" if os.path.exists(lib_path("reference")) else "port"
+            v, per_step, cores, sample, _ = cpu_sample_run(kind, 1, 0, workload_name="c3")
+            cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": UNIT, "cores": None, "kind": None,
+                   "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value32, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms32 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (perturbation over f64 reference)", "data": "synthetic",
+            "config": {"workload": WORKLOAD_DESC[args.workload], "members": len(members),
+                       "cells_per_gpu": cells, "rk_stages_per_step": 3,
+                       "form": "batched_fp32_perturbation (persistent work queue, CUDA graph)",
+                       "tuning": tune["best"],
+                       "l2_policy": "inputs larger than L2 (ensemble state > 126 MB)",
+                       "parallelism": f"replicas x{world}"},
+            "forms": {
+                "batched_fp32": {"value": value32, "ms_per_step": ms32 / args.steps,
+                                 "kernel_ms_per_launch": {k: round(v[0] / v[1], 4)
+                                                          for k, v in kern32.items()},
+                                 "stage_roofline": {"achieved": bw32, "peak": peak,
+                                                    "unit": "GB/s", "frac": bw32 / peak}},
+                "plain_fp64_member_by_member": {"value": value64,
+                                                "ms_per_step": ms64 / args.steps},
+                "batched_fp32_over_plain_fp64": value32 / value64,
+                "accuracy_fp32_vs_fp64": acc,
+                "autotuner": tune,
+            },
+            "roofline": roof,
+            "adjoint": adj,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+                    "d2h_bytes_per_step": nbytes},
+            "gpu_launches": ensemble_launches_per_step(cfg0) * args.steps,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
 
 
 def run_ours(args):
@@ -518,7 +770,8 @@ def run_ours(args):
             from oracle.pyoracle import lib_path
 
             kind = "reference" if os.path.exists(lib_path("reference")) else "port"
-            v, per_step, cores, sample, _ = cpu_sample_run(kind, 1, 0)
+            v, per_step, cores, sample, _ = cpu_sample_run(kind, 1, 0,
+                                                           workload_name=args.workload)
             cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": UNIT, "cores": None, "kind": None,
@@ -580,7 +833,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c5")
+    ap.add_argument("--workload", default="c3")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--acc-steps", type=int, default=5)
@@ -591,6 +844,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload in ("c3", "c3s"):
+        return run_ensemble(args)
     return run_ours(args)
 
 

@@ -179,8 +179,8 @@ int plan(snapb_ensemble* e) {
                          ? ((ncolv + kVicFinishCols - 1) / kVicFinishCols) *
                                ((g.nx1 + kVicFinishLayers - 1) / kVicFinishLayers)
                          : 0;
-    tiles[PH_BCU] = (g.sv + 255) / 256;
-    tiles[PH_BCS] = e->p.nscalar ? (g.sv + 255) / 256 : 0;
+    tiles[PH_BCU] = (ncol1 + 7) / 8;  // 8 x1 rows per tile, one warp each
+    tiles[PH_BCS] = e->p.nscalar ? (ncol1 + 7) / 8 : 0;
     int64_t ncell = (int64_t)(g.iu - g.il + 1) * (g.ju - g.jl + 1) * (g.ku - g.kl + 1);
     tiles[PH_CFL] = (ncell + 1023) / 1024;
     for (int ph = 0; ph < PH_COUNT; ++ph) e->prefix[ph][m + 1] = e->prefix[ph][m] + tiles[ph];
@@ -226,10 +226,12 @@ WorkQueue queue(const snapb_ensemble* e, int ph) {
   return q;
 }
 
-int grid_of(const snapb_ensemble* e, int ph, int per_sm_default) {
-  int per = e->tune.ctas_per_sm > 0 ? e->tune.ctas_per_sm : per_sm_default;
-  int64_t tiles = e->prefix[ph][e->M];
-  return (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)per * e->sms, tiles));
+PersistGrid pgrid(const snapb_ensemble* e, int ph) {
+  PersistGrid g;
+  g.sms = e->sms;
+  g.cap = e->tune.ctas_per_sm;
+  g.tiles = e->prefix[ph][e->M];
+  return g;
 }
 
 }  // namespace
@@ -352,7 +354,7 @@ int snapb_ensemble_max_time_step_f32(snapb_ensemble* e, double factor, void* str
   cudaError_t c = cudaMemsetAsync(e->ws + e->o_counter + PH_CFL * sizeof(unsigned long long), 0,
                                   sizeof(unsigned long long), st);
   if (c != cudaSuccess) return cuda_e(c, "ensemble cfl");
-  k_cfl32_batch<<<grid_of(e, PH_CFL, 8), 256, 0, st>>>(
+  k_cfl32_batch<<<persistent_grid(k_cfl32_batch, 256, 0, pgrid(e, PH_CFL)), 256, 0, st>>>(
       reinterpret_cast<const Member32*>(e->ws + e->o_mem), e->p, queue(e, PH_CFL), slots, e->use1,
       e->use2, e->use3);
   k_cfl_batch_final<<<(e->M + 127) / 128, 128, 0, st>>>(
@@ -373,39 +375,39 @@ int snapb_ensemble_stage_f32(snapb_ensemble* e, int stage, void* stream) {
   int last = e->a3 ? 3 : (e->a2 ? 2 : 1);
   if (e->a1) {
     ScopedTimer t(SNAPB_K_X1, st);
-    c = launch_x1_32_batch(mem, p, queue(e, PH_X1), stage, last == 1, grid_of(e, PH_X1, 2),
+    c = launch_x1_32_batch(mem, p, queue(e, PH_X1), stage, last == 1, pgrid(e, PH_X1),
                            e->x1_smem, st);
     if (c != cudaSuccess) return cuda_e(c, "ensemble x1");
   }
   if (e->a2) {
     ScopedTimer t(SNAPB_K_X2, st);
     c = launch_march32_batch(2, mem, p, queue(e, PH_X2), stage, !e->a1, last == 2,
-                             grid_of(e, PH_X2, 8), st);
+                             pgrid(e, PH_X2), st);
     if (c != cudaSuccess) return cuda_e(c, "ensemble x2");
   }
   if (e->a3) {
     ScopedTimer t(SNAPB_K_X3, st);
     c = launch_march32_batch(3, mem, p, queue(e, PH_X3), stage, !e->a1 && !e->a2, true,
-                             grid_of(e, PH_X3, 8), st);
+                             pgrid(e, PH_X3), st);
     if (c != cudaSuccess) return cuda_e(c, "ensemble x3");
   }
   if (p.implicit_scheme) {
     ScopedTimer t(SNAPB_K_VIC, st);
     int blk = e->mem.empty() ? 64 : e->mem[0].vic_cols;
-    c = launch_vic_column_batch(mem, p, queue(e, PH_VCOL), stage, grid_of(e, PH_VCOL, 8), blk,
+    c = launch_vic_column_batch(mem, p, queue(e, PH_VCOL), stage, pgrid(e, PH_VCOL), blk,
                                 st);
     if (c == cudaSuccess)
-      c = launch_vic_finish_batch(mem, p, queue(e, PH_VFIN), stage, grid_of(e, PH_VFIN, 4), st);
+      c = launch_vic_finish_batch(mem, p, queue(e, PH_VFIN), stage, pgrid(e, PH_VFIN), st);
     if (c != cudaSuccess) return cuda_e(c, "ensemble implicit");
   }
   {
     ScopedTimer t(SNAPB_K_BC, st);
     double igm1 = 1.0 / (e->cfg0.gammad - 1.0);
-    c = launch_bc32_batch(mem, p, queue(e, PH_BCU), SNAPB_CONSERVED, igm1, grid_of(e, PH_BCU, 8),
+    c = launch_bc32_batch(mem, p, queue(e, PH_BCU), SNAPB_CONSERVED, igm1, pgrid(e, PH_BCU),
                           st);
     if (c == cudaSuccess && p.nscalar)
       c = launch_bc32_batch(mem, p, queue(e, PH_BCS), SNAPB_SCALAR, igm1,
-                            grid_of(e, PH_BCS, 8), st);
+                            pgrid(e, PH_BCS), st);
     if (c != cudaSuccess) return cuda_e(c, "ensemble boundary");
   }
   return SNAPB_OK;

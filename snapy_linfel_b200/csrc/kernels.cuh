@@ -106,18 +106,39 @@ __device__ __forceinline__ bool queue_next(const WorkQueue& q, int& m, int64_t& 
   return true;
 }
 
-// persistent launchers of the batched FP32 stage (grid = persistent CTAs)
+// Persistent grid of a batched launch: as many CTAs as fit on the GPU at once
+// (the occupancy calculator's blocks per SM, optionally capped), never more
+// than there are work items.
+struct PersistGrid {
+  int sms;        // multiprocessors
+  int cap;        // CTAs per SM cap (0: occupancy only)
+  int64_t tiles;  // work items in the queue
+};
+template <class K>
+inline int persistent_grid(K kernel, int block, size_t smem, const PersistGrid& pg) {
+  int per = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, block, smem) != cudaSuccess ||
+      per < 1)
+    per = 1;
+  if (pg.cap > 0 && pg.cap < per) per = pg.cap;
+  int64_t g = (int64_t)per * pg.sms;
+  if (g > pg.tiles) g = pg.tiles;
+  return (int)(g < 1 ? 1 : g);
+}
+
+// persistent launchers of the batched FP32 stage
 cudaError_t launch_x1_32_batch(const Member32* mem, const Phys& p, const WorkQueue& q,
-                               int stage, bool last, int grid, size_t smem, cudaStream_t st);
+                               int stage, bool last, const PersistGrid& pg, size_t smem,
+                               cudaStream_t st);
 cudaError_t launch_march32_batch(int axis, const Member32* mem, const Phys& p,
-                                 const WorkQueue& q, int stage, bool first, bool last, int grid,
-                                 cudaStream_t st);
+                                 const WorkQueue& q, int stage, bool first, bool last,
+                                 const PersistGrid& pg, cudaStream_t st);
 cudaError_t launch_vic_column_batch(const Member32* mem, const Phys& p, const WorkQueue& q,
-                                    int stage, int grid, int block, cudaStream_t st);
+                                    int stage, const PersistGrid& pg, int block, cudaStream_t st);
 cudaError_t launch_vic_finish_batch(const Member32* mem, const Phys& p, const WorkQueue& q,
-                                    int stage, int grid, cudaStream_t st);
+                                    int stage, const PersistGrid& pg, cudaStream_t st);
 cudaError_t launch_bc32_batch(const Member32* mem, const Phys& p, const WorkQueue& q, int kind,
-                              double igm1, int grid, cudaStream_t st);
+                              double igm1, const PersistGrid& pg, cudaStream_t st);
 size_t x1_smem32_per_column(const Geo& g, int nvt);
 StageBufs32 bufs32_of(const snapb_hydro_config& c, void* ws);
 size_t workspace_size_f32_of(const snapb_hydro_config& c);

@@ -620,25 +620,44 @@ __global__ void __launch_bounds__(128) k_march32_batch(const Member32* __restric
   }
 }
 
+// boundary fill over x1 rows (k, j): one warp per row; rows inside the x2/x3
+// interior only fill their x1 ghosts, ghost rows fill every cell
 __global__ void __launch_bounds__(256) k_bc32_batch(const Member32* __restrict__ mem, Phys p,
                                                     WorkQueue q, int kind, double igm1) {
   int m;
   int64_t tile;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   while (queue_next(q, m, tile)) {
     const Geo& g = mem[m].g;
     const Member32& mb = mem[m];
+    const int64_t row = tile * 8 + warp;
+    if (row >= (int64_t)g.nc2 * g.nc3) continue;
     AxisBC32 a1{g.nc1, g.ng, mb.bc[0], mb.bc[1]};
     AxisBC32 a2{g.nc2, g.ng, mb.bc[2], mb.bc[3]};
     AxisBC32 a3{g.nc3, g.ng, mb.bc[4], mb.bc[5]};
     float* var = kind == SNAPB_SCALAR ? mb.b.s : mb.b.u;
-    int nv = kind == SNAPB_SCALAR ? p.nscalar : 5;
-    bc32_cell(g.nc1, g.nc2, g.nc3, g.sv, a1, a2, a3, var, nv, kind, mb.b.rb, mb.b.pb, igm1,
-              tile * blockDim.x + threadIdx.x);
+    const int nv = kind == SNAPB_SCALAR ? p.nscalar : 5;
+    const int j = (int)(row % g.nc2), k = (int)(row / g.nc2);
+    const bool inner = j >= g.jl && j <= g.ju && k >= g.kl && k <= g.ku;
+    const int64_t base = row * g.nc1;
+    if (inner) {
+      if (g.nc1 > 1)
+        for (int c = lane; c < 2 * g.ng; c += 32) {
+          int i = c < g.ng ? c : g.nc1 - 2 * g.ng + c;
+          bc32_cell(g.nc1, g.nc2, g.nc3, g.sv, a1, a2, a3, var, nv, kind, mb.b.rb, mb.b.pb,
+                    igm1, base + i);
+        }
+    } else {
+      for (int i = lane; i < g.nc1; i += 32)
+        bc32_cell(g.nc1, g.nc2, g.nc3, g.sv, a1, a2, a3, var, nv, kind, mb.b.rb, mb.b.pb, igm1,
+                  base + i);
+    }
   }
 }
 
 cudaError_t launch_x1_32_batch(const Member32* mem, const Phys& p, const WorkQueue& q,
-                               int stage, bool last, int grid, size_t smem, cudaStream_t st) {
+                               int stage, bool last, const PersistGrid& pg, size_t smem,
+                               cudaStream_t st) {
 #define SNAPB_X1B(NS)                                                                         \
   case NS: {                                                                                  \
     static bool attr = false;                                                                 \
@@ -647,6 +666,7 @@ cudaError_t launch_x1_32_batch(const Member32* mem, const Phys& p, const WorkQue
                            200 * 1024);                                                       \
       attr = true;                                                                            \
     }                                                                                         \
+    int grid = persistent_grid(k_x1_32_batch<NS>, 256, smem, pg);                             \
     k_x1_32_batch<NS><<<grid, 256, smem, st>>>(mem, p, q, stage, last ? 1 : 0);               \
     break;                                                                                    \
   }
@@ -662,14 +682,16 @@ cudaError_t launch_x1_32_batch(const Member32* mem, const Phys& p, const WorkQue
 }
 
 cudaError_t launch_march32_batch(int axis, const Member32* mem, const Phys& p,
-                                 const WorkQueue& q, int stage, bool first, bool last, int grid,
-                                 cudaStream_t st) {
+                                 const WorkQueue& q, int stage, bool first, bool last,
+                                 const PersistGrid& pg, cudaStream_t st) {
 #define SNAPB_MB(NS)                                                                         \
   case NS:                                                                                   \
     if (axis == 2)                                                                           \
-      k_march32_batch<NS, 2><<<grid, 128, 0, st>>>(mem, p, q, stage, first, last);           \
+      k_march32_batch<NS, 2><<<persistent_grid(k_march32_batch<NS, 2>, 128, 0, pg), 128, 0,   \
+                               st>>>(mem, p, q, stage, first, last);                         \
     else                                                                                     \
-      k_march32_batch<NS, 3><<<grid, 128, 0, st>>>(mem, p, q, stage, first, last);           \
+      k_march32_batch<NS, 3><<<persistent_grid(k_march32_batch<NS, 3>, 128, 0, pg), 128, 0,   \
+                               st>>>(mem, p, q, stage, first, last);                         \
     break;
   switch (p.nscalar) {
     SNAPB_MB(0)
@@ -683,8 +705,8 @@ cudaError_t launch_march32_batch(int axis, const Member32* mem, const Phys& p,
 }
 
 cudaError_t launch_bc32_batch(const Member32* mem, const Phys& p, const WorkQueue& q, int kind,
-                              double igm1, int grid, cudaStream_t st) {
-  k_bc32_batch<<<grid, 256, 0, st>>>(mem, p, q, kind, igm1);
+                              double igm1, const PersistGrid& pg, cudaStream_t st) {
+  k_bc32_batch<<<persistent_grid(k_bc32_batch, 256, 0, pg), 256, 0, st>>>(mem, p, q, kind, igm1);
   return cudaGetLastError();
 }
 

@@ -407,18 +407,23 @@ __global__ void __launch_bounds__(256) k_vic_finish_batch(const Member32* __rest
 }
 
 cudaError_t launch_vic_column_batch(const Member32* mem, const Phys& p, const WorkQueue& q,
-                                    int stage, int grid, int block, cudaStream_t st) {
+                                    int stage, const PersistGrid& pg, int block,
+                                    cudaStream_t st) {
   if (vic_n(p) == 5)
-    k_vic_column_batch<5><<<grid, block, 0, st>>>(mem, p, q, stage);
+    k_vic_column_batch<5><<<persistent_grid(k_vic_column_batch<5>, block, 0, pg), block, 0,
+                            st>>>(mem, p, q, stage);
   else
-    k_vic_column_batch<3><<<grid, block, 0, st>>>(mem, p, q, stage);
+    k_vic_column_batch<3><<<persistent_grid(k_vic_column_batch<3>, block, 0, pg), block, 0,
+                            st>>>(mem, p, q, stage);
   return cudaGetLastError();
 }
 
 cudaError_t launch_vic_finish_batch(const Member32* mem, const Phys& p, const WorkQueue& q,
-                                    int stage, int grid, cudaStream_t st) {
+                                    int stage, const PersistGrid& pg, cudaStream_t st) {
   static_assert(kTC == kVicFinishCols && kTL == kVicFinishLayers, "finish tile shape");
-#define SNAPB_VFB(N, NS) k_vic_finish_batch<N, NS><<<grid, 256, 0, st>>>(mem, p, q, stage)
+#define SNAPB_VFB(N, NS)                                                                 \
+  k_vic_finish_batch<N, NS><<<persistent_grid(k_vic_finish_batch<N, NS>, 256, 0, pg), 256, 0, \
+                              st>>>(mem, p, q, stage)
   if (vic_n(p) == 5) {
     switch (p.nscalar) {
       case 0: SNAPB_VFB(5, 0); break;
