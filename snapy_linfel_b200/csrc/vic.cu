@@ -149,21 +149,31 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
   const double gm1f = 0.5 * (p.gammad + p.gammad) - 1.;
   const double dt = *b.dt;
   const double Aa = g.A1, hiv = 0.5 / g.vol, idt = 1. / dt, grav = p.grav1, V = g.vol;
-  double wc[5], wn[5];
+  double wc[5], wn[5], wq[5], dq[N];
   double Am[N][N], Jp[N][N], Jc[N][N], ap[N][N], dp[N];
   load_w(-1, wn);
   jac_block<N>(gm1c, wn, Jp);
   load_w(0, wc);
   absA_block<N>(gm1f, wn, wc, Am);
   jac_block<N>(gm1c, wc, Jc);
+  // the next layer's loads are issued one iteration ahead of their use
+  load_w(1, wq);
+#pragma unroll
+  for (int r = 0; r < N; ++r) dq[r] = vic_d(b, sel<N>(r) * sv + cb);
   double sum_a2 = 0.;
   for (int i = 0; i < nl; ++i) {
-    load_w(i + 1, wn);  // the ghost cell nl at the top
     double Ap[N][N], Jn[N][N], rhs[N];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) wn[v] = wq[v];  // cell i+1 (the ghost cell nl at the top)
+#pragma unroll
+    for (int r = 0; r < N; ++r) rhs[r] = dq[r] / dt;
+    if (i + 2 <= nl) load_w(i + 2, wq);
+    if (i + 1 < nl) {
+#pragma unroll
+      for (int r = 0; r < N; ++r) dq[r] = vic_d(b, sel<N>(r) * sv + cb + i + 1);
+    }
     absA_block<N>(gm1f, wc, wn, Ap);
     jac_block<N>(gm1c, wn, Jn);
-#pragma unroll
-    for (int r = 0; r < N; ++r) rhs[r] = vic_d(b, sel<N>(r) * sv + cb + i) / dt;
     double ai = wc[IDN] * V;
     sum_a2 += ai * ai;
     double a[N][N], bb[N][N], c[N][N];
@@ -235,21 +245,36 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
 #pragma unroll
   for (int r = 0; r < N; ++r) dn[r] = dp[r];
   double b_dry = (vic_d(b, IDN * sv + cb + nl - 1) - dn[0]) * 1. * V;
+  // layer i's reduced block, partial solution and du[IDN], loaded one layer ahead
+  double sa[N * N + N], du0 = 0.;
+  if (nl >= 2) {
+#pragma unroll
+    for (int e = 0; e < N * N + N; ++e) sa[e] = Sat(nl - 2, e);
+    du0 = vic_d(b, IDN * sv + cb + nl - 2);
+  }
   for (int i = nl - 2; i >= 0; --i) {
+    double cur[N * N + N], dcur = du0;
+#pragma unroll
+    for (int e = 0; e < N * N + N; ++e) cur[e] = sa[e];
+    if (i >= 1) {
+#pragma unroll
+      for (int e = 0; e < N * N + N; ++e) sa[e] = Sat(i - 1, e);
+      du0 = vic_d(b, IDN * sv + cb + i - 1);
+    }
     double d[N];
 #pragma unroll
     for (int r = 0; r < N; ++r) {
       double t = 0.;
 #pragma unroll
-      for (int q = 0; q < N; ++q) t += Sat(i, r * N + q) * dn[q];
-      d[r] = Sat(i, N * N + r) - t;
+      for (int q = 0; q < N; ++q) t += cur[r * N + q] * dn[q];
+      d[r] = cur[N * N + r] - t;
     }
 #pragma unroll
     for (int r = 0; r < N; ++r) {
       dn[r] = d[r];
       Sat(i, N * N + r) = d[r];
     }
-    b_dry += (vic_d(b, IDN * sv + cb + i) - d[0]) * 1. * V;
+    b_dry += (dcur - d[0]) * 1. * V;
   }
   Z[0] = sum_a2;
   Z[ncol] = b_dry;
