@@ -588,7 +588,7 @@ __device__ __forceinline__ void set_stage32(StageBufs32& b, int stage) {
 }
 
 template <int NS>
-__global__ void __launch_bounds__(256) k_x1_32_batch(const Member32* __restrict__ mem, Phys p,
+__global__ void __launch_bounds__(256, 4) k_x1_32_batch(const Member32* __restrict__ mem, Phys p,
                                                      WorkQueue q, int stage, int last) {
   extern __shared__ float smf[];
   int m;
@@ -603,7 +603,7 @@ __global__ void __launch_bounds__(256) k_x1_32_batch(const Member32* __restrict_
 }
 
 template <int NS, int AX>
-__global__ void __launch_bounds__(128) k_march32_batch(const Member32* __restrict__ mem, Phys p,
+__global__ void __launch_bounds__(128, 6) k_march32_batch(const Member32* __restrict__ mem, Phys p,
                                                        WorkQueue q, int stage, int first,
                                                        int last) {
   int m;
