@@ -271,6 +271,14 @@ def rel_errors(a, b, it):
     return out
 
 
+# DRAM bytes per interior cell of one launch (dram__bytes_read.sum +
+# dram__bytes_write.sum) from the ncu captures summarised in profiles/, scaled
+# to a launch by the cells it processes (traffic grows with the cells): the
+# batched FP32 kernels of the 12-member ensemble capture.
+NCU_TRAFFIC_PER_CELL_F32 = {"x1_sweep": 67.6, "x2_sweep": 65.5, "x3_sweep": 65.3,
+                            "implicit_vic": 245.0 + 113.3}
+
+
 def dominant_roofline(kern, cfg, cells, elem, peak, peak_src):
     """Roofline line of the kernel with the largest share of the timed region."""
     if not kern:
@@ -280,9 +288,16 @@ def dominant_roofline(kern, cfg, cells, elem, peak, peak_src):
     per_cell = kernel_algo_bytes_per_cell(name, cfg, elem)
     ach = per_cell * cells / per_launch_s / 1e9
     share = tot_ms / sum(v[0] for v in kern.values())
+    traffic = None
+    if elem == 4 and name in NCU_TRAFFIC_PER_CELL_F32:
+        traffic = NCU_TRAFFIC_PER_CELL_F32[name] * cells
     return {"kernel": name, "bound": "hbm", "achieved": ach, "peak": peak,
             "peak_source": peak_src, "unit": "GB/s", "frac": ach / peak,
-            "traffic": None, "algorithmic_bytes_per_cell": per_cell,
+            "traffic": traffic,
+            "traffic_source": ("ncu capture of the 12-member ensemble, bytes per cell x cells "
+                               "(profiles/batched_kernels_ensemble12_fp32.md)"
+                               if traffic is not None else None),
+            "algorithmic_bytes_per_cell": per_cell,
             "cells_per_launch": cells, "ms_per_launch": per_launch_s * 1e3,
             "share_of_timed_kernels": share}
 
