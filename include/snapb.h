@@ -276,10 +276,11 @@ typedef struct snapb_member_f32 {
 } snapb_member_f32;
 
 /* tile shapes; 0 = default.  x1_columns: columns per x1 tile; march_segment:
- * faces per x2/x3 segment; ctas_per_sm: persistent CTAs per SM; vic_block:
- * columns per implicit-column tile (32, 64 or 128). */
+ * faces per x2/x3 segment; ctas_per_sm: persistent CTAs per SM cap; vic_block:
+ * columns per implicit-column tile (32, 64 or 128); vic_regs: register budget
+ * of the implicit-column kernel (0 compiler's choice, 1 ~168, 2 128). */
 typedef struct snapb_ensemble_tuning {
-  int32_t x1_columns, march_segment, ctas_per_sm, vic_block;
+  int32_t x1_columns, march_segment, ctas_per_sm, vic_block, vic_regs;
 } snapb_ensemble_tuning;
 
 typedef struct snapb_ensemble snapb_ensemble; /* opaque host-side plan */

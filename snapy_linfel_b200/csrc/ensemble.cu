@@ -395,7 +395,7 @@ int snapb_ensemble_stage_f32(snapb_ensemble* e, int stage, void* stream) {
     ScopedTimer t(SNAPB_K_VIC, st);
     int blk = e->mem.empty() ? 64 : e->mem[0].vic_cols;
     c = launch_vic_column_batch(mem, p, queue(e, PH_VCOL), stage, pgrid(e, PH_VCOL), blk,
-                                st);
+                                e->tune.vic_regs, st);
     if (c == cudaSuccess)
       c = launch_vic_finish_batch(mem, p, queue(e, PH_VFIN), stage, pgrid(e, PH_VFIN), st);
     if (c != cudaSuccess) return cuda_e(c, "ensemble implicit");

@@ -134,7 +134,8 @@ cudaError_t launch_march32_batch(int axis, const Member32* mem, const Phys& p,
                                  const WorkQueue& q, int stage, bool first, bool last,
                                  const PersistGrid& pg, cudaStream_t st);
 cudaError_t launch_vic_column_batch(const Member32* mem, const Phys& p, const WorkQueue& q,
-                                    int stage, const PersistGrid& pg, int block, cudaStream_t st);
+                                    int stage, const PersistGrid& pg, int block, int variant,
+                                    cudaStream_t st);
 cudaError_t launch_vic_finish_batch(const Member32* mem, const Phys& p, const WorkQueue& q,
                                     int stage, const PersistGrid& pg, cudaStream_t st);
 cudaError_t launch_bc32_batch(const Member32* mem, const Phys& p, const WorkQueue& q, int kind,

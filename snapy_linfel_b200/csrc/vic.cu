@@ -401,9 +401,11 @@ __device__ __forceinline__ void set_stage_vic32(StageBufs32& b, int stage) {
   b.wgt2 = w2;
 }
 
-template <int N>
-__global__ void __launch_bounds__(128) k_vic_column_batch(const Member32* __restrict__ mem,
-                                                          Phys p, WorkQueue q, int stage) {
+// V selects the register budget: 0 = compiler's choice, 1 = at least 3 CTAs of
+// 128 threads per SM (~168 registers), 2 = 4 CTAs (128 registers, some spill)
+template <int N, int V>
+__global__ void __launch_bounds__(128, V == 0 ? 1 : (V == 1 ? 3 : 4))
+    k_vic_column_batch(const Member32* __restrict__ mem, Phys p, WorkQueue q, int stage) {
   int m;
   int64_t tile;
   while (queue_next(q, m, tile)) {
@@ -431,15 +433,25 @@ __global__ void __launch_bounds__(256) k_vic_finish_batch(const Member32* __rest
   }
 }
 
+template <int N, int V>
+static void launch_vcb(const Member32* mem, const Phys& p, const WorkQueue& q, int stage,
+                       const PersistGrid& pg, int block, cudaStream_t st) {
+  k_vic_column_batch<N, V><<<persistent_grid(k_vic_column_batch<N, V>, block, 0, pg), block, 0,
+                             st>>>(mem, p, q, stage);
+}
+
 cudaError_t launch_vic_column_batch(const Member32* mem, const Phys& p, const WorkQueue& q,
-                                    int stage, const PersistGrid& pg, int block,
+                                    int stage, const PersistGrid& pg, int block, int variant,
                                     cudaStream_t st) {
-  if (vic_n(p) == 5)
-    k_vic_column_batch<5><<<persistent_grid(k_vic_column_batch<5>, block, 0, pg), block, 0,
-                            st>>>(mem, p, q, stage);
-  else
-    k_vic_column_batch<3><<<persistent_grid(k_vic_column_batch<3>, block, 0, pg), block, 0,
-                            st>>>(mem, p, q, stage);
+  const bool five = vic_n(p) == 5;
+  switch (variant) {
+    case 1: five ? launch_vcb<5, 1>(mem, p, q, stage, pg, block, st)
+                 : launch_vcb<3, 1>(mem, p, q, stage, pg, block, st); break;
+    case 2: five ? launch_vcb<5, 2>(mem, p, q, stage, pg, block, st)
+                 : launch_vcb<3, 2>(mem, p, q, stage, pg, block, st); break;
+    default: five ? launch_vcb<5, 0>(mem, p, q, stage, pg, block, st)
+                  : launch_vcb<3, 0>(mem, p, q, stage, pg, block, st);
+  }
   return cudaGetLastError();
 }
 

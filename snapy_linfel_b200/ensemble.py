@@ -32,7 +32,8 @@ class MemberF32(ctypes.Structure):
 
 class Tuning(ctypes.Structure):
     _fields_ = [("x1_columns", ctypes.c_int32), ("march_segment", ctypes.c_int32),
-                ("ctas_per_sm", ctypes.c_int32), ("vic_block", ctypes.c_int32)]
+                ("ctas_per_sm", ctypes.c_int32), ("vic_block", ctypes.c_int32),
+                ("vic_regs", ctypes.c_int32)]
 
     def as_dict(self):
         return {k: int(getattr(self, k)) for k, _ in self._fields_}
@@ -172,8 +173,9 @@ class Ensemble:
         state (saved and restored), keep the fastest; returns the table."""
         import torch
 
-        cand = candidates or {"x1_columns": [0, 2, 4, 8], "march_segment": [16, 32, 64],
-                              "ctas_per_sm": [0, 4, 8], "vic_block": [32, 64, 128]}
+        cand = candidates or {"x1_columns": [0, 4, 8], "march_segment": [16, 32, 64],
+                              "ctas_per_sm": [0, 4, 8], "vic_block": [32, 64, 128],
+                              "vic_regs": [0, 1, 2]}
         snap = self.save()
         results = []
         best = None
