@@ -48,6 +48,7 @@ UNIT = "Mcell-updates/s"
 WORKLOAD_DESC = {
     "c3": "ensemble_48_warm_bubbles_3d_{64,96,128}^2x{64,128}_weno5_lmars_vic3",
     "c3s": "ensemble_first_12_of_48_warm_bubbles_3d_weno5_lmars_vic3",
+    "c4": "adjoint_bubble_2d_512x256_weno5_hllc_vic3_200steps",
     "c5": "large_3d_h2he_384x384x192_weno5_roe_vic3_2tracers",
     "c5s": "large_3d_h2he_96x96x192_weno5_roe_vic3_2tracers",
     "c2": "straka_1024x128_weno5_lmars_vic3_diffusion",
@@ -681,6 +682,94 @@ def run_ensemble(args):
     return 0
 
 
+def run_adjoint_check(args):
+    """The 2-D warm-bubble adjoint workload: 512 x 256 cells, WENO5 + HLLC +
+    VIC, 200 RK3 steps at CFL 0.8 with checkpoints every 20 steps,
+    J = domain-integrated kinetic energy at the final time; dJ/dtheta'(x, z)
+    through the hand-written adjoint (torch.autograd) against Richardson-
+    extrapolated FP64 central differences along 64 seeded random directions.
+    A weak seeded flow (0.3 m/s) is added to the bubble at rest: a resting,
+    horizontally uniform pressure puts every x2 face exactly on the HLLC
+    contact switch, where one-sided derivatives differ and a finite
+    difference is not a derivative."""
+    import torch
+
+    from snapy_linfel_b200 import adjoint as A
+    from snapy_linfel_b200 import problems
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    nsteps = args.adj_nsteps
+    opts, w, _ = problems.adjoint_bubble()
+    cfg = opts.hydro
+    rng = np.random.default_rng(4)
+    k3, k2, k1 = np.meshgrid(*[np.arange(n) / n for n in cfg.shape[1:]], indexing="ij")
+    w[1] = 0.3 * np.sin(2 * np.pi * (k1 + 2 * k2) + rng.uniform(0, 6.28))
+    w[2] = 0.3 * np.cos(2 * np.pi * (2 * k1 - k2) + rng.uniform(0, 6.28))
+    base = torch.from_numpy(w).cuda()
+    rd, cp = cfg.rgas, cfg.rgas * cfg.gammad / (cfg.gammad - 1.0)
+    p = base[4]
+    temp0 = p / (rd * base[0])
+    it = cfg.interior()
+
+    def state(dth):
+        wt = torch.cat([(p / (rd * (temp0 + dth * (p / 1.0e5) ** (rd / cp))))[None], base[1:]])
+        return A.initial_state(cfg, wt)
+
+    dth0 = torch.zeros(cfg.shape[1:], dtype=torch.float64, device="cuda")
+    dts = A.cfl_steps(opts, state(dth0).detach(), nsteps=nsteps)
+    runner = A.StepRunner(opts, device="cuda")
+
+    def J(dth):
+        uT, _ = A.rollout(opts, state(dth), None, dts, checkpoint_every=args.adj_every,
+                          runner=runner)
+        return (0.5 * (uT[1] ** 2 + uT[2] ** 2 + uT[3] ** 2) / uT[0])[it].sum()
+
+    x = dth0.clone().requires_grad_(True)
+    torch.autograd.grad(J(x), x)  # warm-up
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    torch.cuda.synchronize()
+    e0.record()
+    j = J(x)
+    e1.record()
+    (grad,) = torch.autograd.grad(j, x)
+    e2.record()
+    torch.cuda.synchronize()
+    fwd_ms, bwd_ms = e0.elapsed_time(e1), e1.elapsed_time(e2)
+    mask = torch.zeros_like(dth0)
+    mask[it] = 1.0
+    gen = torch.Generator(device="cuda").manual_seed(2024)
+    errs = []
+    eps = 1e-3
+    with torch.no_grad():
+        for _ in range(args.adj_dirs):
+            v = torch.randn(dth0.shape, generator=gen, device="cuda", dtype=torch.float64) * mask
+            f = lambda t: float(J(dth0 + t * v))
+            d1 = (f(eps) - f(-eps)) / (2 * eps)
+            d2 = (f(eps / 2) - f(-eps / 2)) / eps
+            fd = (4 * d2 - d1) / 3
+            ad = float((grad * v).sum())
+            errs.append(abs(fd - ad) / max(abs(fd), abs(ad), 1e-300))
+    cells = interior_cells(cfg)
+    line = {
+        "metric": METRIC, "value": cells * 3 * nsteps / (bwd_ms / 1e3) / 1e6, "unit": UNIT,
+        "n_gpus": 1, "steps": nsteps, "warmup": 1, "ms_per_step": bwd_ms / nsteps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "adjoint_bubble_2d_512x256_weno5_hllc_vic3_200steps",
+                   "checkpoint_every": args.adj_every, "objective": "kinetic energy at t_end",
+                   "value_is": "reverse (checkpointed backward) cell-updates per second"},
+        "adjoint": {"forward_ms": fwd_ms, "backward_ms": bwd_ms,
+                    "backward_over_forward": bwd_ms / fwd_ms,
+                    "fd_directions": len(errs), "fd_rel_err_max": max(errs),
+                    "fd_rel_err_median": float(np.median(errs)),
+                    "fd_within_1e-6": int(sum(e < 1e-6 for e in errs)),
+                    "fd": "Richardson-extrapolated central differences, eps = 1e-3 K"},
+        "gpu_launches": None,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -858,6 +947,9 @@ def main():
     ap.add_argument("--acc-steps", type=int, default=5)
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--adj-steps", type=int, default=2)
+    ap.add_argument("--adj-nsteps", type=int, default=200)
+    ap.add_argument("--adj-every", type=int, default=20)
+    ap.add_argument("--adj-dirs", type=int, default=64)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -865,6 +957,8 @@ def main():
         return run_reference(args)
     if args.workload in ("c3", "c3s"):
         return run_ensemble(args)
+    if args.workload == "c4":
+        return run_adjoint_check(args)
     return run_ours(args)
 
 
