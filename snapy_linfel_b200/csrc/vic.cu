@@ -222,11 +222,11 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
 #pragma unroll
     for (int r = 0; r < N; ++r) {
       dp[r] = rhs[r];
-      Sat(i, N * N + r) = rhs[r];
+      __stcs(&Sat(i, N * N + r), rhs[r]);
 #pragma unroll
       for (int q = 0; q < N; ++q) {
         ap[r][q] = c[r][q];
-        Sat(i, r * N + q) = c[r][q];
+        __stcs(&Sat(i, r * N + q), c[r][q]);
       }
     }
 #pragma unroll
@@ -240,7 +240,9 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
 #pragma unroll
     for (int v = 0; v < 5; ++v) wc[v] = wn[v];
   }
-  // back substitution: delta_i -= a'_i delta_{i+1}; B_dry accumulated on the way
+  // back substitution: delta_i -= a'_i delta_{i+1}; B_dry accumulated on the way.
+  // The scratch streams through once each way: streaming loads and stores
+  // (evict-first) keep L1 for the strided state loads of the columns.
   double dn[N];
 #pragma unroll
   for (int r = 0; r < N; ++r) dn[r] = dp[r];
@@ -249,7 +251,7 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
   double sa[N * N + N], du0 = 0.;
   if (nl >= 2) {
 #pragma unroll
-    for (int e = 0; e < N * N + N; ++e) sa[e] = Sat(nl - 2, e);
+    for (int e = 0; e < N * N + N; ++e) sa[e] = __ldcs(&Sat(nl - 2, e));
     du0 = vic_d(b, IDN * sv + cb + nl - 2);
   }
   for (int i = nl - 2; i >= 0; --i) {
@@ -258,7 +260,7 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
     for (int e = 0; e < N * N + N; ++e) cur[e] = sa[e];
     if (i >= 1) {
 #pragma unroll
-      for (int e = 0; e < N * N + N; ++e) sa[e] = Sat(i - 1, e);
+      for (int e = 0; e < N * N + N; ++e) sa[e] = __ldcs(&Sat(i - 1, e));
       du0 = vic_d(b, IDN * sv + cb + i - 1);
     }
     double d[N];
