@@ -944,7 +944,7 @@ def main():
     ap.add_argument("--workload", default="c3")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
-    ap.add_argument("--acc-steps", type=int, default=5)
+    ap.add_argument("--acc-steps", type=int, default=100)
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--adj-steps", type=int, default=2)
     ap.add_argument("--adj-nsteps", type=int, default=200)
