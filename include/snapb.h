@@ -339,6 +339,13 @@ int snapb_hydro_forward_adjoint(const snapb_hydro_config* cfg, const double* dt,
                                 const double* u, const double* g_du, double* g_u,
                                 void* workspace, size_t workspace_bytes, void* stream);
 
+/* Reverse of snapb_riemann for the hydro solvers (nv = 5): given the
+ * cotangent g_flx of the fluxes at every face, writes g_wl = (dF/dwl)^T g_flx
+ * and g_wr = (dF/dwr)^T g_flx (all [5, nc3, nc2, nc1]). */
+int snapb_riemann_adjoint(const snapb_hydro_config* cfg, int solver, int dim,
+                          const double* wl, const double* wr, const double* g_flx,
+                          double* g_wl, double* g_wr, void* stream);
+
 /* Reverse of snapb_bc_apply (out of place): interior cells gather the
  * cotangents of their ghost images (sign flips of reflecting normals for
  * kind != SNAPB_SCALAR), ghost entries of g_out are zero. */

@@ -64,6 +64,7 @@ def lib():
         "snapb_stage_adjoint": (i, [cp, i, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, sz, vp]),
         "snapb_hydro_forward_adjoint": (i, [cp, vp, vp, vp, vp, vp, sz, vp]),
         "snapb_bc_adjoint": (i, [cp, vp, vp, i, i, vp]),
+        "snapb_riemann_adjoint": (i, [cp, i, i, vp, vp, vp, vp, vp, vp]),
         "snapb_ensemble_create": (i, [vp, i, vp, ctypes.POINTER(vp)]),
         "snapb_ensemble_workspace_size": (sz, [vp]),
         "snapb_ensemble_bind": (i, [vp, vp, sz, vp]),
@@ -93,7 +94,8 @@ def exported_symbols():
             "snapb_workspace_size_f32", "snapb_reference_f32", "snapb_to_perturbation",
             "snapb_from_perturbation", "snapb_stage_f32", "snapb_bc_apply_f32",
             "snapb_max_time_step_f32", "snapb_adjoint_workspace_size", "snapb_stage_adjoint",
-            "snapb_hydro_forward_adjoint", "snapb_bc_adjoint", "snapb_ensemble_create",
+            "snapb_hydro_forward_adjoint", "snapb_bc_adjoint", "snapb_riemann_adjoint",
+            "snapb_ensemble_create",
             "snapb_ensemble_workspace_size", "snapb_ensemble_bind", "snapb_ensemble_set_tuning",
             "snapb_ensemble_dt", "snapb_ensemble_max_time_step_f32", "snapb_ensemble_stage_f32",
             "snapb_ensemble_destroy"]

@@ -25,11 +25,12 @@
 //   k_x1_adj        x1 faces of a column in shared memory, gravity, the
 //                   ghost-revision VJP and the U->W VJP into g_u, g_s.
 //
-// Local derivatives: the Riemann solvers, |A|, J and the ghost revision are
-// differentiated with forward-mode dual numbers (dual.cuh) through the very
-// templates the forward kernels use, so every switch (HLLC wave selection, Roe
-// entropy / LLF branches, LMARS upwinding, the pressure clamp) is taken on the
-// branch the forward pass took; WENO5 has a hand-written reverse.  dt is a
+// Local derivatives: the Riemann solvers and WENO5 have hand-written reverses
+// (riemann_adj.cuh, weno5_face_vjp); |A|, J, the other reconstructions and the
+// ghost revision are differentiated with forward-mode dual numbers (dual.cuh)
+// through the very templates the forward kernels use.  Every switch (HLLC wave
+// selection, Roe entropy / LLF branches, LMARS upwinding, the pressure clamp)
+// is taken on the branch the forward pass took.  dt is a
 // constant of the adjoint (the CFL choice is not differentiated).
 //
 // Reference forward path: HydroImpl::forward (src/hydro/hydro_forward.cpp:14-217),
@@ -41,6 +42,7 @@
 
 #include "dual.cuh"
 #include "kernels.cuh"
+#include "riemann_adj.cuh"
 #include "vic_blocks.cuh"
 
 namespace snapb {
@@ -314,28 +316,6 @@ __device__ __forceinline__ void face_states_vjp(int type, bool scale, const doub
   }
 }
 
-// g_F^T dF/d(L, R) of a Riemann flux: ten forward-mode directions
-__device__ __noinline__ void riemann_vjp(int solver, const double* L, const double* R, int ivx,
-                                         double gamma, const double* gF, double* gL, double* gR) {
-#pragma unroll 1
-  for (int k = 0; k < 10; ++k) {
-    Dual Ld[5], Rd[5], Fd[5];
-#pragma unroll
-    for (int v = 0; v < 5; ++v) {
-      Ld[v] = Dual(L[v], k == v ? 1. : 0.);
-      Rd[v] = Dual(R[v], k == 5 + v ? 1. : 0.);
-    }
-    riemann_flux<Dual>(solver, Ld, Rd, ivx, Dual(gamma), Fd);
-    double s = 0.;
-#pragma unroll
-    for (int v = 0; v < 5; ++v) s += gF[v] * Fd[v].d;
-    if (k < 5)
-      gL[k] = s;
-    else
-      gR[k - 5] = s;
-  }
-}
-
 // Reverse of one face: window q (cells f-3 .. f+2) of the nvar primitives and
 // the ns mixing ratios, the cotangent gFin of its nvar + ns fluxes; adds the
 // window cotangents into gq.  rev_l / rev_r: the x1 hydrostatic face
@@ -388,7 +368,7 @@ __device__ __forceinline__ void face_vjp(const Phys& p, int rtype, int rshock, i
         gR[5 + n] = gs * F[IDN];
       }
     }
-    riemann_vjp(p.riemann, L, R, ivx, p.gammad, gF, gL, gR);
+    riemann_vjp_rev(p.riemann, L, R, ivx, p.gammad, gF, gL, gR);
   }
   if (rev_l) {
     gR[IPR] += gL[IPR];
@@ -1283,6 +1263,26 @@ static cudaError_t launch_vic_adj_ns(const Geo& g, const Phys& p, const AdjBufs&
   return launch_vic_adj_n<3, NS>(g, p, b, st);
 }
 
+// reverse of snapb_riemann's hydro solvers, one thread per face
+__global__ void k_riemann_adj(int64_t n, int solver, int ivx, double gamma, const double* wl,
+                              const double* wr, const double* gflx, double* gwl, double* gwr) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  double L[5], R[5], gF[5], gL[5] = {0., 0., 0., 0., 0.}, gR[5] = {0., 0., 0., 0., 0.};
+#pragma unroll
+  for (int v = 0; v < 5; ++v) {
+    L[v] = wl[v * n + t];
+    R[v] = wr[v * n + t];
+    gF[v] = gflx[v * n + t];
+  }
+  riemann_vjp_rev(solver, L, R, ivx, gamma, gF, gL, gR);
+#pragma unroll
+  for (int v = 0; v < 5; ++v) {
+    gwl[v * n + t] = gL[v];
+    gwr[v * n + t] = gR[v];
+  }
+}
+
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
@@ -1542,6 +1542,20 @@ int snapb_hydro_forward_adjoint(const snapb_hydro_config* cfg, const double* dt,
   k_mask_interior<<<(unsigned)((g.sv + 255) / 256), 256, 0, st>>>(g, g_du, ab.GD, 5);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_rc(e, "hydro_forward_adjoint mask");
   return reverse_core(cfg, g, p, dt, u, nullptr, ab, st, "hydro_forward_adjoint");
+}
+
+int snapb_riemann_adjoint(const snapb_hydro_config* cfg, int solver, int dim, const double* wl,
+                          const double* wr, const double* g_flx, double* g_wl, double* g_wr,
+                          void* stream) {
+  if (const char* e = internal_check_config(cfg))
+    return internal_fail(SNAPB_ERR_ARG, std::string("riemann_adjoint: ") + e);
+  if (dim < 1 || dim > 3 || !wl || !wr || !g_flx || !g_wl || !g_wr ||
+      solver < SNAPB_RIEMANN_ROE || solver > SNAPB_RIEMANN_HLLC)
+    return internal_fail(SNAPB_ERR_ARG, "riemann_adjoint: bad arguments (hydro solvers only)");
+  Geo g = make_geo(*cfg);
+  k_riemann_adj<<<(unsigned)((g.sv + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+      g.sv, solver, IPR - dim, cfg->gammad, wl, wr, g_flx, g_wl, g_wr);
+  return cuda_rc(cudaGetLastError(), "riemann_adjoint");
 }
 
 int snapb_bc_adjoint(const snapb_hydro_config* cfg, const double* g_in, double* g_out, int nv,

@@ -305,3 +305,63 @@ def test_rollout_gradient_fd(L):
         with torch.no_grad():
             fd = richardson(lambda t: float(J(dth0 + t * v)), 1e-3)
         check(fd, dot(grad, v), f"rollout trial {trial}")
+
+
+def _face_states(cfg, regime, dim, gen):
+    """random left/right primitive states on every face of the array"""
+    shape = cfg.shape
+    u = lambda lo, hi: lo + (hi - lo) * torch.rand(shape[1:], generator=gen, device="cuda",
+                                                   dtype=torch.float64)
+    ivx = 4 - dim
+    wl = torch.empty(shape, dtype=torch.float64, device="cuda")
+    wr = torch.empty_like(wl)
+    for w in (wl, wr):
+        w[0] = u(0.5, 2.0)
+        w[4] = u(0.5, 2.0)
+        for v in (1, 2, 3):
+            w[v] = u(-0.5, 0.5)
+    if regime == "smooth":
+        wr.copy_(wl * (1.0 + 0.1 * (torch.rand(shape, generator=gen, device="cuda",
+                                               dtype=torch.float64) - 0.5)))
+    elif regime == "supersonic":  # every wave one way: upwind / one-sided branches
+        wl[ivx] = u(2.5, 4.0)
+        wr[ivx] = u(2.5, 4.0)
+        half = shape[1] // 2
+        wl[ivx][:half] *= -1.0
+        wr[ivx][:half] *= -1.0
+    else:  # strong rarefaction and pressure jumps: Roe's LLF fallback, shocked PVRS
+        wl[ivx] = u(-4.0, -2.0)
+        wr[ivx] = u(2.0, 4.0)
+        wr[4] = wr[4] * 10.0
+    return wl, wr
+
+
+@pytest.mark.parametrize("regime", ["smooth", "supersonic", "strong"])
+@pytest.mark.parametrize("dim", [3, 2, 1])
+@pytest.mark.parametrize("solver", ["hllc", "lmars", "roe"])
+def test_riemann_adjoint_fd(L, solver, dim, regime):
+    """the hand-written reverse of each Riemann solver (snapb_riemann_adjoint)
+    against central differences of snapb_riemann, in every branch regime"""
+    from snapy_linfel_b200.config import RIEMANN
+
+    cfg = make_config(nx1=8, nx2=8, nx3=8, gammad=1.4)
+    sid = RIEMANN[solver]
+    gen = torch.Generator(device="cuda").manual_seed(100 + 10 * dim + len(regime))
+    wl, wr = _face_states(cfg, regime, dim, gen)
+    flx = torch.empty_like(wl)
+
+    def F(a, b):
+        L.check(L.lib().snapb_riemann(ctypes.byref(cfg), sid, dim, L.ptr(a), L.ptr(b), 5,
+                                      L.ptr(flx), None, None, L.stream_ptr()), "riemann")
+        return flx.clone()
+
+    g = torch.randn(wl.shape, generator=gen, device="cuda", dtype=torch.float64)
+    gwl, gwr = torch.empty_like(wl), torch.empty_like(wr)
+    L.check(L.lib().snapb_riemann_adjoint(ctypes.byref(cfg), sid, dim, L.ptr(wl), L.ptr(wr),
+                                          L.ptr(g), L.ptr(gwl), L.ptr(gwr), L.stream_ptr()),
+            "riemann_adjoint")
+    for trial in range(2):
+        vl = torch.randn(wl.shape, generator=gen, device="cuda", dtype=torch.float64) * wl.abs()
+        vr = torch.randn(wr.shape, generator=gen, device="cuda", dtype=torch.float64) * wr.abs()
+        fd = richardson(lambda t: dot(g, F(wl + t * vl, wr + t * vr)), 2e-7)
+        check(fd, dot(gwl, vl) + dot(gwr, vr), f"{solver} dim {dim} {regime} trial {trial}")
