@@ -140,3 +140,29 @@ def test_implicit_scheme_bits():
     # scheme 1 -> 3x3 partial blocks, 9 -> 5x5 full blocks
     for s, n in ((1, 3), (9, 5)):
         assert (5 if (s >> 3) & 1 else 3) == n
+
+
+def test_ensemble_structs_match_c():
+    from snapy_linfel_b200.ensemble import MemberF32, Tuning
+
+    src = f"""
+#include <stdio.h>
+#include <stddef.h>
+#include "{HEADER}"
+int main() {{
+  printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(snapb_member_f32),
+         offsetof(snapb_member_f32, u), offsetof(snapb_member_f32, workspace),
+         offsetof(snapb_member_f32, workspace_bytes), sizeof(snapb_ensemble_tuning),
+         offsetof(snapb_ensemble_tuning, vic_regs));
+  return 0;
+}}"""
+    d = os.path.join(REPO, "_work")
+    os.makedirs(d, exist_ok=True)
+    c_path = os.path.join(d, "layout_ens.c")
+    exe = os.path.join(d, "layout_ens")
+    open(c_path, "w").write(src)
+    subprocess.run(["gcc", c_path, "-o", exe], check=True)
+    vals = list(map(int, subprocess.run([exe], capture_output=True, text=True).stdout.split()))
+    py = [ctypes.sizeof(MemberF32), MemberF32.u.offset, MemberF32.workspace.offset,
+          MemberF32.workspace_bytes.offset, ctypes.sizeof(Tuning), Tuning.vic_regs.offset]
+    assert vals == py
