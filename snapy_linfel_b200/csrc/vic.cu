@@ -126,6 +126,47 @@ __device__ __forceinline__ double vic_full_rho(const StageBufs32& b, double u_rh
   return u_rho + b.rb[xi];
 }
 
+// Block construction per form: the FP64 plain form in FP64; the FP32
+// perturbation form forms |A| and J in FP32 from the full states (only the
+// elimination and the balance terms stay FP64 there) and widens them.
+template <int N>
+__device__ __forceinline__ void absA_of(const StageBufs&, double gm1, const double* wl,
+                                        const double* wr, double (&A)[N][N]) {
+  absA_block<N>(gm1, wl, wr, A);
+}
+template <int N>
+__device__ __forceinline__ void jac_of(const StageBufs&, double gm1, const double* w,
+                                       double (&J)[N][N]) {
+  jac_block<N>(gm1, w, J);
+}
+template <int N>
+__device__ __forceinline__ void absA_of(const StageBufs32&, double gm1, const double* wl,
+                                        const double* wr, double (&A)[N][N]) {
+  float fl[5], fr[5], F[N][N];
+#pragma unroll
+  for (int v = 0; v < 5; ++v) {
+    fl[v] = (float)wl[v];
+    fr[v] = (float)wr[v];
+  }
+  absA_block<N, float>((float)gm1, fl, fr, F);
+#pragma unroll
+  for (int r = 0; r < N; ++r)
+#pragma unroll
+    for (int q = 0; q < N; ++q) A[r][q] = (double)F[r][q];
+}
+template <int N>
+__device__ __forceinline__ void jac_of(const StageBufs32&, double gm1, const double* w,
+                                       double (&J)[N][N]) {
+  float fw[5], F[N][N];
+#pragma unroll
+  for (int v = 0; v < 5; ++v) fw[v] = (float)w[v];
+  jac_block<N, float>((float)gm1, fw, F);
+#pragma unroll
+  for (int r = 0; r < N; ++r)
+#pragma unroll
+    for (int q = 0; q < N; ++q) J[r][q] = (double)F[r][q];
+}
+
 // (1) one thread per column: blocks formed a layer ahead of the
 // block-Thomas elimination, back substitution and the column sums.  Loads of
 // a layer's w and du go 32 columns apart across a warp; the next layers of
@@ -152,10 +193,10 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
   double wc[5], wn[5], wq[5], dq[N];
   double Am[N][N], Jp[N][N], Jc[N][N], ap[N][N], dp[N];
   load_w(-1, wn);
-  jac_block<N>(gm1c, wn, Jp);
+  jac_of<N>(b, gm1c, wn, Jp);
   load_w(0, wc);
-  absA_block<N>(gm1f, wn, wc, Am);
-  jac_block<N>(gm1c, wc, Jc);
+  absA_of<N>(b, gm1f, wn, wc, Am);
+  jac_of<N>(b, gm1c, wc, Jc);
   // the next layer's loads are issued one iteration ahead of their use
   load_w(1, wq);
 #pragma unroll
@@ -172,8 +213,8 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
 #pragma unroll
       for (int r = 0; r < N; ++r) dq[r] = vic_d(b, sel<N>(r) * sv + cb + i + 1);
     }
-    absA_block<N>(gm1f, wc, wn, Ap);
-    jac_block<N>(gm1c, wn, Jn);
+    absA_of<N>(b, gm1f, wc, wn, Ap);
+    jac_of<N>(b, gm1c, wn, Jn);
     double ai = wc[IDN] * V;
     sum_a2 += ai * ai;
     double a[N][N], bb[N][N], c[N][N];
