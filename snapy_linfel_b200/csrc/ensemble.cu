@@ -179,8 +179,13 @@ int plan(snapb_ensemble* e) {
                          ? ((ncolv + kVicFinishCols - 1) / kVicFinishCols) *
                                ((g.nx1 + kVicFinishLayers - 1) / kVicFinishLayers)
                          : 0;
-    tiles[PH_BCU] = (ncol1 + 7) / 8;  // 8 x1 rows per tile, one warp each
-    tiles[PH_BCS] = e->p.nscalar ? (ncol1 + 7) / 8 : 0;
+    // ghost-shell cells, 256 per tile (same count as bc_shell_slots)
+    const int64_t nj = g.ju - g.jl + 1, nk = g.ku - g.kl + 1;
+    const int64_t shell = (g.nc1 > 1 ? nj * nk * 2 * g.ng : 0) +
+                          ((g.nc3 > 1 ? (int64_t)2 * g.ng * g.nc2 : 0) +
+                           (g.nc2 > 1 ? nk * 2 * g.ng : 0)) * g.nc1;
+    tiles[PH_BCU] = (shell + 255) / 256;
+    tiles[PH_BCS] = e->p.nscalar ? (shell + 255) / 256 : 0;
     int64_t ncell = (int64_t)(g.iu - g.il + 1) * (g.ju - g.jl + 1) * (g.ku - g.kl + 1);
     tiles[PH_CFL] = (ncell + 1023) / 1024;
     for (int ph = 0; ph < PH_COUNT; ++ph) e->prefix[ph][m + 1] = e->prefix[ph][m] + tiles[ph];

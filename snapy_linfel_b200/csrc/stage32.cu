@@ -620,38 +620,64 @@ __global__ void __launch_bounds__(128, 6) k_march32_batch(const Member32* __rest
   }
 }
 
-// boundary fill over x1 rows (k, j): one warp per row; rows inside the x2/x3
-// interior only fill their x1 ghosts, ghost rows fill every cell
+// boundary fill over the ghost shell only, one thread per ghost cell:
+// slots [0, A) are the x1 ghosts of rows inside the x2/x3 interior
+// (2 ng per row), slots [A, A + B) the cells of the ghost rows (x3-ghost slabs
+// first, then the x2-ghost strips of interior x3 planes)
+__device__ __forceinline__ int64_t bc_shell_slots(const Geo& g) {
+  const int64_t nj = g.ju - g.jl + 1, nk = g.ku - g.kl + 1;
+  const int64_t A = g.nc1 > 1 ? nj * nk * 2 * g.ng : 0;
+  const int64_t c1 = g.nc3 > 1 ? (int64_t)2 * g.ng * g.nc2 : 0;
+  const int64_t c2 = g.nc2 > 1 ? nk * 2 * g.ng : 0;
+  return A + (c1 + c2) * g.nc1;
+}
+
+__device__ __forceinline__ int64_t bc_shell_cell(const Geo& g, int64_t s) {
+  const int64_t nj = g.ju - g.jl + 1, nk = g.ku - g.kl + 1;
+  const int ng2 = 2 * g.ng;
+  const int64_t A = g.nc1 > 1 ? nj * nk * ng2 : 0;
+  int i, j, k;
+  if (s < A) {
+    const int c = (int)(s % ng2);
+    const int64_t row = s / ng2;
+    i = c < g.ng ? c : g.nc1 - ng2 + c;
+    j = g.jl + (int)(row % nj);
+    k = g.kl + (int)(row / nj);
+  } else {
+    s -= A;
+    i = (int)(s % g.nc1);
+    int64_t row = s / g.nc1;
+    const int64_t c1 = g.nc3 > 1 ? (int64_t)ng2 * g.nc2 : 0;
+    if (row < c1) {
+      j = (int)(row % g.nc2);
+      const int kk = (int)(row / g.nc2);
+      k = kk < g.ng ? kk : g.nc3 - ng2 + kk;
+    } else {
+      row -= c1;
+      const int jj = (int)(row % ng2);
+      j = jj < g.ng ? jj : g.nc2 - ng2 + jj;
+      k = g.kl + (int)(row / ng2);
+    }
+  }
+  return ((int64_t)k * g.nc2 + j) * g.nc1 + i;
+}
+
 __global__ void __launch_bounds__(256) k_bc32_batch(const Member32* __restrict__ mem, Phys p,
                                                     WorkQueue q, int kind, double igm1) {
   int m;
   int64_t tile;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   while (queue_next(q, m, tile)) {
     const Geo& g = mem[m].g;
     const Member32& mb = mem[m];
-    const int64_t row = tile * 8 + warp;
-    if (row >= (int64_t)g.nc2 * g.nc3) continue;
+    const int64_t slot = tile * blockDim.x + threadIdx.x;
+    if (slot >= bc_shell_slots(g)) continue;
     AxisBC32 a1{g.nc1, g.ng, mb.bc[0], mb.bc[1]};
     AxisBC32 a2{g.nc2, g.ng, mb.bc[2], mb.bc[3]};
     AxisBC32 a3{g.nc3, g.ng, mb.bc[4], mb.bc[5]};
     float* var = kind == SNAPB_SCALAR ? mb.b.s : mb.b.u;
     const int nv = kind == SNAPB_SCALAR ? p.nscalar : 5;
-    const int j = (int)(row % g.nc2), k = (int)(row / g.nc2);
-    const bool inner = j >= g.jl && j <= g.ju && k >= g.kl && k <= g.ku;
-    const int64_t base = row * g.nc1;
-    if (inner) {
-      if (g.nc1 > 1)
-        for (int c = lane; c < 2 * g.ng; c += 32) {
-          int i = c < g.ng ? c : g.nc1 - 2 * g.ng + c;
-          bc32_cell(g.nc1, g.nc2, g.nc3, g.sv, a1, a2, a3, var, nv, kind, mb.b.rb, mb.b.pb,
-                    igm1, base + i);
-        }
-    } else {
-      for (int i = lane; i < g.nc1; i += 32)
-        bc32_cell(g.nc1, g.nc2, g.nc3, g.sv, a1, a2, a3, var, nv, kind, mb.b.rb, mb.b.pb, igm1,
-                  base + i);
-    }
+    bc32_cell(g.nc1, g.nc2, g.nc3, g.sv, a1, a2, a3, var, nv, kind, mb.b.rb, mb.b.pb, igm1,
+              bc_shell_cell(g, slot));
   }
 }
 
