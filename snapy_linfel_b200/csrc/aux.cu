@@ -54,7 +54,8 @@ cudaError_t launch_prim2cons(const Geo& g, const Phys& p, const double* w, doubl
 // x3-outer (src/mesh/meshblock.cpp:717-730).  Each fill copies from cells
 // that are interior along its own axis, so the sequence composes per axis:
 // the final value of a cell is var[m3(k)][m2(j)][m1(i)] times the sign flips
-// of the reflecting axes it crossed.  One thread per cell of the ghost shell.
+// of the reflecting axes it crossed.  One thread per cell of the ghost shell
+// (bc_shell_cell enumerates exactly the ghost cells).
 // ---------------------------------------------------------------------------
 struct AxisBC {
   int n, ng, lo_type, hi_type;
@@ -82,10 +83,13 @@ __device__ __forceinline__ int bc_map(const AxisBC& a, int i, bool& flip) {
   return i;
 }
 
-__global__ void k_bc(int nc1, int nc2, int nc3, int64_t sv, AxisBC a1, AxisBC a2, AxisBC a3,
-                     double* var, int nv, int flip_normals) {
-  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= sv) return;
+__global__ void k_bc(Geo g, AxisBC a1, AxisBC a2, AxisBC a3, double* var, int nv,
+                     int flip_normals) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= bc_shell_slots(g)) return;
+  const int nc1 = g.nc1, nc2 = g.nc2;
+  const int64_t sv = g.sv;
+  const int64_t t = bc_shell_cell(g, s);
   int i = (int)(t % nc1);
   int j = (int)((t / nc1) % nc2);
   int k = (int)(t / ((int64_t)nc1 * nc2));
@@ -108,8 +112,9 @@ cudaError_t launch_bc(const Geo& g, const snapb_hydro_config& c, double* var, in
   AxisBC a2{g.nc2, g.ng, c.bc[2], c.bc[3]};
   AxisBC a3{g.nc3, g.ng, c.bc[4], c.bc[5]};
   int flip = (kind == SNAPB_CONSERVED || kind == SNAPB_PRIMITIVE) ? 1 : 0;
-  k_bc<<<(unsigned)((g.sv + 255) / 256), 256, 0, st>>>(g.nc1, g.nc2, g.nc3, g.sv, a1, a2, a3, var,
-                                                       nv, flip);
+  const int64_t n = bc_shell_slots_host(g);
+  if (n == 0) return cudaSuccess;
+  k_bc<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g, a1, a2, a3, var, nv, flip);
   return cudaGetLastError();
 }
 

@@ -100,6 +100,50 @@ inline Phys make_phys(const snapb_hydro_config& c) {
   return p;
 }
 
+// The ghost shell of a block, one slot per ghost cell:
+// slots [0, A) are the x1 ghosts of rows inside the x2/x3 interior
+// (2 ng per row), slots [A, A + B) the cells of the ghost rows (x3-ghost slabs
+// first, then the x2-ghost strips of interior x3 planes)
+__host__ __device__ __forceinline__ int64_t bc_shell_slots(const Geo& g) {
+  const int64_t nj = g.ju - g.jl + 1, nk = g.ku - g.kl + 1;
+  const int64_t A = g.nc1 > 1 ? nj * nk * 2 * g.ng : 0;
+  const int64_t c1 = g.nc3 > 1 ? (int64_t)2 * g.ng * g.nc2 : 0;
+  const int64_t c2 = g.nc2 > 1 ? nk * 2 * g.ng : 0;
+  return A + (c1 + c2) * g.nc1;
+}
+
+__host__ __device__ __forceinline__ int64_t bc_shell_cell(const Geo& g, int64_t s) {
+  const int64_t nj = g.ju - g.jl + 1, nk = g.ku - g.kl + 1;
+  const int ng2 = 2 * g.ng;
+  const int64_t A = g.nc1 > 1 ? nj * nk * ng2 : 0;
+  int i, j, k;
+  if (s < A) {
+    const int c = (int)(s % ng2);
+    const int64_t row = s / ng2;
+    i = c < g.ng ? c : g.nc1 - ng2 + c;
+    j = g.jl + (int)(row % nj);
+    k = g.kl + (int)(row / nj);
+  } else {
+    s -= A;
+    i = (int)(s % g.nc1);
+    int64_t row = s / g.nc1;
+    const int64_t c1 = g.nc3 > 1 ? (int64_t)ng2 * g.nc2 : 0;
+    if (row < c1) {
+      j = (int)(row % g.nc2);
+      const int kk = (int)(row / g.nc2);
+      k = kk < g.ng ? kk : g.nc3 - ng2 + kk;
+    } else {
+      row -= c1;
+      const int jj = (int)(row % ng2);
+      j = jj < g.ng ? jj : g.nc2 - ng2 + jj;
+      k = g.kl + (int)(row / ng2);
+    }
+  }
+  return ((int64_t)k * g.nc2 + j) * g.nc1 + i;
+}
+
+inline int64_t bc_shell_slots_host(const Geo& g) { return bc_shell_slots(g); }
+
 template <class T>
 __host__ __device__ __forceinline__ T sqr(T x) {
   return x * x;

@@ -489,11 +489,12 @@ __device__ __forceinline__ void bc32_cell(int nc1, int nc2, int nc3, int64_t sv,
   }
 }
 
-__global__ void k_bc32(int nc1, int nc2, int nc3, int64_t sv, AxisBC32 a1, AxisBC32 a2,
-                       AxisBC32 a3, float* var, int nv, int kind, const double* rb,
-                       const double* pb, double igm1) {
-  bc32_cell(nc1, nc2, nc3, sv, a1, a2, a3, var, nv, kind, rb, pb, igm1,
-            (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+__global__ void k_bc32(Geo g, AxisBC32 a1, AxisBC32 a2, AxisBC32 a3, float* var, int nv,
+                       int kind, const double* rb, const double* pb, double igm1) {
+  const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= bc_shell_slots(g)) return;
+  bc32_cell(g.nc1, g.nc2, g.nc3, g.sv, a1, a2, a3, var, nv, kind, rb, pb, igm1,
+            bc_shell_cell(g, s));
 }
 
 // conversions between the FP64 state and the FP32 perturbation
@@ -620,48 +621,7 @@ __global__ void __launch_bounds__(128, 6) k_march32_batch(const Member32* __rest
   }
 }
 
-// boundary fill over the ghost shell only, one thread per ghost cell:
-// slots [0, A) are the x1 ghosts of rows inside the x2/x3 interior
-// (2 ng per row), slots [A, A + B) the cells of the ghost rows (x3-ghost slabs
-// first, then the x2-ghost strips of interior x3 planes)
-__device__ __forceinline__ int64_t bc_shell_slots(const Geo& g) {
-  const int64_t nj = g.ju - g.jl + 1, nk = g.ku - g.kl + 1;
-  const int64_t A = g.nc1 > 1 ? nj * nk * 2 * g.ng : 0;
-  const int64_t c1 = g.nc3 > 1 ? (int64_t)2 * g.ng * g.nc2 : 0;
-  const int64_t c2 = g.nc2 > 1 ? nk * 2 * g.ng : 0;
-  return A + (c1 + c2) * g.nc1;
-}
-
-__device__ __forceinline__ int64_t bc_shell_cell(const Geo& g, int64_t s) {
-  const int64_t nj = g.ju - g.jl + 1, nk = g.ku - g.kl + 1;
-  const int ng2 = 2 * g.ng;
-  const int64_t A = g.nc1 > 1 ? nj * nk * ng2 : 0;
-  int i, j, k;
-  if (s < A) {
-    const int c = (int)(s % ng2);
-    const int64_t row = s / ng2;
-    i = c < g.ng ? c : g.nc1 - ng2 + c;
-    j = g.jl + (int)(row % nj);
-    k = g.kl + (int)(row / nj);
-  } else {
-    s -= A;
-    i = (int)(s % g.nc1);
-    int64_t row = s / g.nc1;
-    const int64_t c1 = g.nc3 > 1 ? (int64_t)ng2 * g.nc2 : 0;
-    if (row < c1) {
-      j = (int)(row % g.nc2);
-      const int kk = (int)(row / g.nc2);
-      k = kk < g.ng ? kk : g.nc3 - ng2 + kk;
-    } else {
-      row -= c1;
-      const int jj = (int)(row % ng2);
-      j = jj < g.ng ? jj : g.nc2 - ng2 + jj;
-      k = g.kl + (int)(row / ng2);
-    }
-  }
-  return ((int64_t)k * g.nc2 + j) * g.nc1 + i;
-}
-
+// boundary fill over the ghost shell only (bc_shell_cell, common.cuh)
 __global__ void __launch_bounds__(256) k_bc32_batch(const Member32* __restrict__ mem, Phys p,
                                                     WorkQueue q, int kind, double igm1) {
   int m;
@@ -816,9 +776,10 @@ cudaError_t launch_bc32(const Geo& g, const snapb_hydro_config& c, float* var, i
   AxisBC32 a1{g.nc1, g.ng, c.bc[0], c.bc[1]};
   AxisBC32 a2{g.nc2, g.ng, c.bc[2], c.bc[3]};
   AxisBC32 a3{g.nc3, g.ng, c.bc[4], c.bc[5]};
-  k_bc32<<<(unsigned)((g.sv + 255) / 256), 256, 0, st>>>(g.nc1, g.nc2, g.nc3, g.sv, a1, a2, a3,
-                                                         var, nv, kind, rb, pb,
-                                                         1.0 / (c.gammad - 1.0));
+  const int64_t n = bc_shell_slots_host(g);
+  if (n == 0) return cudaSuccess;
+  k_bc32<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g, a1, a2, a3, var, nv, kind, rb, pb,
+                                                     1.0 / (c.gammad - 1.0));
   return cudaGetLastError();
 }
 
