@@ -149,27 +149,23 @@ __global__ void __launch_bounds__(256) k_x1(Geo g, Phys p, StageBufs b, int C, i
   }
   __syncthreads();
 
-  // (2) isentropic extrapolation of p and rho into the x1 ghosts
-  if (p.grav1 != 0. && tid < C && col0 + tid < ncol) {
-    double* pp = sw + (tid * NV + IPR) * nc1;
-    double* rr = sw + (tid * NV + IDN) * nc1;
+  // (2) isentropic extrapolation of p and rho into the x1 ghosts, one thread
+  // per (column, end)
+  if (p.grav1 != 0. && tid < 2 * C && col0 + (tid >> 1) < ncol) {
+    const int c = tid >> 1, top = tid & 1;
+    double* pp = sw + (c * NV + IPR) * nc1;
+    double* rr = sw + (c * NV + IDN) * nc1;
     const double gamma = p.gammad;
     const double a = (gamma - 1.) / gamma, ig = 1. / gamma, ia = 1. / a;
     const double grav = -p.grav1, dz = g.dx1;
-    const int is = g.il, ie = g.iu;
-    double K = pp[is] / pow(rr[is], gamma);
-    double kg = pow(K, ig);
+    const int e = top ? g.iu : g.il, dir = top ? 1 : -1;
+    const double K = pp[e] / pow(rr[e], gamma);
+    const double kg = pow(K, ig);
     for (int n = 0; n < g.ng; ++n) {
-      double h = pow(pp[is - n], a) + a * grav * dz / kg;
-      pp[is - n - 1] = pow(h, ia);
-      rr[is - n - 1] = pow(pp[is - n - 1] / K, ig);
-    }
-    K = pp[ie] / pow(rr[ie], gamma);
-    kg = pow(K, ig);
-    for (int n = 0; n < g.ng; ++n) {
-      double h = pow(pp[ie + n], a) - a * grav * dz / kg;
-      pp[ie + n + 1] = pow(h, ia);
-      rr[ie + n + 1] = pow(pp[ie + n + 1] / K, ig);
+      double h = top ? pow(pp[e + dir * n], a) - a * grav * dz / kg
+                     : pow(pp[e + dir * n], a) + a * grav * dz / kg;
+      pp[e + dir * (n + 1)] = pow(h, ia);
+      rr[e + dir * (n + 1)] = pow(pp[e + dir * (n + 1)] / K, ig);
     }
   }
   __syncthreads();

@@ -192,36 +192,26 @@ __device__ __forceinline__ void x1_32_tile(const Geo& g, const Phys& p, const St
   }
   __syncthreads();
 
-  // isentropic x1 ghost revision on full values, in FP64
-  if (p.grav1 != 0. && tid < C && col0 + tid < ncol) {
-    float* pp = sw + (tid * NV + IPR) * nc1;
-    float* rr = sw + (tid * NV + IDN) * nc1;
+  // isentropic x1 ghost revision on full values, in FP64; one thread per
+  // (column, end): the two ends of a column are independent
+  if (p.grav1 != 0. && tid < 2 * C && col0 + (tid >> 1) < ncol) {
+    const int c = tid >> 1, top = tid & 1;
+    float* pp = sw + (c * NV + IPR) * nc1;
+    float* rr = sw + (c * NV + IDN) * nc1;
     const double gam = p.gammad;
     const double a = (gam - 1.) / gam, ig = 1. / gam, ia = 1. / a;
     const double grav = -p.grav1, dz = g.dx1;
-    const int is = g.il, ie = g.iu;
-    double ps = b.pb[is] + pp[is], rs = b.rb[is] + rr[is];
-    double K = ps / pow(rs, gam), kg = pow(K, ig);
+    const int e = top ? g.iu : g.il, dir = top ? 1 : -1;
+    const double ps = b.pb[e] + pp[e], rs = b.rb[e] + rr[e];
+    const double K = ps / pow(rs, gam), kg = pow(K, ig);
     double pc = ps;
     for (int n = 0; n < g.ng; ++n) {
-      double h = pow(pc, a) + a * grav * dz / kg;
+      double h = top ? pow(pc, a) - a * grav * dz / kg : pow(pc, a) + a * grav * dz / kg;
       double pn = pow(h, ia);
       double rn = pow(pn / K, ig);
-      pp[is - n - 1] = (float)(pn - b.pb[is - n - 1]);
-      rr[is - n - 1] = (float)(rn - b.rb[is - n - 1]);
-      pc = pn;
-    }
-    ps = b.pb[ie] + pp[ie];
-    rs = b.rb[ie] + rr[ie];
-    K = ps / pow(rs, gam);
-    kg = pow(K, ig);
-    pc = ps;
-    for (int n = 0; n < g.ng; ++n) {
-      double h = pow(pc, a) - a * grav * dz / kg;
-      double pn = pow(h, ia);
-      double rn = pow(pn / K, ig);
-      pp[ie + n + 1] = (float)(pn - b.pb[ie + n + 1]);
-      rr[ie + n + 1] = (float)(rn - b.rb[ie + n + 1]);
+      const int cell = e + dir * (n + 1);
+      pp[cell] = (float)(pn - b.pb[cell]);
+      rr[cell] = (float)(rn - b.rb[cell]);
       pc = pn;
     }
   }
