@@ -192,27 +192,28 @@ __device__ __forceinline__ void x1_32_tile(const Geo& g, const Phys& p, const St
   }
   __syncthreads();
 
-  // isentropic x1 ghost revision on full values, in FP64; one thread per
-  // (column, end): the two ends of a column are independent
-  if (p.grav1 != 0. && tid < 2 * C && col0 + (tid >> 1) < ncol) {
-    const int c = tid >> 1, top = tid & 1;
-    float* pp = sw + (c * NV + IPR) * nc1;
-    float* rr = sw + (c * NV + IDN) * nc1;
-    const double gam = p.gammad;
-    const double a = (gam - 1.) / gam, ig = 1. / gam, ia = 1. / a;
-    const double grav = -p.grav1, dz = g.dx1;
-    const int e = top ? g.iu : g.il, dir = top ? 1 : -1;
-    const double ps = b.pb[e] + pp[e], rs = b.rb[e] + rr[e];
-    const double K = ps / pow(rs, gam), kg = pow(K, ig);
-    double pc = ps;
-    for (int n = 0; n < g.ng; ++n) {
-      double h = top ? pow(pc, a) - a * grav * dz / kg : pow(pc, a) + a * grav * dz / kg;
-      double pn = pow(h, ia);
-      double rn = pow(pn / K, ig);
-      const int cell = e + dir * (n + 1);
+  // isentropic x1 ghost revision on full values, in FP64.  The recurrence
+  // p_{n+1} = (p_n^a + c)^(1/a) has h_n = p_n^a = p_e^a + n c, so every ghost
+  // level is independent: one thread per (column, end, level)
+  if (p.grav1 != 0. && tid < 2 * g.ng * C) {
+    const int c = tid / (2 * g.ng), rest = tid - c * 2 * g.ng;
+    const int top = rest / g.ng, n = rest - top * g.ng;
+    if (col0 + c < ncol) {
+      float* pp = sw + (c * NV + IPR) * nc1;
+      float* rr = sw + (c * NV + IDN) * nc1;
+      const double gam = p.gammad;
+      const double a = (gam - 1.) / gam, ig = 1. / gam, ia = 1. / a;
+      const double grav = -p.grav1, dz = g.dx1;
+      const int e = top ? g.iu : g.il, dir = top ? 1 : -1;
+      const double ps = b.pb[e] + pp[e], rs = b.rb[e] + rr[e];
+      const double K = ps / pow(rs, gam), kg = pow(K, ig);
+      const double step = (top ? -a : a) * grav * dz / kg;
+      const double h = pow(ps, a) + (n + 1) * step;
+      const double pn = pow(h, ia);
+      const double rn = pow(pn / K, ig);
+      const int cell = e + dir * (n + 1);  // ghosts only; the edge cell is never written
       pp[cell] = (float)(pn - b.pb[cell]);
       rr[cell] = (float)(rn - b.rb[cell]);
-      pc = pn;
     }
   }
   __syncthreads();
