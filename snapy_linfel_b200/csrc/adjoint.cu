@@ -395,6 +395,92 @@ __device__ __forceinline__ void face_vjp(const Phys& p, int rtype, int rshock, i
   }
 }
 
+// The same reverse for an x1 face whose window lives in shared memory (wb:
+// the column's NV rows of nc1 cells); the window cotangents are added into the
+// column's shared accumulator gb with shared-memory atomics, so no per-face
+// array of contributions is held in registers.
+template <int NS>
+__device__ __forceinline__ void face_vjp_smem(const Phys& p, int rtype, int rshock, int rscale,
+                                              bool disabled, bool rev_l, bool rev_r,
+                                              const double* wb, int nc1, int f,
+                                              const double (&gFin)[5 + NS], double* gb) {
+  constexpr int NV = 5 + NS;
+  double L[NV], R[NV], Lraw[NV > 5 ? NV : 6], Rraw[NV > 5 ? NV : 6];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    double q[6];
+#pragma unroll
+    for (int t = 0; t < 6; ++t) q[t] = wb[v * nc1 + f - 3 + t];
+    if (v < 5) {
+      int typ = (rshock || v == IDN) ? rtype : interp2_of(rtype);
+      face_states(typ, rscale != 0, q, L[v], R[v]);
+    } else {
+      face_states(p.rs_type, p.rs_scale != 0, q, Lraw[v], Rraw[v]);
+      L[v] = Lraw[v] < 0. ? 0. : Lraw[v];
+      R[v] = Rraw[v] < 0. ? 0. : Rraw[v];
+    }
+  }
+  if (rev_l) {
+    L[IPR] = R[IPR];
+    L[IDN] = R[IDN];
+  }
+  if (rev_r) {
+    R[IPR] = L[IPR];
+    R[IDN] = L[IDN];
+  }
+  double gL[NV], gR[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) gL[v] = gR[v] = 0.;
+  if (!disabled) {
+    double F[5];
+    riemann_flux(p.riemann, L, R, IVX, p.gammad, F);
+    double gF[5];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) gF[v] = gFin[v];
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+      double gs = gFin[5 + n];
+      if (F[IDN] > 0.) {
+        gF[IDN] += gs * L[5 + n];
+        gL[5 + n] = gs * F[IDN];
+      } else {
+        gF[IDN] += gs * R[5 + n];
+        gR[5 + n] = gs * F[IDN];
+      }
+    }
+    riemann_vjp_rev(p.riemann, L, R, IVX, p.gammad, gF, gL, gR);
+  }
+  if (rev_l) {
+    gR[IPR] += gL[IPR];
+    gL[IPR] = 0.;
+    gR[IDN] += gL[IDN];
+    gL[IDN] = 0.;
+  }
+  if (rev_r) {
+    gL[IPR] += gR[IPR];
+    gR[IPR] = 0.;
+    gL[IDN] += gR[IDN];
+    gR[IDN] = 0.;
+  }
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    double q[6], t6[6] = {0., 0., 0., 0., 0., 0.};
+#pragma unroll
+    for (int t = 0; t < 6; ++t) q[t] = wb[v * nc1 + f - 3 + t];
+    if (v < 5) {
+      int typ = (rshock || v == IDN) ? rtype : interp2_of(rtype);
+      face_states_vjp(typ, rscale != 0, q, gL[v], gR[v], t6);
+    } else {
+      double gl = Lraw[v] < 0. ? 0. : gL[v];
+      double gr = Rraw[v] < 0. ? 0. : gR[v];
+      face_states_vjp(p.rs_type, p.rs_scale != 0, q, gl, gr, t6);
+    }
+#pragma unroll
+    for (int t = 0; t < 6; ++t)
+      if (t6[t] != 0.) atomicAdd(gb + v * nc1 + f - 3 + t, t6[t]);
+  }
+}
+
 // Buffers of the stage adjoint (all [var][sv], FP64)
 struct AdjBufs {
   const double* dt;
@@ -513,7 +599,7 @@ __device__ __forceinline__ void revise_end(T P, T Rr, double gamma, double a, do
 }
 
 template <int NS>
-__global__ void __launch_bounds__(256) k_x1_adj(Geo g, Phys p, AdjBufs b, int C) {
+__global__ void __launch_bounds__(256, 2) k_x1_adj(Geo g, Phys p, AdjBufs b, int C) {
   constexpr int NV = 5 + NS;
   extern __shared__ double sm[];
   const int nc1 = g.nc1;
@@ -543,48 +629,24 @@ __global__ void __launch_bounds__(256) k_x1_adj(Geo g, Phys p, AdjBufs b, int C)
   }
   __syncthreads();
 
-  // x1 faces il .. iu+1 of interior columns, contributions added in six
-  // conflict-free phases (phase o: face f adds to cell f-3+o)
+  // x1 faces il .. iu+1 of interior columns; window cotangents accumulate in
+  // shared memory through atomics
   const int nf = g.nx1 + 1;
   const double cf = dt * g.A1 / g.vol;
-  for (int base = 0; base < C * nf; base += nt) {
-    int idx = base + tid;
+  const bool grav = p.grav1 != 0.;
+  for (int idx = tid; idx < C * nf; idx += nt) {
     int c = idx / nf, f = g.il + (idx - c * nf);
     int64_t col = col0 + c;
-    bool act = idx < C * nf && col < ncol;
-    if (act) {
-      int j = (int)(col % g.nc2), k = (int)(col / g.nc2);
-      act = j >= g.jl && j <= g.ju && k >= g.kl && k <= g.ku;
-    }
-    double gq[NV][6];
+    if (col >= ncol) continue;
+    int j = (int)(col % g.nc2), k = (int)(col / g.nc2);
+    if (j < g.jl || j > g.ju || k < g.kl || k > g.ku) continue;
+    int64_t off = col * nc1 + f;
+    double gF[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v)
-#pragma unroll
-      for (int t = 0; t < 6; ++t) gq[v][t] = 0.;
-    if (act) {
-      const double* wb = sw + (size_t)c * NV * nc1;
-      double q[NV][6];
-#pragma unroll
-      for (int v = 0; v < NV; ++v)
-#pragma unroll
-        for (int t = 0; t < 6; ++t) q[v][t] = wb[v * nc1 + f - 3 + t];
-      int64_t off = col * nc1 + f;
-      double gF[NV];
-#pragma unroll
-      for (int v = 0; v < NV; ++v) gF[v] = cf * (b.GD[v * sv + off] - b.GD[v * sv + off - 1]);
-      bool grav = p.grav1 != 0.;
-      face_vjp<NS>(p, p.r1_type, p.r1_shock, p.r1_scale, IVX, p.disable1 != 0,
-                   grav && f == g.il, grav && f == g.iu + 1, q, gF, gq);
-    }
-#pragma unroll
-    for (int o = 0; o < 6; ++o) {
-      __syncthreads();
-      if (act) {
-        double* gb = sg + (size_t)c * NV * nc1 + f - 3 + o;
-#pragma unroll
-        for (int v = 0; v < NV; ++v) gb[v * nc1] += gq[v][o];
-      }
-    }
+    for (int v = 0; v < NV; ++v) gF[v] = cf * (b.GD[v * sv + off] - b.GD[v * sv + off - 1]);
+    face_vjp_smem<NS>(p, p.r1_type, p.r1_shock, p.r1_scale, p.disable1 != 0, grav && f == g.il,
+                      grav && f == g.iu + 1, sw + (size_t)c * NV * nc1, nc1, f, gF,
+                      sg + (size_t)c * NV * nc1);
   }
   __syncthreads();
 
@@ -1315,7 +1377,7 @@ static cudaError_t launch_sweeps_adj_ns(const Geo& g, const Phys& p, const AdjBu
   if (a1) {
     const int nv = 5 + NS;
     size_t per = (size_t)2 * nv * g.nc1 * sizeof(double);
-    int C = (int)std::max<size_t>(1, (64 * 1024) / per);
+    int C = (int)std::max<size_t>(1, (48 * 1024) / per);
     C = std::min(C, 8);
     size_t smem = per * C;
     cudaFuncSetAttribute(k_x1_adj<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
