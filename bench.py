@@ -509,10 +509,9 @@ def run_ensemble(args):
         torch.cuda.synchronize()
 
     def max_ms(ms):
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return t.item()
+        from snapy_linfel_b200.replicas import max_over_ranks
+
+        return max_over_ranks(ms, dev)
 
     members = problems.ensemble_members(n=48, seed=2024)
     if args.workload == "c3s":  # a quarter of the ensemble, for profiling captures
