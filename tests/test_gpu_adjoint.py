@@ -261,6 +261,65 @@ def test_stage_adjoint_fd(L, name, stage):
         check(fd, ad, f"{name} stage {stage} trial {trial}")
 
 
+AUTOGRAD_CONFIGS = {
+    "col2d_lmars_vic3": CONFIGS["col2d_lmars_vic3"],
+    "sod1d_weno5shock_hllc": CONFIGS["sod1d_weno5shock_hllc"],
+    "box3d_hllc_vic3": dict(
+        cfg=dict(nx1=10, nx2=6, nx3=6, x1=(0.0, 1000.0), x2=(0.0, 600.0), x3=(0.0, 600.0),
+                 gammad=1004.0 / 717.0, rgas=287.0, riemann="hllc", implicit_scheme=1,
+                 grav=(-9.81, 0.0, 0.0),
+                 bc=("reflecting", "reflecting", "periodic", "periodic", "outflow",
+                     "outflow")), grav=True),
+    "box3d_roe_cp5": dict(
+        cfg=dict(nx1=8, nx2=6, nx3=5, recon23="cp5", riemann="roe",
+                 bc=("outflow", "reflecting", "periodic", "periodic", "outflow",
+                     "reflecting")), grav=False),
+}
+
+
+@pytest.mark.parametrize("stage", [0, 1, 2])
+@pytest.mark.parametrize("name", list(AUTOGRAD_CONFIGS))
+def test_stage_adjoint_matches_torch_autograd(L, name, stage):
+    """the hand-written reverse of one stage against torch autograd through
+    the torch restatement of the same stage (pinned to the C++ oracle on the
+    CPU): every entry of d<g, stage(u, u0)>/du and /du0, ghosts included.
+    Bound: 1e-6 of each variable's largest gradient entry."""
+    from oracle import torch_step
+
+    from snapy_linfel_b200.adjoint import Adjoint
+
+    spec = AUTOGRAD_CONFIGS[name]
+    cfg = make_config(**spec["cfg"])
+    w, _ = make_state(cfg, 31 + stage, spec["grav"])
+    mb = block(cfg, w, None)
+    u = mb.hydro_u.clone()
+    u0 = u.clone()
+    if stage:
+        w0, _ = make_state(cfg, 77, spec["grav"])
+        u0 = block(cfg, w0, None).hydro_u.clone()
+    dt = mb.max_time_step().clone() * 0.5
+    gen = torch.Generator(device="cuda").manual_seed(41 + stage)
+    gout = torch.randn(u.shape, generator=gen, device="cuda", dtype=torch.float64) / scales(u)
+
+    adj = Adjoint(cfg)
+    gu0 = torch.zeros_like(u)
+    gu, _ = adj.stage(stage, dt, u, None, gout, None, gu0, None)
+    torch.cuda.synchronize()
+
+    ut = u.clone().requires_grad_(True)
+    u0t = ut if stage == 0 else u0.clone().requires_grad_(True)
+    out = torch_step.stage(ut, u0t, stage, float(dt.reshape(-1)[0]), cfg)
+    (out * gout).sum().backward()
+    pairs = [("u", gu + gu0 if stage == 0 else gu, ut.grad)]
+    if stage:
+        pairs.append(("u0", gu0, u0t.grad))
+    for what, got, want in pairs:
+        for v in range(5):
+            scale = float(want[v].abs().max())
+            err = float((got[v] - want[v]).abs().max()) / max(scale, 1e-300)
+            assert err < TOL, f"{name} stage {stage} d/d{what}[{v}]: rel {err:.2e}"
+
+
 def test_rollout_gradient_fd(L):
     """J = kinetic energy after 6 RK3 steps (checkpoints every 2 steps) of a
     warm bubble, gradient wrt the initial potential-temperature perturbation
