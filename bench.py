@@ -585,6 +585,9 @@ def run_ensemble(args):
     ens.restore(init32)
     for (opts, w, r), mb in zip(members, blocks):
         mb.initialize(w, r)
+    # domain-total mass per member (compensated device sums), both forms
+    mass0_32 = [float(b.totals()[0]) for b in ens.blocks]
+    mass0_64 = [float(b.totals()[0]) for b in blocks]
     for _ in range(args.acc_steps):
         ens.max_time_step()
         dts = ens.dts().clone()
@@ -611,9 +614,12 @@ def run_ensemble(args):
             den[k] += float(y.abs().sum())
             emax[k] = max(emax[k], float(d.max()))
             vmax[k] = max(vmax[k], float(y.abs().max()))
+    drift32 = max(abs(float(b.totals()[0]) / m - 1.0) for b, m in zip(ens.blocks, mass0_32))
+    drift64 = max(abs(float(b.totals()[0]) / m - 1.0) for b, m in zip(blocks, mass0_64))
     acc = {"steps": args.acc_steps, "fields": names,
            "rel_l1": [float(n / max(d, 1e-300)) for n, d in zip(num, den)],
-           "linf": [float(e / max(v, 1e-300)) for e, v in zip(emax, vmax)]}
+           "linf": [float(e / max(v, 1e-300)) for e, v in zip(emax, vmax)],
+           "mass_drift_max_member": {"fp32_form": drift32, "fp64_form": drift64}}
     del blocks
     torch.cuda.empty_cache()
 

@@ -352,6 +352,24 @@ int snapb_riemann_adjoint(const snapb_hydro_config* cfg, int solver, int dim,
 int snapb_bc_adjoint(const snapb_hydro_config* cfg, const double* g_in, double* g_out, int nv,
                      int kind, void* stream);
 
+/* ---- conserved totals (compensated) ----
+ * out[v] = cell volume * sum over interior cells of var[v], v < nv, written
+ * to DEVICE memory.  Replaces the torch sum of hydro_u * cell_volume over the
+ * interior that MeshBlockImpl reports as "mass0"
+ * (src/mesh/meshblock.cpp:855-870).  Accumulated as double-double sums in
+ * an order fixed by the configuration: the exact total rounded once (to
+ * ~2^-100 of the largest partial sum), bit-identical across calls.
+ * snapb_conserved_totals_f32 takes the FP32 perturbation form's conserved
+ * u' and adds the FP64 reference of the workspace (snapb_reference_f32)
+ * back cell by cell, so its totals are of the full state; nv <= nvar.
+ * scratch: snapb_totals_scratch_size(cfg, nv) bytes of device memory. */
+size_t snapb_totals_scratch_size(const snapb_hydro_config* cfg, int nv);
+int snapb_conserved_totals(const snapb_hydro_config* cfg, const double* var, int nv,
+                           double* out, void* scratch, size_t scratch_bytes, void* stream);
+int snapb_conserved_totals_f32(const snapb_hydro_config* cfg, const float* u, int nv,
+                               double* out, const void* workspace, size_t workspace_bytes,
+                               void* scratch, size_t scratch_bytes, void* stream);
+
 /* ---- diagnostics: per-kernel device time ----
  * While enabled, snapb_stage, snapb_hydro_forward, snapb_stage_f32 and the
  * adjoint entry points record a CUDA event pair around every kernel (or

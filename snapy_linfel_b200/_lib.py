@@ -73,6 +73,9 @@ def lib():
         "snapb_ensemble_max_time_step_f32": (i, [vp, d, vp]),
         "snapb_ensemble_stage_f32": (i, [vp, i, vp]),
         "snapb_ensemble_destroy": (None, [vp]),
+        "snapb_totals_scratch_size": (sz, [cp, i]),
+        "snapb_conserved_totals": (i, [cp, vp, i, vp, vp, sz, vp]),
+        "snapb_conserved_totals_f32": (i, [cp, vp, i, vp, vp, sz, vp, sz, vp]),
         "snapb_timing_enable": (i, [i]),
         "snapb_timing_query": (i, [i, ctypes.POINTER(d), ctypes.POINTER(i)]),
     }
@@ -98,7 +101,8 @@ def exported_symbols():
             "snapb_ensemble_create",
             "snapb_ensemble_workspace_size", "snapb_ensemble_bind", "snapb_ensemble_set_tuning",
             "snapb_ensemble_dt", "snapb_ensemble_max_time_step_f32", "snapb_ensemble_stage_f32",
-            "snapb_ensemble_destroy"]
+            "snapb_ensemble_destroy", "snapb_totals_scratch_size", "snapb_conserved_totals",
+            "snapb_conserved_totals_f32"]
 
 
 KERNELS = {"x1_sweep": 0, "diffusion": 1, "x2_sweep": 2, "x3_sweep": 3, "finalize": 4,

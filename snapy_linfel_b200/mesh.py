@@ -17,6 +17,23 @@ from . import _lib
 from .config import CONSERVED, PRIMITIVE, SCALAR, HydroConfig, MeshBlockOptions
 
 
+def conserved_totals(cfg, var, stream=None):
+    """Compensated interior totals of var [nv, nc3, nc2, nc1] (FP64, device)
+    times the cell volume, as a [nv] FP64 device tensor."""
+    import torch
+
+    L = _lib.lib()
+    nv = int(var.shape[0])
+    nb = L.snapb_totals_scratch_size(ctypes.byref(cfg), nv)
+    scratch = torch.empty(nb, dtype=torch.uint8, device=var.device)
+    out = torch.empty(nv, dtype=torch.float64, device=var.device)
+    _lib.check(L.snapb_conserved_totals(ctypes.byref(cfg), _lib.ptr(var), nv, _lib.ptr(out),
+                                        _lib.ptr(scratch), ctypes.c_size_t(nb),
+                                        stream if stream is not None else _lib.stream_ptr()),
+               "snapb_conserved_totals")
+    return out
+
+
 class MeshBlock:
     def __init__(self, options: MeshBlockOptions | HydroConfig, device=None):
         import torch
@@ -150,8 +167,10 @@ class MeshBlock:
         return t[(slice(None),) + self.cfg.interior()]
 
     def totals(self):
-        """Domain totals of the conserved variables (mass0, ..., energy)."""
-        return self.interior(self.hydro_u).sum(dim=(1, 2, 3))
+        """Domain totals of hydro_u * cell volume over the interior (mass0,
+        momenta, energy; src/mesh/meshblock.cpp:855-870), compensated sums on
+        the device: a [nvar] FP64 device tensor."""
+        return conserved_totals(self.cfg, self.hydro_u, self._stream())
 
 
 class MeshBlockF32:
@@ -276,6 +295,23 @@ class MeshBlockF32:
         for s in range(3):
             self.forward(s)
         self.cycle += 1
+
+    def totals(self):
+        """Domain totals of the full conserved state (u_bar + u') * cell volume
+        over the interior, compensated sums of the FP32 perturbations plus
+        the FP64 reference: a [nvar] FP64 device tensor."""
+        import torch
+
+        c = self.cfg
+        L = _lib.lib()
+        nb = L.snapb_totals_scratch_size(ctypes.byref(c), c.nvar)
+        scratch = torch.empty(nb, dtype=torch.uint8, device=self.device)
+        out = torch.empty(c.nvar, dtype=torch.float64, device=self.device)
+        ws, wb = self._ws()
+        self._call("snapb_conserved_totals_f32", ctypes.byref(c), _lib.ptr(self.hydro_u),
+                   c.nvar, _lib.ptr(out), ws, wb, _lib.ptr(scratch), ctypes.c_size_t(nb),
+                   _lib.stream_ptr())
+        return out
 
     def state64(self):
         """FP64 conserved state u = u_bar + u'."""
