@@ -58,6 +58,45 @@ size_t vic_scratch_bytes(const Geo& g, const Phys& p) {
 constexpr int kTC = 32;  // columns per tile
 constexpr int kTL = 32;  // layers per tile (redistribution)
 
+// Back substitution: the reduced block, partial solution and du[IDN] of a
+// layer are fetched kBackDepth<N> layers ahead into a per-thread ring in
+// shared memory by asynchronous copies (cp.async), so the short recurrence
+// does not wait a memory latency per layer and holds no extra registers.
+// Ring layout [slot][element][thread] (element ES = du[IDN]), doubles.
+constexpr int kFwdDepth = 4;  // layers of the forward sweep in flight
+
+template <int N>
+struct BackRing {
+  static constexpr int depth = N == 3 ? 6 : 2;
+  static constexpr int elems = N * N + N + 1;
+};
+template <int N>
+constexpr size_t back_ring_bytes(int threads) {
+  return (size_t)threads * BackRing<N>::depth * BackRing<N>::elems * sizeof(double);
+}
+
+__device__ __forceinline__ void cp_async_bytes8(void* smem, const void* gmem) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_bytes4(void* smem, const void* gmem) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int n>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_elem(void* smem, const double* g) { cp_async_bytes8(smem, g); }
+__device__ __forceinline__ void cp_async_elem(void* smem, const float* g) { cp_async_bytes4(smem, g); }
+__device__ __forceinline__ double ring_elem(const double* slot, const double*) { return *slot; }
+__device__ __forceinline__ double ring_elem(const double* slot, const float*) {
+  return (double)*reinterpret_cast<const float*>(slot);
+}
+
 // (k, j, il) offset of interior column `col`
 __device__ __forceinline__ int64_t column_base(const Geo& g, int64_t col) {
   const int nj = g.ju - g.jl + 1;
@@ -74,6 +113,13 @@ __device__ __forceinline__ double vic_w(const StageBufs& b, int64_t sv, int v, i
 __device__ __forceinline__ double vic_w(const StageBufs32& b, int64_t sv, int v, int64_t off,
                                         int xi) {
   double x = (double)b.w[v * sv + off];
+  if (v == IDN) x += b.rb[xi];
+  if (v == IPR) x += b.pb[xi];
+  return x;
+}
+// full primitive of variable v at x1 index xi from a stored value x
+__device__ __forceinline__ double vic_full(const StageBufs&, double x, int v, int xi) { return x; }
+__device__ __forceinline__ double vic_full(const StageBufs32& b, double x, int v, int xi) {
   if (v == IDN) x += b.rb[xi];
   if (v == IPR) x += b.pb[xi];
   return x;
@@ -190,29 +236,42 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
   const double gm1f = 0.5 * (p.gammad + p.gammad) - 1.;
   const double dt = *b.dt;
   const double Aa = g.A1, hiv = 0.5 / g.vol, idt = 1. / dt, grav = p.grav1, V = g.vol;
-  double wc[5], wn[5], wq[5], dq[N];
+  // Forward sweep inputs (w of cell L and the rows of du at layer L-1,
+  // 1 <= L <= nl) arrive kFwdDepth layers ahead through the same per-thread
+  // shared-memory ring as the back substitution, layout [slot][element][thread].
+  constexpr int DF = kFwdDepth, FE = 5 + N;
+  static_assert(DF * FE <= BackRing<N>::depth * BackRing<N>::elems, "ring too small");
+  extern __shared__ double vic_ring[];
+  const int nt = blockDim.x, lane = threadIdx.x;
+  auto fring = [&](int slot, int e) { return vic_ring + ((size_t)(slot * FE + e) * nt + lane); };
+  auto ffetch = [&](int L, int slot) {
+    if (L <= nl) {
+#pragma unroll
+      for (int v = 0; v < 5; ++v) cp_async_elem(fring(slot, v), b.w + v * sv + cb + L);
+#pragma unroll
+      for (int r = 0; r < N; ++r)
+        cp_async_elem(fring(slot, 5 + r), b.D + sel<N>(r) * sv + cb + L - 1);
+    }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int k = 0; k < DF; ++k) ffetch(1 + k, k);
+  double wc[5], wn[5];
   double Am[N][N], Jp[N][N], Jc[N][N], ap[N][N], dp[N];
   load_w(-1, wn);
   jac_of<N>(b, gm1c, wn, Jp);
   load_w(0, wc);
   absA_of<N>(b, gm1f, wn, wc, Am);
   jac_of<N>(b, gm1c, wc, Jc);
-  // the next layer's loads are issued one iteration ahead of their use
-  load_w(1, wq);
-#pragma unroll
-  for (int r = 0; r < N; ++r) dq[r] = vic_d(b, sel<N>(r) * sv + cb);
   double sum_a2 = 0.;
-  for (int i = 0; i < nl; ++i) {
+  for (int i = 0, fslot = 0; i < nl; ++i) {
     double Ap[N][N], Jn[N][N], rhs[N];
+    cp_async_wait<DF - 1>();  // the group of cell i+1 has landed
 #pragma unroll
-    for (int v = 0; v < 5; ++v) wn[v] = wq[v];  // cell i+1 (the ghost cell nl at the top)
+    for (int v = 0; v < 5; ++v)  // cell i+1 (the ghost cell nl at the top)
+      wn[v] = vic_full(b, ring_elem(fring(fslot, v), b.w), v, g.il + i + 1);
 #pragma unroll
-    for (int r = 0; r < N; ++r) rhs[r] = dq[r] / dt;
-    if (i + 2 <= nl) load_w(i + 2, wq);
-    if (i + 1 < nl) {
-#pragma unroll
-      for (int r = 0; r < N; ++r) dq[r] = vic_d(b, sel<N>(r) * sv + cb + i + 1);
-    }
+    for (int r = 0; r < N; ++r) rhs[r] = ring_elem(fring(fslot, 5 + r), b.D) / dt;
     absA_of<N>(b, gm1f, wc, wn, Ap);
     jac_of<N>(b, gm1c, wn, Jn);
     double ai = wc[IDN] * V;
@@ -260,6 +319,9 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
       }
     }
     block_solve<N>(a, c, rhs);
+    // the slot's values are consumed (the solve depends on them): refill it
+    ffetch(i + 1 + DF, fslot);
+    fslot = fslot + 1 == DF ? 0 : fslot + 1;
 #pragma unroll
     for (int r = 0; r < N; ++r) {
       dp[r] = rhs[r];
@@ -281,29 +343,31 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
 #pragma unroll
     for (int v = 0; v < 5; ++v) wc[v] = wn[v];
   }
-  // back substitution: delta_i -= a'_i delta_{i+1}; B_dry accumulated on the way.
-  // The scratch streams through once each way: streaming loads and stores
-  // (evict-first) keep L1 for the strided state loads of the columns.
+  // back substitution: delta_i -= a'_i delta_{i+1}; B_dry accumulated on the
+  // way, the inputs of each layer arriving through the shared-memory ring.
+  constexpr int DB = BackRing<N>::depth, RE = BackRing<N>::elems;
+  cp_async_wait<0>();  // the forward ring is drained before its memory is reused
+  auto ring = [&](int slot, int e) { return vic_ring + ((size_t)(slot * RE + e) * nt + lane); };
+  auto fetch = [&](int i, int slot) {
+    if (i >= 0) {
+#pragma unroll
+      for (int e = 0; e < ES; ++e) cp_async_bytes8(ring(slot, e), &Sat(i, e));
+      cp_async_elem(ring(slot, ES), b.D + IDN * sv + cb + i);
+    }
+    cp_async_commit();
+  };
   double dn[N];
 #pragma unroll
   for (int r = 0; r < N; ++r) dn[r] = dp[r];
   double b_dry = (vic_d(b, IDN * sv + cb + nl - 1) - dn[0]) * 1. * V;
-  // layer i's reduced block, partial solution and du[IDN], loaded one layer ahead
-  double sa[N * N + N], du0 = 0.;
-  if (nl >= 2) {
 #pragma unroll
-    for (int e = 0; e < N * N + N; ++e) sa[e] = __ldcs(&Sat(nl - 2, e));
-    du0 = vic_d(b, IDN * sv + cb + nl - 2);
-  }
-  for (int i = nl - 2; i >= 0; --i) {
-    double cur[N * N + N], dcur = du0;
+  for (int k = 0; k < DB; ++k) fetch(nl - 2 - k, k);
+  for (int i = nl - 2, slot = 0; i >= 0; --i) {
+    cp_async_wait<DB - 1>();  // the group of layer i has landed
+    double cur[ES];
 #pragma unroll
-    for (int e = 0; e < N * N + N; ++e) cur[e] = sa[e];
-    if (i >= 1) {
-#pragma unroll
-      for (int e = 0; e < N * N + N; ++e) sa[e] = __ldcs(&Sat(i - 1, e));
-      du0 = vic_d(b, IDN * sv + cb + i - 1);
-    }
+    for (int e = 0; e < ES; ++e) cur[e] = *ring(slot, e);
+    const double dcur = ring_elem(ring(slot, ES), b.D);
     double d[N];
 #pragma unroll
     for (int r = 0; r < N; ++r) {
@@ -312,15 +376,33 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
       for (int q = 0; q < N; ++q) t += cur[r * N + q] * dn[q];
       d[r] = cur[N * N + r] - t;
     }
+    b_dry += (dcur - d[0]) * 1. * V;
+    fetch(i - DB, slot);  // the slot's values are consumed: refill it
+    slot = slot + 1 == DB ? 0 : slot + 1;
 #pragma unroll
     for (int r = 0; r < N; ++r) {
       dn[r] = d[r];
       Sat(i, N * N + r) = d[r];
     }
-    b_dry += (dcur - d[0]) * 1. * V;
   }
+  cp_async_wait<0>();
   Z[0] = sum_a2;
   Z[ncol] = b_dry;
+}
+
+// the ring of a 128-thread CTA exceeds the default 48 KB of dynamic shared
+// memory; raise the kernel's limit once (before any graph capture)
+template <class K>
+static void allow_ring_smem(K kernel, size_t bytes) {
+  static std::mutex mu;
+  static const void* done[32];
+  static int ndone = 0;
+  std::lock_guard<std::mutex> lock(mu);
+  const void* f = reinterpret_cast<const void*>(kernel);
+  for (int k = 0; k < ndone; ++k)
+    if (done[k] == f) return;
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (ndone < 32) done[ndone++] = f;
 }
 
 template <int N, class B>
@@ -411,7 +493,9 @@ static cudaError_t launch_vic_n(const Geo& g, const Phys& p, const B& b, cudaStr
   const int nl = g.nx1;
   // small column counts: narrower CTAs spread the sequential sweeps over more SMs
   int bs = ncol >= 148 * 128 ? 128 : (ncol >= 148 * 64 ? 64 : 32);
-  k_vic_column<N, B><<<(unsigned)((ncol + bs - 1) / bs), bs, 0, st>>>(g, p, b);
+  allow_ring_smem(k_vic_column<N, B>, back_ring_bytes<N>(128));
+  k_vic_column<N, B><<<(unsigned)((ncol + bs - 1) / bs), bs, back_ring_bytes<N>(bs), st>>>(g, p,
+                                                                                      b);
   dim3 gf((unsigned)((ncol + kTC - 1) / kTC), (unsigned)((nl + kTL - 1) / kTL));
   switch (p.nscalar) {
     case 0: k_vic_finish<N, 0, B><<<gf, 256, 0, st>>>(g, p, b); break;
@@ -449,15 +533,22 @@ __device__ __forceinline__ void set_stage_vic32(StageBufs32& b, int stage) {
 template <int N, int V>
 __global__ void __launch_bounds__(128, V == 0 ? 1 : (V == 1 ? 3 : 4))
     k_vic_column_batch(const Member32* __restrict__ mem, Phys p, WorkQueue q, int stage) {
+  // The member's descriptor is read from shared memory as the sweep needs its
+  // fields instead of being copied into registers (~50 of them) for the tile.
+  __shared__ Member32 s_mem;
+  static_assert(sizeof(Member32) % sizeof(int) == 0, "member descriptor copy");
   int m;
   int64_t tile;
-  while (queue_next(q, m, tile)) {
-    const Geo g = mem[m].g;
-    StageBufs32 b = mem[m].b;
-    set_stage_vic32(b, stage);
-    const int64_t col = tile * mem[m].vic_cols + threadIdx.x;
-    if ((int)threadIdx.x < mem[m].vic_cols) vic_column<N, StageBufs32>(g, p, b, col);
+  while (queue_next(q, m, tile)) {  // (starts with a barrier: the last tile is done)
+    const int* src = reinterpret_cast<const int*>(mem + m);
+    int* dst = reinterpret_cast<int*>(&s_mem);
+    for (int k = threadIdx.x; k < (int)(sizeof(Member32) / sizeof(int)); k += blockDim.x)
+      dst[k] = src[k];
+    __syncthreads();
+    const int64_t col = tile * s_mem.vic_cols + threadIdx.x;
+    if ((int)threadIdx.x < s_mem.vic_cols) vic_column<N, StageBufs32>(s_mem.g, p, s_mem.b, col);
   }
+  (void)stage;
 }
 
 template <int N, int NS>
@@ -479,8 +570,10 @@ __global__ void __launch_bounds__(256) k_vic_finish_batch(const Member32* __rest
 template <int N, int V>
 static void launch_vcb(const Member32* mem, const Phys& p, const WorkQueue& q, int stage,
                        const PersistGrid& pg, int block, cudaStream_t st) {
-  k_vic_column_batch<N, V><<<persistent_grid(k_vic_column_batch<N, V>, block, 0, pg), block, 0,
-                             st>>>(mem, p, q, stage);
+  const size_t smem = back_ring_bytes<N>(block);
+  allow_ring_smem(k_vic_column_batch<N, V>, back_ring_bytes<N>(128));
+  k_vic_column_batch<N, V><<<persistent_grid(k_vic_column_batch<N, V>, block, smem, pg), block,
+                             smem, st>>>(mem, p, q, stage);
 }
 
 cudaError_t launch_vic_column_batch(const Member32* mem, const Phys& p, const WorkQueue& q,
