@@ -67,7 +67,7 @@ constexpr int kFwdDepth = 4;  // layers of the forward sweep in flight
 
 template <int N>
 struct BackRing {
-  static constexpr int depth = N == 3 ? 6 : 2;
+  static constexpr int depth = N == 3 ? 4 : 2;
   static constexpr int elems = N * N + N + 1;
 };
 template <int N>
