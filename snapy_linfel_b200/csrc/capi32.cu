@@ -65,8 +65,7 @@ Layout32 layout32(const snapb_hydro_config& c) {
   o = a256(o + (size_t)(c.nvar + c.nscalar) * svf);
   L.R = o;
   o = a256(o + (size_t)c.nscalar * svf);
-  L.M = o;
-  o = a256(o + (c.implicit_scheme ? (size_t)g.sv * sizeof(double) : 0));
+  L.M = o;  // the FP32 form has no mass-correction output (scalars use it in place)
   L.VIC = o;
   o = a256(o + vic_scratch_bytes(g, p));
   L.PF = o;
@@ -102,7 +101,7 @@ StageBufs32 bufs32(const snapb_hydro_config& c, void* ws) {
   std::memset(&b, 0, sizeof(b));
   b.D = at<float>(ws, L.D);
   b.R = at<float>(ws, L.R);
-  b.M = c.implicit_scheme ? at<double>(ws, L.M) : nullptr;
+  b.M = nullptr;
   b.vic = at<double>(ws, L.VIC);
   b.pf = at<double>(ws, L.PF);
   b.offL = at<float>(ws, L.OFFL);

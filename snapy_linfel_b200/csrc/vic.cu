@@ -25,6 +25,7 @@
 // flux Jacobian and Roe eigenvectors (src/implicit/flux_decomposition_impl.h:133-245).
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 #include <string>
 
 #include "kernels.cuh"
@@ -63,6 +64,8 @@ constexpr int kTL = 32;  // layers per tile (redistribution)
 // shared memory by asynchronous copies (cp.async), so the short recurrence
 // does not wait a memory latency per layer and holds no extra registers.
 // Ring layout [slot][element][thread] (element ES = du[IDN]), doubles.
+constexpr int kFinThreads = 256;                // threads of a finish CTA
+constexpr int kFinItems = kTC * kTL / kFinThreads;  // cells per finish thread
 constexpr int kFwdDepth = 4;  // layers of the forward sweep in flight
 
 template <int N>
@@ -135,31 +138,23 @@ __device__ __forceinline__ void vic_set_d(const StageBufs32& b, int64_t idx, dou
   b.D[idx] = (float)x;
 }
 // RK combination of one stored value (u' for the FP32 form: the reference
-// part of u is constant in time, so the combination is the same)
-__device__ __forceinline__ double vic_rk(double* q, double* q0, int64_t o, int stage, double w0,
-                                         double w1, double w2, double d) {
-  double qo = q[o];
-  double q0v;
-  if (stage == 0) {
-    q0v = qo;
-    q0[o] = qo;
-  } else {
-    q0v = q0[o];
-  }
+// part of u is constant in time, so the combination is the same), from
+// values already loaded (qo = q[o], q0o = q0[o] when stage > 0); the stored
+// q keeps the stored precision
+__device__ __forceinline__ double vic_rk_from(double* q, double* q0, int64_t o, bool first,
+                                              double qo, double q0o, double w0, double w1,
+                                              double w2, double d) {
+  double q0v = first ? qo : q0o;
+  if (first) q0[o] = qo;
   double qn = w0 * q0v + w1 * qo + w2 * d;
   q[o] = qn;
   return qn;
 }
-__device__ __forceinline__ double vic_rk(float* q, float* q0, int64_t o, int stage, double w0,
-                                         double w1, double w2, double d) {
-  double qo = q[o];
-  double q0v;
-  if (stage == 0) {
-    q0v = qo;
-    q0[o] = (float)qo;
-  } else {
-    q0v = q0[o];
-  }
+__device__ __forceinline__ double vic_rk_from(float* q, float* q0, int64_t o, bool first,
+                                              double qo, double q0o, double w0, double w1,
+                                              double w2, double d) {
+  double q0v = first ? qo : q0o;
+  if (first) q0[o] = (float)qo;
   float qn = (float)(w0 * q0v + w1 * qo + w2 * d);
   q[o] = qn;
   return qn;
@@ -438,30 +433,71 @@ __device__ __forceinline__ void vic_finish_tile(const Geo& g, const Phys& p, con
     zs[k][c] = col0 + c < ncol ? Z[k * ncol + col0 + c] : 1.;
   }
   __syncthreads();
-  for (int idx = tid; idx < kTC * kTL; idx += blockDim.x) {
-    int s = idx % kTL, c = idx / kTL;
-    int64_t col = col0 + c;
-    int i = i0 + s;
-    if (col >= ncol || i >= nl) continue;
+  // (2) each thread's kFinItems cells: every load first (no store in
+  // between, so they are all in flight together), then the arithmetic and
+  // the stores.  Cells are distinct, so the order is the sequential one's.
+  constexpr int IT = kFinItems, NSA = NS > 0 ? NS : 1;
+  using T = std::remove_pointer_t<decltype(b.u)>;  // stored precision (FP32 / FP64)
+  T rho[IT], et[IT], dvy[IT], dvz[IT], uo[IT][5], u0o[IT][5];
+  T so[IT][NSA], s0o[IT][NSA], ro[IT][NSA], dso[IT][NSA];
+  int64_t offs[IT];
+  bool ok[IT];
+  const bool du_only = b.vic_du_only, first = b.stage == 0;
+#pragma unroll
+  for (int k = 0; k < IT; ++k) {
+    const int idx = tid + k * kFinThreads;
+    const int s = idx % kTL, c = idx / kTL;
+    const int64_t col = col0 + c;
+    const int i = i0 + s;
+    ok[k] = col < ncol && i < nl;
+    if (!ok[k]) continue;
     const int64_t off = column_base(g, col) + i;
-    const int xi = g.il + i;
-    double rho = vic_w(b, sv, IDN, off, xi);
-    double ai = rho * g.vol;
-    double et = vic_d(b, IDN * sv + off);
-    double fix = dl[0][c][s] - et;
+    offs[k] = off;
+    rho[k] = b.w[IDN * sv + off];
+    et[k] = b.D[IDN * sv + off];
+    if constexpr (N == 3) {
+      dvy[k] = b.D[IVY * sv + off];
+      dvz[k] = b.D[IVZ * sv + off];
+    }
+    if (!du_only) {
+#pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        uo[k][v] = b.u[v * sv + off];
+        if (!first) u0o[k][v] = b.u0[v * sv + off];
+      }
+#pragma unroll
+      for (int n = 0; n < NS; ++n) {
+        const int64_t o = n * sv + off;
+        so[k][n] = b.s[o];
+        if (!first) s0o[k][n] = b.s0[o];
+        ro[k][n] = b.r[o];
+        dso[k][n] = b.D[(5 + n) * sv + off];
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < IT; ++k) {
+    if (!ok[k]) continue;
+    const int idx = tid + k * kFinThreads;
+    const int s = idx % kTL, c = idx / kTL;
+    const int64_t off = offs[k];
+    const int xi = g.il + i0 + s;
+    const double rhok = vic_full(b, (double)rho[k], IDN, xi), etk = et[k];
+    double ai = rhok * g.vol;
+    double fix = dl[0][c][s] - etk;
     double du[5];
-    du[IDN] = et + fix * 1. + rho * ai * zs[1][c] / zs[0][c];
+    du[IDN] = etk + fix * 1. + rhok * ai * zs[1][c] / zs[0][c];
     if constexpr (N == 3) {
       du[IVX] = dl[1][c][s];
-      du[IVY] = vic_d(b, IVY * sv + off);
-      du[IVZ] = vic_d(b, IVZ * sv + off);
+      du[IVY] = dvy[k];
+      du[IVZ] = dvz[k];
       du[IPR] = dl[2][c][s];
     } else {
 #pragma unroll
       for (int v = 1; v < 5; ++v) du[v] = dl[v][c][s];
     }
     if (b.M) b.M[IDN * sv + off] = fix;
-    if (b.vic_du_only) {
+    if (du_only) {
 #pragma unroll
       for (int v = 0; v < 5; ++v) vic_set_d(b, v * sv + off, du[v]);
       continue;
@@ -469,21 +505,23 @@ __device__ __forceinline__ void vic_finish_tile(const Geo& g, const Phys& p, con
     double unew_rho = 0.;
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
-      double un = vic_rk(b.u, b.u0, v * sv + off, b.stage, b.wgt0, b.wgt1, b.wgt2, du[v]);
+      double un = vic_rk_from(b.u, b.u0, v * sv + off, first, uo[k][v], u0o[k][v], b.wgt0,
+                              b.wgt1, b.wgt2, du[v]);
       if (v == IDN) unew_rho = vic_full_rho(b, un, xi);
     }
 #pragma unroll
     for (int n = 0; n < NS; ++n) {
-      int64_t o = n * sv + off;
-      double ds = vic_d(b, (5 + n) * sv + off) + fix * (double)b.r[o];
-      double sn = vic_rk(b.s, b.s0, o, b.stage, b.wgt0, b.wgt1, b.wgt2, ds);
+      const int64_t o = n * sv + off;
+      double ds = (double)dso[k][n] + fix * (double)ro[k][n];
+      double sn = vic_rk_from(b.s, b.s0, o, first, so[k][n], s0o[k][n], b.wgt0, b.wgt1,
+                              b.wgt2, ds);
       b.r[o] = sn / unew_rho;
     }
   }
 }
 
 template <int N, int NS, class B>
-__global__ void __launch_bounds__(256) k_vic_finish(Geo g, Phys p, B b) {
+__global__ void __launch_bounds__(kFinThreads) k_vic_finish(Geo g, Phys p, B b) {
   vic_finish_tile<N, NS, B>(g, p, b, (int64_t)blockIdx.x * kTC, (int)blockIdx.y * kTL);
 }
 
@@ -498,10 +536,10 @@ static cudaError_t launch_vic_n(const Geo& g, const Phys& p, const B& b, cudaStr
                                                                                       b);
   dim3 gf((unsigned)((ncol + kTC - 1) / kTC), (unsigned)((nl + kTL - 1) / kTL));
   switch (p.nscalar) {
-    case 0: k_vic_finish<N, 0, B><<<gf, 256, 0, st>>>(g, p, b); break;
-    case 1: k_vic_finish<N, 1, B><<<gf, 256, 0, st>>>(g, p, b); break;
-    case 2: k_vic_finish<N, 2, B><<<gf, 256, 0, st>>>(g, p, b); break;
-    case 3: k_vic_finish<N, 3, B><<<gf, 256, 0, st>>>(g, p, b); break;
+    case 0: k_vic_finish<N, 0, B><<<gf, kFinThreads, 0, st>>>(g, p, b); break;
+    case 1: k_vic_finish<N, 1, B><<<gf, kFinThreads, 0, st>>>(g, p, b); break;
+    case 2: k_vic_finish<N, 2, B><<<gf, kFinThreads, 0, st>>>(g, p, b); break;
+    case 3: k_vic_finish<N, 3, B><<<gf, kFinThreads, 0, st>>>(g, p, b); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
@@ -552,18 +590,23 @@ __global__ void __launch_bounds__(128, V == 0 ? 1 : (V == 1 ? 3 : 4))
 }
 
 template <int N, int NS>
-__global__ void __launch_bounds__(256) k_vic_finish_batch(const Member32* __restrict__ mem,
+__global__ void __launch_bounds__(kFinThreads, 2) k_vic_finish_batch(const Member32* __restrict__ mem,
                                                           Phys p, WorkQueue q, int stage) {
+  __shared__ Member32 s_mem;  // the member's descriptor, read as needed (see the column kernel)
   int m;
   int64_t tile;
-  while (queue_next(q, m, tile)) {
-    const Geo g = mem[m].g;
-    StageBufs32 b = mem[m].b;
-    set_stage_vic32(b, stage);
-    const int nlb = (g.nx1 + kTL - 1) / kTL;
+  while (queue_next(q, m, tile)) {  // (starts with a barrier: the last tile is done)
+    const int* src = reinterpret_cast<const int*>(mem + m);
+    int* dst = reinterpret_cast<int*>(&s_mem);
+    for (int k = threadIdx.x; k < (int)(sizeof(Member32) / sizeof(int)); k += blockDim.x)
+      dst[k] = src[k];
+    __syncthreads();
+    if (threadIdx.x == 0) set_stage_vic32(s_mem.b, stage);
+    __syncthreads();
+    const int nlb = (s_mem.g.nx1 + kTL - 1) / kTL;
     const int64_t cb = tile / nlb;
     const int lb = (int)(tile - cb * nlb);
-    vic_finish_tile<N, NS, StageBufs32>(g, p, b, cb * kTC, lb * kTL);
+    vic_finish_tile<N, NS, StageBufs32>(s_mem.g, p, s_mem.b, cb * kTC, lb * kTL);
   }
 }
 
@@ -595,7 +638,8 @@ cudaError_t launch_vic_finish_batch(const Member32* mem, const Phys& p, const Wo
                                     int stage, const PersistGrid& pg, cudaStream_t st) {
   static_assert(kTC == kVicFinishCols && kTL == kVicFinishLayers, "finish tile shape");
 #define SNAPB_VFB(N, NS)                                                                 \
-  k_vic_finish_batch<N, NS><<<persistent_grid(k_vic_finish_batch<N, NS>, 256, 0, pg), 256, 0, \
+  k_vic_finish_batch<N, NS><<<persistent_grid(k_vic_finish_batch<N, NS>, kFinThreads, 0, pg), \
+                              kFinThreads, 0, \
                               st>>>(mem, p, q, stage)
   if (vic_n(p) == 5) {
     switch (p.nscalar) {
