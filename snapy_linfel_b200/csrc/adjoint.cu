@@ -148,9 +148,9 @@ struct CombineArgs {
 __global__ void k_adj_combine(Geo g, CombineArgs A) {
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= g.sv) return;
-  const int i = (int)(t % g.nc1);
-  const int j = (int)((t / g.nc1) % g.nc2);
-  const int k = (int)(t / ((int64_t)g.nc1 * g.nc2));
+  const int i = umod(t, g.nc1);
+  const int j = umod(udiv(t, g.nc1), g.nc2);
+  const int k = udiv(t, (int64_t)g.nc1 * g.nc2);
   const bool inner = i >= g.il && i <= g.iu && j >= g.jl && j <= g.ju && k >= g.kl && k <= g.ku;
   const int64_t sv = g.sv;
   for (int v = 0; v < 5; ++v) {
@@ -175,9 +175,9 @@ __global__ void k_bc_adjoint(Geo g, const double* gin, double* gout, int nv, int
                              AxisAdj a1, AxisAdj a2, AxisAdj a3) {
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= g.sv) return;
-  const int i = (int)(t % g.nc1);
-  const int j = (int)((t / g.nc1) % g.nc2);
-  const int k = (int)(t / ((int64_t)g.nc1 * g.nc2));
+  const int i = umod(t, g.nc1);
+  const int j = umod(udiv(t, g.nc1), g.nc2);
+  const int k = udiv(t, (int64_t)g.nc1 * g.nc2);
   const bool inner = i >= g.il && i <= g.iu && j >= g.jl && j <= g.ju && k >= g.kl && k <= g.ku;
   for (int v = 0; v < nv; ++v)
     gout[v * g.sv + t] =
@@ -188,9 +188,9 @@ __global__ void k_bc_adjoint(Geo g, const double* gin, double* gout, int nv, int
 __global__ void k_mask_interior(Geo g, const double* src, double* dst, int nv) {
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= g.sv) return;
-  const int i = (int)(t % g.nc1);
-  const int j = (int)((t / g.nc1) % g.nc2);
-  const int k = (int)(t / ((int64_t)g.nc1 * g.nc2));
+  const int i = umod(t, g.nc1);
+  const int j = umod(udiv(t, g.nc1), g.nc2);
+  const int k = udiv(t, (int64_t)g.nc1 * g.nc2);
   const bool inner = i >= g.il && i <= g.iu && j >= g.jl && j <= g.ju && k >= g.kl && k <= g.ku;
   for (int v = 0; v < nv; ++v) dst[v * g.sv + t] = inner ? src[v * g.sv + t] : 0.;
 }
@@ -513,8 +513,8 @@ __global__ void __launch_bounds__(128) k_march_adj(Geo g, Phys p, AdjBufs b, int
   const int no = ohi - olo + 1;
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (tid >= (int64_t)ni * no) return;
-  const int i = g.il + (int)(tid % ni);
-  const int o = olo + (int)(tid / ni);
+  const int i = g.il + umod(tid, ni);
+  const int o = olo + udiv(tid, ni);
   const int f0 = lo + blockIdx.y * seglen;
   if (f0 > hi + 1) return;
   const int f1 = min(f0 + seglen - 1, hi + 1);
@@ -638,7 +638,7 @@ __global__ void __launch_bounds__(256, 2) k_x1_adj(Geo g, Phys p, AdjBufs b, int
     int c = idx / nf, f = g.il + (idx - c * nf);
     int64_t col = col0 + c;
     if (col >= ncol) continue;
-    int j = (int)(col % g.nc2), k = (int)(col / g.nc2);
+    int j = umod(col, g.nc2), k = udiv(col, g.nc2);
     if (j < g.jl || j > g.ju || k < g.kl || k > g.ku) continue;
     int64_t off = col * nc1 + f;
     double gF[NV];
@@ -656,7 +656,7 @@ __global__ void __launch_bounds__(256, 2) k_x1_adj(Geo g, Phys p, AdjBufs b, int
     int c = idx / g.nx1, i = g.il + (idx - c * g.nx1);
     int64_t col = col0 + c;
     if (col >= ncol) continue;
-    int j = (int)(col % g.nc2), k = (int)(col / g.nc2);
+    int j = umod(col, g.nc2), k = udiv(col, g.nc2);
     if (j < g.jl || j > g.ju || k < g.kl || k > g.ku) continue;
     int64_t off = col * nc1 + i;
     const double* wb = sw + (size_t)c * NV * nc1 + i;
@@ -764,9 +764,9 @@ __global__ void k_cell_adj(Geo g, Phys p, AdjBufs b) {
   if (t >= g.sv) return;
   const int64_t sv = g.sv;
   const double dt = *b.dt;
-  const int i = (int)(t % g.nc1);
-  const int j = (int)((t / g.nc1) % g.nc2);
-  const int k = (int)(t / ((int64_t)g.nc1 * g.nc2));
+  const int i = umod(t, g.nc1);
+  const int j = umod(udiv(t, g.nc1), g.nc2);
+  const int k = udiv(t, (int64_t)g.nc1 * g.nc2);
   const bool inner = i >= g.il && i <= g.iu && j >= g.jl && j <= g.ju && k >= g.kl && k <= g.ku;
   double gw[5 + NS];
 #pragma unroll
@@ -843,7 +843,7 @@ constexpr int kCTL = 32;   // cells per tile (contraction)
 
 __device__ __forceinline__ int64_t adj_column_base(const Geo& g, int64_t col) {
   const int nj = g.ju - g.jl + 1;
-  const int j = g.jl + (int)(col % nj), k = g.kl + (int)(col / nj);
+  const int j = g.jl + umod(col, nj), k = g.kl + udiv(col, nj);
   return (int64_t)k * g.s3 + (int64_t)j * g.s2 + g.il;
 }
 

@@ -90,9 +90,9 @@ __global__ void k_bc(Geo g, AxisBC a1, AxisBC a2, AxisBC a3, double* var, int nv
   const int nc1 = g.nc1, nc2 = g.nc2;
   const int64_t sv = g.sv;
   const int64_t t = bc_shell_cell(g, s);
-  int i = (int)(t % nc1);
-  int j = (int)((t / nc1) % nc2);
-  int k = (int)(t / ((int64_t)nc1 * nc2));
+  int i = umod(t, nc1);
+  int j = umod(udiv(t, nc1), nc2);
+  int k = udiv(t, (int64_t)nc1 * nc2);
   bool f1, f2, f3;
   int si = bc_map(a1, i, f1), sj = bc_map(a2, j, f2), sk = bc_map(a3, k, f3);
   if (si == i && sj == j && sk == k) return;  // interior (or identity-mapped) cell
@@ -135,9 +135,9 @@ __global__ void k_cfl(Geo g, double gammad, int use1, int use2, int use3, const 
   double m1 = DBL_MAX, m2 = DBL_MAX, m3 = DBL_MAX;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
        t += (int64_t)gridDim.x * blockDim.x) {
-    int i = g.il + (int)(t % ni);
-    int j = g.jl + (int)((t / ni) % nj);
-    int k = g.kl + (int)(t / ((int64_t)ni * nj));
+    int i = g.il + umod(t, ni);
+    int j = g.jl + umod(udiv(t, ni), nj);
+    int k = g.kl + udiv(t, (int64_t)ni * nj);
     int64_t o = (int64_t)k * g.s3 + (int64_t)j * g.s2 + i;
     double rho = w[IDN * g.sv + o], pr = w[IPR * g.sv + o];
     double cs = sqrt(gammad * pr / rho);
@@ -259,9 +259,9 @@ __global__ void k_check(Geo g, double gm1, const double* u, int* flags) {
   const int64_t n = (int64_t)ni * nj * nk;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
        t += (int64_t)gridDim.x * blockDim.x) {
-    int i = g.il + (int)(t % ni);
-    int j = g.jl + (int)((t / ni) % nj);
-    int k = g.kl + (int)(t / ((int64_t)ni * nj));
+    int i = g.il + umod(t, ni);
+    int j = g.jl + umod(udiv(t, ni), nj);
+    int k = g.kl + udiv(t, (int64_t)ni * nj);
     int64_t o = (int64_t)k * g.s3 + (int64_t)j * g.s2 + i;
     double uc[5], wc[5];
 #pragma unroll
@@ -301,11 +301,11 @@ __global__ void k_reconstruct(Geo g, Phys p, int dim, int group, const double* w
                               double* wlr) {
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= g.sv * nv) return;
-  int v = (int)(t / g.sv);
+  int v = udiv(t, g.sv);
   int64_t cell = t - (int64_t)v * g.sv;
-  int i = (int)(cell % g.nc1);
-  int j = (int)((cell / g.nc1) % g.nc2);
-  int k = (int)(cell / ((int64_t)g.nc1 * g.nc2));
+  int i = umod(cell, g.nc1);
+  int j = umod(udiv(cell, g.nc1), g.nc2);
+  int k = udiv(cell, (int64_t)g.nc1 * g.nc2);
   int n, pos;
   int64_t st;
   if (dim == 3) n = g.nc1, pos = i, st = 1;

@@ -49,6 +49,8 @@ const char* check_config(const snapb_hydro_config* c) {
   if (c->nu_iso < 0. || c->kappa_iso < 0.) return "diffusion coefficients must be >= 0";
   if (c->non_hydrostatic < 0. || c->non_hydrostatic > 1.) return "non-hydrostatic outside [0,1]";
   Geo g = make_geo(*c);
+  if ((int64_t)(c->nvar + c->nscalar) * g.sv >= ((int64_t)1 << 31))
+    return "block too large: (nvar + nscalar) x cells (ghosts included) must stay below 2^31";
   if (g.nc1 > 1 && x1_smem_per_column(g, 5 + c->nscalar) > 200 * 1024)
     return "x1 column too long for one CTA's shared memory";
   return nullptr;

@@ -5,6 +5,8 @@
 // Variable order IDN, IVX, IVY, IVZ, IPR (src/snap.h:34-46).
 #pragma once
 
+#include <cstdint>
+
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -100,6 +102,17 @@ inline Phys make_phys(const snapb_hydro_config& c) {
   return p;
 }
 
+// Index arithmetic.  Every element, cell, column, line and slot index of a
+// block is below 2^31 (check_config rejects larger blocks), so quotients and
+// remainders by run-time divisors are taken in 32 bits: a 64-bit division is
+// a long instruction sequence, and the sweeps take several per face.
+__host__ __device__ __forceinline__ int udiv(int64_t a, int64_t b) {
+  return (int)((uint32_t)a / (uint32_t)b);
+}
+__host__ __device__ __forceinline__ int umod(int64_t a, int64_t b) {
+  return (int)((uint32_t)a % (uint32_t)b);
+}
+
 // The ghost shell of a block, one slot per ghost cell:
 // slots [0, A) are the x1 ghosts of rows inside the x2/x3 interior
 // (2 ng per row), slots [A, A + B) the cells of the ghost rows (x3-ghost slabs
@@ -118,25 +131,25 @@ __host__ __device__ __forceinline__ int64_t bc_shell_cell(const Geo& g, int64_t 
   const int64_t A = g.nc1 > 1 ? nj * nk * ng2 : 0;
   int i, j, k;
   if (s < A) {
-    const int c = (int)(s % ng2);
-    const int64_t row = s / ng2;
+    const int c = umod(s, ng2);
+    const int row = udiv(s, ng2);
     i = c < g.ng ? c : g.nc1 - ng2 + c;
-    j = g.jl + (int)(row % nj);
-    k = g.kl + (int)(row / nj);
+    j = g.jl + umod(row, nj);
+    k = g.kl + udiv(row, nj);
   } else {
     s -= A;
-    i = (int)(s % g.nc1);
-    int64_t row = s / g.nc1;
-    const int64_t c1 = g.nc3 > 1 ? (int64_t)ng2 * g.nc2 : 0;
+    i = umod(s, g.nc1);
+    int row = udiv(s, g.nc1);
+    const int c1 = g.nc3 > 1 ? ng2 * g.nc2 : 0;
     if (row < c1) {
-      j = (int)(row % g.nc2);
-      const int kk = (int)(row / g.nc2);
+      j = umod(row, g.nc2);
+      const int kk = udiv(row, g.nc2);
       k = kk < g.ng ? kk : g.nc3 - ng2 + kk;
     } else {
       row -= c1;
-      const int jj = (int)(row % ng2);
+      const int jj = umod(row, ng2);
       j = jj < g.ng ? jj : g.nc2 - ng2 + jj;
-      k = g.kl + (int)(row / ng2);
+      k = g.kl + udiv(row, ng2);
     }
   }
   return ((int64_t)k * g.nc2 + j) * g.nc1 + i;

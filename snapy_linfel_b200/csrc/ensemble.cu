@@ -47,9 +47,9 @@ __global__ void __launch_bounds__(256) k_cfl32_batch(const Member32* __restrict_
     double m1 = 1.7e308, m2 = 1.7e308, m3 = 1.7e308;
     const int64_t t0 = tile * 1024;
     for (int64_t t = t0 + threadIdx.x; t < min(t0 + 1024, n); t += blockDim.x) {
-      int i = g.il + (int)(t % ni);
-      int j = g.jl + (int)((t / ni) % nj);
-      int k = g.kl + (int)(t / ((int64_t)ni * nj));
+      int i = g.il + umod(t, ni);
+      int j = g.jl + umod(udiv(t, ni), nj);
+      int k = g.kl + udiv(t, (int64_t)ni * nj);
       int64_t o = (int64_t)k * g.s3 + (int64_t)j * g.s2 + i;
       double rho = rb[i] + w[IDN * g.sv + o], pr = pb[i] + w[IPR * g.sv + o];
       double cs = sqrt(p.gammad * pr / rho);

@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(256) k_x1(Geo g, Phys p, StageBufs b, int C, i
     int c = idx / nf, f = g.il + (idx - c * nf);
     int64_t col = col0 + c;
     if (col >= ncol) continue;
-    int j = (int)(col % g.nc2), k = (int)(col / g.nc2);
+    int j = umod(col, g.nc2), k = udiv(col, g.nc2);
     if (j < g.jl || j > g.ju || k < g.kl || k > g.ku) continue;
     const double* base = sw + (size_t)c * NV * nc1;
     double L[NV], R[NV], F[NV];
@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(256) k_x1(Geo g, Phys p, StageBufs b, int C, i
     int c = idx / g.nx1, i = g.il + (idx - c * g.nx1);
     int64_t col = col0 + c;
     if (col >= ncol) continue;
-    int j = (int)(col % g.nc2), k = (int)(col / g.nc2);
+    int j = umod(col, g.nc2), k = udiv(col, g.nc2);
     if (j < g.jl || j > g.ju || k < g.kl || k > g.ku) continue;
     int64_t off = col * nc1 + i;
     double d[NV];
@@ -290,8 +290,8 @@ __global__ void __launch_bounds__(128) k_march(Geo g, Phys p, StageBufs b, int s
   const int no = ohi - olo + 1;
   const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (tid >= (int64_t)ni * no) return;
-  const int i = g.il + (int)(tid % ni);
-  const int o = olo + (int)(tid / ni);
+  const int i = g.il + umod(tid, ni);
+  const int o = olo + udiv(tid, ni);
   const int f0 = lo + blockIdx.y * seglen;
   if (f0 > hi) return;
   const int f1 = min(f0 + seglen, hi + 1);
@@ -432,9 +432,9 @@ __global__ void k_diff(Geo g, Phys p, StageBufs b) {
   const int ni = g.iu - g.il + 1, nj = g.ju - g.jl + 1, nk = g.ku - g.kl + 1;
   int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (tid >= (int64_t)ni * nj * nk) return;
-  int i = g.il + (int)(tid % ni);
-  int j = g.jl + (int)((tid / ni) % nj);
-  int k = g.kl + (int)(tid / ((int64_t)ni * nj));
+  int i = g.il + umod(tid, ni);
+  int j = g.jl + umod(udiv(tid, ni), nj);
+  int k = g.kl + udiv(tid, (int64_t)ni * nj);
   int64_t t = (int64_t)k * g.s3 + (int64_t)j * g.s2 + i;
   double acc[5] = {0., 0., 0., 0., 0.};
   const double A[3] = {g.A1, g.A2, g.A3};
@@ -457,9 +457,9 @@ __global__ void k_finalize(Geo g, Phys p, StageBufs b) {
   const int ni = g.iu - g.il + 1, nj = g.ju - g.jl + 1, nk = g.ku - g.kl + 1;
   int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (tid >= (int64_t)ni * nj * nk) return;
-  int i = g.il + (int)(tid % ni);
-  int j = g.jl + (int)((tid / ni) % nj);
-  int k = g.kl + (int)(tid / ((int64_t)ni * nj));
+  int i = g.il + umod(tid, ni);
+  int j = g.jl + umod(udiv(tid, ni), nj);
+  int k = g.kl + udiv(tid, (int64_t)ni * nj);
   int64_t off = (int64_t)k * g.s3 + (int64_t)j * g.s2 + i;
   double d[NV], wc[5];
 #pragma unroll

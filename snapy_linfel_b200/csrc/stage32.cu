@@ -233,7 +233,7 @@ __device__ __forceinline__ void x1_32_tile(const Geo& g, const Phys& p, const St
     int c = idx / nf, f = g.il + (idx - c * nf);
     int64_t col = col0 + c;
     if (col >= ncol) continue;
-    int j = (int)(col % g.nc2), k = (int)(col / g.nc2);
+    int j = umod(col, g.nc2), k = udiv(col, g.nc2);
     if (j < g.jl || j > g.ju || k < g.kl || k > g.ku) continue;
     const float* base = sw + (size_t)c * NV * nc1;
     float L[NV], R[NV], F[NV];
@@ -291,7 +291,7 @@ __device__ __forceinline__ void x1_32_tile(const Geo& g, const Phys& p, const St
     int c = idx / g.nx1, i = g.il + (idx - c * g.nx1);
     int64_t col = col0 + c;
     if (col >= ncol) continue;
-    int j = (int)(col % g.nc2), k = (int)(col / g.nc2);
+    int j = umod(col, g.nc2), k = udiv(col, g.nc2);
     if (j < g.jl || j > g.ju || k < g.kl || k > g.ku) continue;
     int64_t off = col * nc1 + i;
     float d[NV];
@@ -338,8 +338,8 @@ __device__ __forceinline__ void march32_line(const Geo& g, const Phys& p, const 
   }
   const int no = ohi - olo + 1;
   if (tid >= (int64_t)ni * no) return;
-  const int i = g.il + (int)(tid % ni);
-  const int o = olo + (int)(tid / ni);
+  const int i = g.il + umod(tid, ni);
+  const int o = olo + udiv(tid, ni);
   const int f0 = lo + seg * seglen;
   if (f0 > hi) return;
   const int f1 = min(f0 + seglen, hi + 1);
@@ -461,9 +461,9 @@ __device__ __forceinline__ void bc32_cell(int nc1, int nc2, int nc3, int64_t sv,
                                           int kind, const double* rb, const double* pb,
                                           double igm1, int64_t t) {
   if (t >= sv) return;
-  int i = (int)(t % nc1);
-  int j = (int)((t / nc1) % nc2);
-  int k = (int)(t / ((int64_t)nc1 * nc2));
+  int i = umod(t, nc1);
+  int j = umod(udiv(t, nc1), nc2);
+  int k = udiv(t, (int64_t)nc1 * nc2);
   bool f1, f2, f3;
   int si = bc_map32(a1, i, f1), sj = bc_map32(a2, j, f2), sk = bc_map32(a3, k, f3);
   if (si == i && sj == j && sk == k) return;
@@ -493,7 +493,7 @@ __global__ void k_to_pert(int64_t n, int nc1, int kind, double igm1, const doubl
                           const double* rb, const double* pb, float* out) {
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
-  int i = (int)(t % nc1);
+  int i = umod(t, nc1);
   out[IDN * n + t] = (float)(in[IDN * n + t] - rb[i]);
   out[IVX * n + t] = (float)in[IVX * n + t];
   out[IVY * n + t] = (float)in[IVY * n + t];
@@ -506,7 +506,7 @@ __global__ void k_from_pert(int64_t n, int nc1, int kind, double igm1, const flo
                             const double* rb, const double* pb, double* out) {
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
-  int i = (int)(t % nc1);
+  int i = umod(t, nc1);
   out[IDN * n + t] = (double)in[IDN * n + t] + rb[i];
   out[IVX * n + t] = in[IVX * n + t];
   out[IVY * n + t] = in[IVY * n + t];
@@ -529,9 +529,9 @@ __global__ void k_cfl32(Geo g, double gammad, int use1, int use2, int use3, cons
   double m1 = 1.7e308, m2 = 1.7e308, m3 = 1.7e308;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
        t += (int64_t)gridDim.x * blockDim.x) {
-    int i = g.il + (int)(t % ni);
-    int j = g.jl + (int)((t / ni) % nj);
-    int k = g.kl + (int)(t / ((int64_t)ni * nj));
+    int i = g.il + umod(t, ni);
+    int j = g.jl + umod(udiv(t, ni), nj);
+    int k = g.kl + udiv(t, (int64_t)ni * nj);
     int64_t o = (int64_t)k * g.s3 + (int64_t)j * g.s2 + i;
     double rho = rb[i] + w[IDN * g.sv + o], pr = pb[i] + w[IPR * g.sv + o];
     double cs = sqrt(gammad * pr / rho);

@@ -103,7 +103,7 @@ __device__ __forceinline__ double ring_elem(const double* slot, const float*) {
 // (k, j, il) offset of interior column `col`
 __device__ __forceinline__ int64_t column_base(const Geo& g, int64_t col) {
   const int nj = g.ju - g.jl + 1;
-  const int j = g.jl + (int)(col % nj), k = g.kl + (int)(col / nj);
+  const int j = g.jl + umod(col, nj), k = g.kl + udiv(col, nj);
   return (int64_t)k * g.s3 + (int64_t)j * g.s2 + g.il;
 }
 
@@ -420,6 +420,7 @@ __device__ __forceinline__ void vic_finish_tile(const Geo& g, const Phys& p, con
   const double* Z = S + (int64_t)nl * ES * ncol;
   __shared__ double dl[N][kTC][kTL + 1];
   __shared__ double zs[2][kTC];
+  __shared__ int64_t cbs[kTC];  // (k, j, il) offsets of the tile's columns
   const int tid = threadIdx.x;
   for (int idx = tid; idx < N * kTC * kTL; idx += blockDim.x) {
     int c = idx % kTC, rest = idx / kTC;
@@ -431,6 +432,7 @@ __device__ __forceinline__ void vic_finish_tile(const Geo& g, const Phys& p, con
   if (tid < 2 * kTC) {
     int c = tid % kTC, k = tid / kTC;
     zs[k][c] = col0 + c < ncol ? Z[k * ncol + col0 + c] : 1.;
+    if (k == 0) cbs[c] = col0 + c < ncol ? column_base(g, col0 + c) : 0;
   }
   __syncthreads();
   // (2) each thread's kFinItems cells: every load first (no store in
@@ -451,7 +453,7 @@ __device__ __forceinline__ void vic_finish_tile(const Geo& g, const Phys& p, con
     const int i = i0 + s;
     ok[k] = col < ncol && i < nl;
     if (!ok[k]) continue;
-    const int64_t off = column_base(g, col) + i;
+    const int64_t off = cbs[c] + i;
     offs[k] = off;
     rho[k] = b.w[IDN * sv + off];
     et[k] = b.D[IDN * sv + off];
