@@ -29,6 +29,7 @@ rank, no exchange) — ``scaling: weak``.
 from __future__ import annotations
 
 import argparse
+import datetime
 import json
 import os
 import statistics
@@ -116,21 +117,39 @@ class ClockSampler:
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,"
+              "timestamp")
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except FileNotFoundError:
             self.proc = None
         return self
+
+    def mark_start(self):
+        """the timed region starts now (samples outside it are dropped)"""
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
+
+    def _in_window(self, stamp):
+        if self.t0 is None or self.t1 is None:
+            return True
+        try:
+            t = datetime.datetime.strptime(stamp.strip(), "%Y/%m/%d %H:%M:%S.%f").timestamp()
+        except ValueError:
+            return True
+        return self.t0 - 0.06 <= t <= self.t1 + 0.06
 
     def __exit__(self, *exc):
         self.lines = []
@@ -148,6 +167,8 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in getattr(self, "lines", []):
             f = [x.strip() for x in ln.split(",")]
+            if len(f) > 9 and not self._in_window(f[9]):
+                continue
             try:
                 sm.append(float(f[1]))
                 mx = float(f[2])
@@ -523,19 +544,26 @@ def run_ensemble(args):
     # ---- batched FP32: autotune, capture, replay ----
     ens = Ensemble(members, device=dev)
     init32 = ens.save()
-    tune = ens.tune(steps=1)
+    if args.tuning:
+        # fixed tile shapes (reproducible launch sequence, e.g. for profiling)
+        fixed = {k: int(v) for k, v in (kv.split("=") for kv in args.tuning.split(","))}
+        ens.set_tuning(**fixed)
+        tune = {"fixed": ens.tuning.as_dict()}
+    else:
+        tune = ens.tune(steps=1)
     ens.restore(init32)
     ens.capture()
-    for _ in range(args.warmup):
-        ens.step()
-    barrier()
     with ClockSampler(local) as clk:
+        for _ in range(args.warmup):
+            ens.step()
         barrier()
+        clk.mark_start()
         ev0.record(stream)
         for _ in range(args.steps):
             ens.step()
         ev1.record(stream)
         barrier()
+        clk.mark_end()
     ms32 = max_ms(ev0.elapsed_time(ev1))
     value32 = world * cells * 3 * args.steps / (ms32 / 1e3) / 1e6
     _lib.timing_enable(True)
@@ -805,18 +833,19 @@ def run_ours(args):
         torch.cuda.synchronize()
 
     # ---- device-resident throughput (value) ----
-    for _ in range(args.warmup):
-        mb.step()
-    barrier()
-    _lib.timing_enable(True)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
+        for _ in range(args.warmup):
+            mb.step()
         barrier()
+        _lib.timing_enable(True)
+        clk.mark_start()
         ev0.record(stream)
         for _ in range(args.steps):
             mb.step()
         ev1.record(stream)
         barrier()
+        clk.mark_end()
     ms = ev0.elapsed_time(ev1)
     kern = _lib.timing_query()
     _lib.timing_enable(False)
@@ -951,6 +980,9 @@ def main():
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--acc-steps", type=int, default=100)
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--tuning", default="",
+                    help="fixed ensemble tile shapes instead of the autotuner, "
+                         "e.g. x1_columns=8,march_segment=16,vic_block=32,vic_regs=0")
     ap.add_argument("--adj-steps", type=int, default=2)
     ap.add_argument("--adj-nsteps", type=int, default=200)
     ap.add_argument("--adj-every", type=int, default=20)
