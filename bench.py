@@ -548,7 +548,7 @@ def run_ensemble(args):
         # fixed tile shapes (reproducible launch sequence, e.g. for profiling)
         fixed = {k: int(v) for k, v in (kv.split("=") for kv in args.tuning.split(","))}
         ens.set_tuning(**fixed)
-        tune = {"fixed": ens.tuning.as_dict()}
+        tune = {"best": ens.tuning.as_dict(), "fixed": True}
     else:
         tune = ens.tune(steps=1)
     ens.restore(init32)
