@@ -297,8 +297,8 @@ def rel_errors(a, b, it):
 # dram__bytes_write.sum) from the ncu captures summarised in profiles/, scaled
 # to a launch by the cells it processes (traffic grows with the cells): the
 # batched FP32 kernels of the 12-member ensemble capture.
-NCU_TRAFFIC_PER_CELL_F32 = {"x1_sweep": 67.6, "x2_sweep": 65.5, "x3_sweep": 65.3,
-                            "implicit_vic": 245.0 + 113.3}
+NCU_TRAFFIC_PER_CELL_F32 = {"x1_sweep": 68.2, "x2_sweep": 63.2, "x3_sweep": 63.2,
+                            "implicit_vic": 243.9 + 104.1}
 
 
 def dominant_roofline(kern, cfg, cells, elem, peak, peak_src):
@@ -317,7 +317,7 @@ def dominant_roofline(kern, cfg, cells, elem, peak, peak_src):
             "peak_source": peak_src, "unit": "GB/s", "frac": ach / peak,
             "traffic": traffic,
             "traffic_source": ("ncu capture of the 12-member ensemble, bytes per cell x cells "
-                               "(profiles/batched_kernels_ensemble12_fp32.md)"
+                               "(profiles/batched_fp32_kernels_warm_bubble_ensemble.md)"
                                if traffic is not None else None),
             "algorithmic_bytes_per_cell": per_cell,
             "cells_per_launch": cells, "ms_per_launch": per_launch_s * 1e3,
