@@ -42,6 +42,7 @@
 
 #include "dual.cuh"
 #include "kernels.cuh"
+#include "ring.cuh"
 #include "riemann_adj.cuh"
 #include "vic_blocks.cuh"
 
@@ -946,9 +947,23 @@ __device__ __noinline__ void solve_transposed(const double (&M)[N][N], double (&
   block_solve<N>(Mt, Z, y);
 }
 
+// Per-thread ring (see ring.cuh) for the five sequential passes of
+// k_vadj_sweep: depth layers ahead, elems doubles per slot (the widest pass,
+// the transposed sweep: t rows, |A| and J of the face / cell above, ahat).
+template <int N>
+struct VadjRing {
+  static constexpr int depth = N == 3 ? 4 : 2;
+  static constexpr int elems = 3 * N * N + N;
+};
+template <int N>
+constexpr size_t vadj_ring_bytes(int threads) {
+  return (size_t)threads * VadjRing<N>::depth * VadjRing<N>::elems * sizeof(double);
+}
+
 template <int N>
 __global__ void __launch_bounds__(128) k_vadj_sweep(Geo g, Phys p, AdjBufs b) {
-  constexpr int E1 = VadjDims<N>::E1, ES = VadjDims<N>::ES;
+  constexpr int E1 = VadjDims<N>::E1, ES = VadjDims<N>::ES, NN = N * N;
+  constexpr int D = VadjRing<N>::depth;
   const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
   const int64_t col = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= ncol) return;
@@ -956,33 +971,68 @@ __global__ void __launch_bounds__(128) k_vadj_sweep(Geo g, Phys p, AdjBufs b) {
   const double* T = b.vic + col;
   double* S = b.vic + (int64_t)(nl + 2) * E1 * ncol + col;
   double* Z = S + (int64_t)nl * ES * ncol;
-  auto Tat = [&](int t, int e) { return T[((int64_t)t * E1 + e) * ncol]; };
+  auto Tp = [&](int t, int e) { return T + ((int64_t)t * E1 + e) * ncol; };
   auto Sat = [&](int i, int e) -> double& { return S[((int64_t)i * ES + e) * ncol]; };
-  const int oAT = 0, oAH = N * N, oD = 2 * N * N, oT = 2 * N * N + N;
+  const int oAT = 0, oAH = NN, oD = 2 * NN, oT = 2 * NN + N;
+  // T entries of index t: |A| (0), J (NN), du rows (2NN), rho (2NN+N),
+  // output cotangent rows (2NN+N+1), g_fix (2NN+2N+1)
+  const int tA = 0, tJ = NN, tDU = 2 * NN, tRHO = 2 * NN + N, tG = 2 * NN + N + 1,
+            tGF = 2 * NN + 2 * N + 1;
+  extern __shared__ double vadj_ring[];
+  // ring pass: fetch(i, slot) issues layer i's copies; the sweep visits
+  // layers i0, i0+step, ... (n of them)
+  auto prologue = [&](auto fetch, int i0, int step, int n) {
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+      if (k < n) fetch(i0 + k * step, k);
+      else cp_async_commit();
+    }
+  };
+  const int nt = blockDim.x, lane = threadIdx.x;
 
   const double dt = *b.dt;
   const double Aa = g.A1, hiv = 0.5 / g.vol, idt = 1. / dt, grav = p.grav1, V = g.vol;
-  // (1) forward elimination, as k_vic_sweep, keeping ahat_i
+
+  // (1) forward elimination, as the forward column sweep, keeping ahat_i
+  constexpr int E_1 = 2 * NN + N + 1;
+  Ring r1{vadj_ring, E_1, nt, lane};
+  auto fetch1 = [&](int i, int slot) {
+    if (i < nl) {
+#pragma unroll
+      for (int e = 0; e < NN; ++e) cp_async_bytes8(r1.at(slot, e), Tp(i + 1, tA + e));
+#pragma unroll
+      for (int e = 0; e < NN; ++e) cp_async_bytes8(r1.at(slot, NN + e), Tp(i + 2, tJ + e));
+#pragma unroll
+      for (int r = 0; r < N; ++r) cp_async_bytes8(r1.at(slot, 2 * NN + r), Tp(i, tDU + r));
+      cp_async_bytes8(r1.at(slot, 2 * NN + N), Tp(i, tRHO));
+    }
+    cp_async_commit();
+  };
+  prologue(fetch1, 0, 1, D);
   double Am[N][N], Jp[N][N], Jc[N][N], ap[N][N], dp[N];
 #pragma unroll
   for (int r = 0; r < N; ++r)
 #pragma unroll
     for (int q = 0; q < N; ++q) {
-      Am[r][q] = Tat(0, r * N + q);
-      Jp[r][q] = Tat(0, N * N + r * N + q);
-      Jc[r][q] = Tat(1, N * N + r * N + q);
+      Am[r][q] = *Tp(0, tA + r * N + q);
+      Jp[r][q] = *Tp(0, tJ + r * N + q);
+      Jc[r][q] = *Tp(1, tJ + r * N + q);
     }
-  for (int i = 0; i < nl; ++i) {
+  double sum_a2 = 0.;
+  for (int i = 0, slot = 0; i < nl; ++i) {
     double Ap[N][N], Jn[N][N], rhs[N];
+    cp_async_wait<D - 1>();
 #pragma unroll
     for (int r = 0; r < N; ++r) {
-      rhs[r] = Tat(i, 2 * N * N + r) / dt;
+      rhs[r] = *r1.at(slot, 2 * NN + r) / dt;
 #pragma unroll
       for (int q = 0; q < N; ++q) {
-        Ap[r][q] = Tat(i + 1, r * N + q);
-        Jn[r][q] = Tat(i + 2, N * N + r * N + q);
+        Ap[r][q] = *r1.at(slot, r * N + q);
+        Jn[r][q] = *r1.at(slot, NN + r * N + q);
       }
     }
+    const double ai = *r1.at(slot, 2 * NN + N) * V;
+    sum_a2 += ai * ai;
     double a[N][N], bb[N][N], c[N][N];
 #pragma unroll
     for (int r = 0; r < N; ++r)
@@ -1030,6 +1080,8 @@ __global__ void __launch_bounds__(128) k_vadj_sweep(Geo g, Phys p, AdjBufs b) {
 #pragma unroll
       for (int q = 0; q < N; ++q) Sat(i, oAH + r * N + q) = a[r][q];
     block_solve<N>(a, c, rhs);
+    fetch1(i + D, slot);  // consumed: refill
+    slot = slot + 1 == D ? 0 : slot + 1;
 #pragma unroll
     for (int r = 0; r < N; ++r) {
       dp[r] = rhs[r];
@@ -1049,99 +1101,177 @@ __global__ void __launch_bounds__(128) k_vadj_sweep(Geo g, Phys p, AdjBufs b) {
         Jc[r][q] = Jn[r][q];
       }
   }
-  // (2) back substitution
+  cp_async_wait<0>();
+
+  // (2) back substitution, B_dry accumulated from the top as in the forward
+  constexpr int E_2 = NN + N + 1;
+  Ring r2{vadj_ring, E_2, nt, lane};
+  // the reduced block and the partial solution of layer i (not adjacent in S)
+  auto fetch2d = [&](int i, int slot) {
+    if (i >= 0) {
+#pragma unroll
+      for (int e = 0; e < NN; ++e) cp_async_bytes8(r2.at(slot, e), &Sat(i, oAT + e));
+#pragma unroll
+      for (int r = 0; r < N; ++r) cp_async_bytes8(r2.at(slot, NN + r), &Sat(i, oD + r));
+      cp_async_bytes8(r2.at(slot, NN + N), Tp(i, tDU));
+    }
+    cp_async_commit();
+  };
   double dn[N];
 #pragma unroll
   for (int r = 0; r < N; ++r) dn[r] = dp[r];
-  for (int i = nl - 2; i >= 0; --i) {
+  double b_dry = (*Tp(nl - 1, tDU) - dn[0]) * 1. * V;
+  prologue(fetch2d, nl - 2, -1, nl - 1);
+  for (int i = nl - 2, slot = 0; i >= 0; --i) {
+    cp_async_wait<D - 1>();
+    double cur[NN + N];
+#pragma unroll
+    for (int e = 0; e < NN + N; ++e) cur[e] = *r2.at(slot, e);
+    const double du0 = *r2.at(slot, NN + N);
     double d[N];
 #pragma unroll
     for (int r = 0; r < N; ++r) {
       double t = 0.;
 #pragma unroll
-      for (int q = 0; q < N; ++q) t += Sat(i, oAT + r * N + q) * dn[q];
-      d[r] = Sat(i, oD + r) - t;
+      for (int q = 0; q < N; ++q) t += cur[r * N + q] * dn[q];
+      d[r] = cur[NN + r] - t;
     }
+    b_dry += (du0 - d[0]) * 1. * V;
+    fetch2d(i - D, slot);
+    slot = slot + 1 == D ? 0 : slot + 1;
 #pragma unroll
     for (int r = 0; r < N; ++r) {
       dn[r] = d[r];
       Sat(i, oD + r) = d[r];
     }
   }
-  // (3) column sums and the cotangents of the redistribution's B_dry and S
-  double sum_a2 = 0., b_dry = 0.;
-  for (int i = 0; i < nl; ++i) {
-    double ai = Tat(i, 2 * N * N + N) * V;
-    sum_a2 += ai * ai;
-    b_dry += (Tat(i, 2 * N * N) - Sat(i, oD)) * 1. * V;
-  }
+  cp_async_wait<0>();
+
+  // (3) cotangents of the redistribution's B_dry and S
+  Ring r3{vadj_ring, 2, nt, lane};
+  auto fetch3 = [&](int i, int slot) {
+    if (i < nl) {
+      cp_async_bytes8(r3.at(slot, 0), Tp(i, tRHO));
+      cp_async_bytes8(r3.at(slot, 1), Tp(i, tG));  // cotangent of du_out[IDN]
+    }
+    cp_async_commit();
+  };
+  prologue(fetch3, 0, 1, D);
   double gb = 0., gS = 0.;
-  for (int i = 0; i < nl; ++i) {
-    double rho = Tat(i, 2 * N * N + N);
-    double go = Tat(i, 2 * N * N + N + 1);  // cotangent of du_out[IDN]
+  for (int i = 0, slot = 0; i < nl; ++i) {
+    cp_async_wait<D - 1>();
+    const double rho = *r3.at(slot, 0), go = *r3.at(slot, 1);
     gb += go * rho * (rho * V) / sum_a2;
     gS -= go * rho * (rho * V) * b_dry / (sum_a2 * sum_a2);
+    fetch3(i + D, slot);
+    slot = slot + 1 == D ? 0 : slot + 1;
   }
+  cp_async_wait<0>();
   Z[0] = b_dry / sum_a2;
   Z[ncol] = gS;
   Z[2 * ncol] = gb;
+
   // (4) h_i = g_delta_i - a~_{i-1}^T h_{i-1}
+  constexpr int E_4 = N + 1 + NN;
+  Ring r4{vadj_ring, E_4, nt, lane};
+  auto fetch4 = [&](int i, int slot) {
+    if (i < nl) {
+#pragma unroll
+      for (int r = 0; r < N; ++r) cp_async_bytes8(r4.at(slot, r), Tp(i, tG + r));
+      cp_async_bytes8(r4.at(slot, N), Tp(i, tGF));
+      if (i > 0) {
+#pragma unroll
+        for (int e = 0; e < NN; ++e) cp_async_bytes8(r4.at(slot, N + 1 + e), &Sat(i - 1, oAT + e));
+      }
+    }
+    cp_async_commit();
+  };
+  prologue(fetch4, 0, 1, D);
   double hp[N];
 #pragma unroll
   for (int r = 0; r < N; ++r) hp[r] = 0.;
-  for (int i = 0; i < nl; ++i) {
+  for (int i = 0, slot = 0; i < nl; ++i) {
+    cp_async_wait<D - 1>();
     double h[N];
 #pragma unroll
-    for (int r = 0; r < N; ++r) h[r] = Tat(i, 2 * N * N + N + 1 + r);
-    h[0] += -V * gb + Tat(i, 2 * N * N + 2 * N + 1);
+    for (int r = 0; r < N; ++r) h[r] = *r4.at(slot, r);
+    h[0] += -V * gb + *r4.at(slot, N);
     if (i > 0) {
 #pragma unroll
       for (int q = 0; q < N; ++q) {
-        double s = 0.;
+        double sacc = 0.;
 #pragma unroll
-        for (int r = 0; r < N; ++r) s += Sat(i - 1, oAT + r * N + q) * hp[r];
-        h[q] -= s;
+        for (int r = 0; r < N; ++r) sacc += *r4.at(slot, N + 1 + r * N + q) * hp[r];
+        h[q] -= sacc;
       }
     }
+    fetch4(i + D, slot);
+    slot = slot + 1 == D ? 0 : slot + 1;
 #pragma unroll
     for (int r = 0; r < N; ++r) {
       hp[r] = h[r];
       Sat(i, oT + r) = h[r];
     }
   }
+  cp_async_wait<0>();
+
   // (5) t_i = ahat_i^-T (h_i - b_{i+1}^T t_{i+1}),
   //     b_{i+1} = -(|A|_{face i+1} + J_{cell i}) A hiv
+  constexpr int E_5 = 3 * NN + N;
+  Ring r5{vadj_ring, E_5, nt, lane};
+  auto fetch5 = [&](int i, int slot) {
+    if (i >= 0) {
+#pragma unroll
+      for (int r = 0; r < N; ++r) cp_async_bytes8(r5.at(slot, r), &Sat(i, oT + r));
+#pragma unroll
+      for (int e = 0; e < NN; ++e) cp_async_bytes8(r5.at(slot, N + e), &Sat(i, oAH + e));
+      if (i + 1 < nl) {
+#pragma unroll
+        for (int e = 0; e < NN; ++e) {
+          cp_async_bytes8(r5.at(slot, N + NN + e), Tp(i + 1, tA + e));
+          cp_async_bytes8(r5.at(slot, N + 2 * NN + e), Tp(i + 1, tJ + e));
+        }
+      }
+    }
+    cp_async_commit();
+  };
+  prologue(fetch5, nl - 1, -1, nl);
   double tn[N];
 #pragma unroll
   for (int r = 0; r < N; ++r) tn[r] = 0.;
-  for (int i = nl - 1; i >= 0; --i) {
+  for (int i = nl - 1, slot = 0; i >= 0; --i) {
+    cp_async_wait<D - 1>();
     double y[N];
 #pragma unroll
-    for (int r = 0; r < N; ++r) y[r] = Sat(i, oT + r);
+    for (int r = 0; r < N; ++r) y[r] = *r5.at(slot, r);
     if (i + 1 < nl) {
 #pragma unroll
       for (int q = 0; q < N; ++q) {
-        double s = 0.;
+        double sacc = 0.;
 #pragma unroll
         for (int r = 0; r < N; ++r) {
-          double bq = -(Tat(i + 1, r * N + q) + Tat(i + 1, N * N + r * N + q)) * Aa * hiv;
-          s += bq * tn[r];
+          double bq = -(*r5.at(slot, N + NN + r * N + q) + *r5.at(slot, N + 2 * NN + r * N + q)) *
+                      Aa * hiv;
+          sacc += bq * tn[r];
         }
-        y[q] -= s;
+        y[q] -= sacc;
       }
     }
     double M[N][N];
 #pragma unroll
     for (int r = 0; r < N; ++r)
 #pragma unroll
-      for (int q = 0; q < N; ++q) M[r][q] = Sat(i, oAH + r * N + q);
+      for (int q = 0; q < N; ++q) M[r][q] = *r5.at(slot, N + r * N + q);
     solve_transposed<N>(M, y);
+    fetch5(i - D, slot);
+    slot = slot + 1 == D ? 0 : slot + 1;
 #pragma unroll
     for (int r = 0; r < N; ++r) {
       tn[r] = y[r];
       Sat(i, oT + r) = y[r];
     }
   }
+  cp_async_wait<0>();
 }
 
 // d/dw of y^T |A|(wl, wr) x, one primitive slot of one side per dual pass
@@ -1311,8 +1441,9 @@ static cudaError_t launch_vic_adj_n(const Geo& g, const Phys& p, const AdjBufs& 
   const int nl = g.nx1;
   dim3 ga((unsigned)((ncol + kATC - 1) / kATC), (unsigned)((nl + 2 + kATL<N> - 1) / kATL<N>));
   k_vadj_assemble<N, NS><<<ga, 256, 0, st>>>(g, p, b);
-  int bs = ncol >= 148 * 128 ? 128 : (ncol >= 148 * 64 ? 64 : 32);
-  k_vadj_sweep<N><<<(unsigned)((ncol + bs - 1) / bs), bs, 0, st>>>(g, p, b);
+  // the ring takes vadj_ring_bytes per thread: 32-thread CTAs
+  const int bs = 32;
+  k_vadj_sweep<N><<<(unsigned)((ncol + bs - 1) / bs), bs, vadj_ring_bytes<N>(bs), st>>>(g, p, b);
   dim3 gc((unsigned)((ncol + kCTC - 1) / kCTC), (unsigned)((nl + 2 + kCTL - 1) / kCTL));
   k_vadj_contract<N, NS><<<gc, 128, 0, st>>>(g, p, b);
   return cudaGetLastError();

@@ -23,6 +23,7 @@ struct StageBufs {
   double* R;         // [nscalar][sv] scalar mixing ratio of the stage input
   double* M;         // [nvar][sv] implicit mass correction (IDN row used)
   double* vic;       // implicit-solve scratch
+  double* vicT;      // per-layer |A| and J blocks (split column sweep), or null
   int stage;
   double wgt0, wgt1, wgt2;
   int write_du;      // 1: finalize writes du into D instead of updating u
@@ -166,6 +167,7 @@ cudaError_t launch_diffusion(const Geo& g, const Phys& p, const StageBufs& b, cu
 cudaError_t launch_vic(const Geo& g, const Phys& p, const StageBufs& b, cudaStream_t st);
 cudaError_t launch_vic32(const Geo& g, const Phys& p, const StageBufs32& b, cudaStream_t st);
 size_t vic_scratch_bytes(const Geo& g, const Phys& p);
+size_t vic_blocks_bytes(const Geo& g, const Phys& p);
 
 cudaError_t launch_cons2prim(const Geo& g, const Phys& p, const double* u, double* w,
                              cudaStream_t st);

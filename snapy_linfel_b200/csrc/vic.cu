@@ -29,6 +29,7 @@
 #include <string>
 
 #include "kernels.cuh"
+#include "ring.cuh"
 #include "vic_blocks.cuh"
 
 namespace snapb {
@@ -56,6 +57,25 @@ size_t vic_scratch_bytes(const Geo& g, const Phys& p) {
   return (size_t)(nl * es * ncol + 2 * ncol) * sizeof(double);
 }
 
+// Few columns (2-D domains, thin 3-D ones) leave most of the GPU idle with one
+// thread per column: the blocks |A| (per face) and J (per cell) are then
+// formed by a fully parallel kernel first, so the sequential sweep only
+// eliminates.  Scratch T [nl+2][2 N*N][ncol]: index t holds |A| of the face
+// between cells t-1 and t, and J of cell t-1.
+constexpr int64_t kSplitMaxCols = 8192;
+
+bool vic_split(const Geo& g, const Phys& p) {
+  const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
+  return p.implicit_scheme != 0 && ncol <= kSplitMaxCols;
+}
+
+size_t vic_blocks_bytes(const Geo& g, const Phys& p) {
+  if (!vic_split(g, p)) return 0;
+  int N = vic_n(p);
+  int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
+  return (size_t)((int64_t)(g.nx1 + 2) * 2 * N * N * ncol) * sizeof(double);
+}
+
 constexpr int kTC = 32;  // columns per tile
 constexpr int kTL = 32;  // layers per tile (redistribution)
 
@@ -78,27 +98,6 @@ constexpr size_t back_ring_bytes(int threads) {
   return (size_t)threads * BackRing<N>::depth * BackRing<N>::elems * sizeof(double);
 }
 
-__device__ __forceinline__ void cp_async_bytes8(void* smem, const void* gmem) {
-  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_bytes4(void* smem, const void* gmem) {
-  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
-template <int n>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(n) : "memory");
-}
-__device__ __forceinline__ void cp_async_elem(void* smem, const double* g) { cp_async_bytes8(smem, g); }
-__device__ __forceinline__ void cp_async_elem(void* smem, const float* g) { cp_async_bytes4(smem, g); }
-__device__ __forceinline__ double ring_elem(const double* slot, const double*) { return *slot; }
-__device__ __forceinline__ double ring_elem(const double* slot, const float*) {
-  return (double)*reinterpret_cast<const float*>(slot);
-}
 
 // (k, j, il) offset of interior column `col`
 __device__ __forceinline__ int64_t column_base(const Geo& g, int64_t col) {
@@ -208,6 +207,118 @@ __device__ __forceinline__ void jac_of(const StageBufs32&, double gm1, const dou
     for (int q = 0; q < N; ++q) J[r][q] = (double)F[r][q];
 }
 
+// One layer of the block-Thomas forward elimination: a_i, b_i, c_i from |A|
+// at the layer's lower / upper faces (Am, Ap) and J of the cells below /
+// above (Jp, Jn); the previous reduced block and partial solution (ap, dp)
+// are eliminated, and c (reduced block) and rhs (partial solution) return the
+// new ones.  The same arithmetic for the fused and the split sweeps.
+template <int N, class BT>
+__device__ __forceinline__ void vic_layer(const BT (&Am)[N][N], const BT (&Ap)[N][N],
+                                          const BT (&Jp)[N][N], const BT (&Jn)[N][N],
+                                          const double (&ap)[N][N], const double (&dp)[N],
+                                          double (&rhs)[N], double (&c)[N][N], int i, int nl,
+                                          double Aa, double hiv, double idt, double grav) {
+  double a[N][N], bb[N][N];
+#pragma unroll
+  for (int r = 0; r < N; ++r)
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+      double phi = 0.;
+      if (r == 1 && q == 0) phi = grav;
+      if (N == 3 && r == 2 && q == 1) phi = grav;
+      if (N == 5 && r == IPR && q == IVX) phi = grav;
+      a[r][q] = (Am[r][q] * Aa + Ap[r][q] * Aa) * hiv - phi;
+      bb[r][q] = -(Am[r][q] + Jp[r][q]) * Aa * hiv;
+      c[r][q] = -(Ap[r][q] - Jn[r][q]) * Aa * hiv;
+    }
+#pragma unroll
+  for (int r = 0; r < N; ++r) a[r][r] += idt;
+  if (i == 0) {
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+      for (int q = 0; q < N; ++q) a[r][q] += bb[r][q] * (q == 1 ? -1. : 1.);
+  }
+  if (i == nl - 1) {
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+      for (int q = 0; q < N; ++q) a[r][q] += c[r][q] * (q == 1 ? -1. : 1.);
+  }
+  if (i > 0) {
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      double bd = 0.;
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        double t = 0.;
+#pragma unroll
+        for (int kk = 0; kk < N; ++kk) t += bb[r][kk] * ap[kk][q];
+        a[r][q] -= t;
+        bd += bb[r][q] * dp[q];
+      }
+      rhs[r] = rhs[r] - bd;
+    }
+  }
+  block_solve<N>(a, c, rhs);
+}
+
+// Back substitution delta_i -= a'_i delta_{i+1} and the MS-VIC column sums
+// (sum (rho V)^2 from the forward sweep, B_dry accumulated here); the inputs
+// of each layer arrive through the thread's shared-memory ring.
+template <int N, class B>
+__device__ __forceinline__ void vic_back(const B& b, double* S, double* Z, int64_t ncol,
+                                         int64_t sv, int64_t cb, int nl, const double (&dp)[N],
+                                         double sum_a2, double V) {
+  constexpr int ES = VicDims<N>::ES;
+  constexpr int DB = BackRing<N>::depth, RE = BackRing<N>::elems;
+  extern __shared__ double vic_ring[];
+  const int nt = blockDim.x, lane = threadIdx.x;
+  auto Sat = [&](int i, int e) -> double& { return S[((int64_t)i * ES + e) * ncol]; };
+  cp_async_wait<0>();  // the forward ring is drained before its memory is reused
+  auto ring = [&](int slot, int e) { return vic_ring + ((size_t)(slot * RE + e) * nt + lane); };
+  auto fetch = [&](int i, int slot) {
+    if (i >= 0) {
+#pragma unroll
+      for (int e = 0; e < ES; ++e) cp_async_bytes8(ring(slot, e), &Sat(i, e));
+      cp_async_elem(ring(slot, ES), b.D + IDN * sv + cb + i);
+    }
+    cp_async_commit();
+  };
+  double dn[N];
+#pragma unroll
+  for (int r = 0; r < N; ++r) dn[r] = dp[r];
+  double b_dry = (vic_d(b, IDN * sv + cb + nl - 1) - dn[0]) * 1. * V;
+#pragma unroll
+  for (int k = 0; k < DB; ++k) fetch(nl - 2 - k, k);
+  for (int i = nl - 2, slot = 0; i >= 0; --i) {
+    cp_async_wait<DB - 1>();  // the group of layer i has landed
+    double cur[ES];
+#pragma unroll
+    for (int e = 0; e < ES; ++e) cur[e] = *ring(slot, e);
+    const double dcur = ring_elem(ring(slot, ES), b.D);
+    double d[N];
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      double t = 0.;
+#pragma unroll
+      for (int q = 0; q < N; ++q) t += cur[r * N + q] * dn[q];
+      d[r] = cur[N * N + r] - t;
+    }
+    b_dry += (dcur - d[0]) * 1. * V;
+    fetch(i - DB, slot);  // the slot's values are consumed: refill it
+    slot = slot + 1 == DB ? 0 : slot + 1;
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      dn[r] = d[r];
+      Sat(i, N * N + r) = d[r];
+    }
+  }
+  cp_async_wait<0>();
+  Z[0] = sum_a2;
+  Z[ncol] = b_dry;
+}
+
 // (1) one thread per column: blocks formed a layer ahead of the
 // block-Thomas elimination, back substitution and the column sums.  Loads of
 // a layer's w and du go 32 columns apart across a warp; the next layers of
@@ -271,49 +382,8 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
     jac_of<N>(b, gm1c, wn, Jn);
     double ai = wc[IDN] * V;
     sum_a2 += ai * ai;
-    double a[N][N], bb[N][N], c[N][N];
-#pragma unroll
-    for (int r = 0; r < N; ++r)
-#pragma unroll
-      for (int q = 0; q < N; ++q) {
-        double phi = 0.;
-        if (r == 1 && q == 0) phi = grav;
-        if (N == 3 && r == 2 && q == 1) phi = grav;
-        if (N == 5 && r == IPR && q == IVX) phi = grav;
-        a[r][q] = (Am[r][q] * Aa + Ap[r][q] * Aa) * hiv - phi;
-        bb[r][q] = -(Am[r][q] + Jp[r][q]) * Aa * hiv;
-        c[r][q] = -(Ap[r][q] - Jn[r][q]) * Aa * hiv;
-      }
-#pragma unroll
-    for (int r = 0; r < N; ++r) a[r][r] += idt;
-    if (i == 0) {
-#pragma unroll
-      for (int r = 0; r < N; ++r)
-#pragma unroll
-        for (int q = 0; q < N; ++q) a[r][q] += bb[r][q] * (q == 1 ? -1. : 1.);
-    }
-    if (i == nl - 1) {
-#pragma unroll
-      for (int r = 0; r < N; ++r)
-#pragma unroll
-        for (int q = 0; q < N; ++q) a[r][q] += c[r][q] * (q == 1 ? -1. : 1.);
-    }
-    if (i > 0) {
-#pragma unroll
-      for (int r = 0; r < N; ++r) {
-        double bd = 0.;
-#pragma unroll
-        for (int q = 0; q < N; ++q) {
-          double t = 0.;
-#pragma unroll
-          for (int kk = 0; kk < N; ++kk) t += bb[r][kk] * ap[kk][q];
-          a[r][q] -= t;
-          bd += bb[r][q] * dp[q];
-        }
-        rhs[r] = rhs[r] - bd;
-      }
-    }
-    block_solve<N>(a, c, rhs);
+    double c[N][N];
+    vic_layer<N>(Am, Ap, Jp, Jn, ap, dp, rhs, c, i, nl, Aa, hiv, idt, grav);
     // the slot's values are consumed (the solve depends on them): refill it
     ffetch(i + 1 + DF, fslot);
     fslot = fslot + 1 == DF ? 0 : fslot + 1;
@@ -338,51 +408,143 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
 #pragma unroll
     for (int v = 0; v < 5; ++v) wc[v] = wn[v];
   }
-  // back substitution: delta_i -= a'_i delta_{i+1}; B_dry accumulated on the
-  // way, the inputs of each layer arriving through the shared-memory ring.
-  constexpr int DB = BackRing<N>::depth, RE = BackRing<N>::elems;
-  cp_async_wait<0>();  // the forward ring is drained before its memory is reused
-  auto ring = [&](int slot, int e) { return vic_ring + ((size_t)(slot * RE + e) * nt + lane); };
-  auto fetch = [&](int i, int slot) {
-    if (i >= 0) {
+  vic_back<N>(b, S, Z, ncol, sv, cb, nl, dp, sum_a2, V);
+}
+
+// ---- split sweep (few columns): blocks first, then the elimination ----
+template <int N>
+struct PreRing {
+  static constexpr int elems = 2 * N * N + N + 1;  // A_{i+1}, J_{i+2}, du rows, rho
+};
+template <int N>
+constexpr size_t pre_ring_bytes(int threads) {
+  return (size_t)threads * sizeof(double) *
+         (kFwdDepth * PreRing<N>::elems > BackRing<N>::depth * BackRing<N>::elems
+              ? kFwdDepth * PreRing<N>::elems
+              : BackRing<N>::depth * BackRing<N>::elems);
+}
+
+// one thread per (column, t), t in [0, nl+1], column fastest (coalesced stores)
+template <int N>
+__global__ void __launch_bounds__(256) k_vic_blocks(Geo g, Phys p, StageBufs b) {
+  constexpr int NN = N * N;
+  const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
+  const int nl = g.nx1;
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= ncol * (nl + 2)) return;
+  const int64_t col = idx - (int64_t)udiv(idx, ncol) * ncol;
+  const int t = udiv(idx, ncol);
+  const int64_t sv = g.sv, cb = column_base(g, col);
+  const double gm1c = p.gammad - 1.;
+  const double gm1f = 0.5 * (p.gammad + p.gammad) - 1.;
+  double wl[5], wr[5];
 #pragma unroll
-      for (int e = 0; e < ES; ++e) cp_async_bytes8(ring(slot, e), &Sat(i, e));
-      cp_async_elem(ring(slot, ES), b.D + IDN * sv + cb + i);
+  for (int v = 0; v < 5; ++v) wl[v] = b.w[v * sv + cb + t - 1];
+  double* out = b.vicT + (int64_t)t * 2 * NN * ncol + col;
+  double J[N][N];
+  jac_of<N>(b, gm1c, wl, J);
+#pragma unroll
+  for (int r = 0; r < N; ++r)
+#pragma unroll
+    for (int q = 0; q < N; ++q) out[(NN + r * N + q) * ncol] = J[r][q];
+  if (t <= nl) {
+#pragma unroll
+    for (int v = 0; v < 5; ++v) wr[v] = b.w[v * sv + cb + t];
+    double A[N][N];
+    absA_of<N>(b, gm1f, wl, wr, A);
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+      for (int q = 0; q < N; ++q) out[(r * N + q) * ncol] = A[r][q];
+  }
+}
+
+// the elimination of one column from the precomputed blocks
+template <int N>
+__global__ void __launch_bounds__(128) k_vic_column_pre(Geo g, Phys p, StageBufs b) {
+  constexpr int ES = VicDims<N>::ES, NN = N * N, DF = kFwdDepth, FE = PreRing<N>::elems;
+  const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
+  const int64_t col = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= ncol) return;
+  const int nl = g.nx1;
+  const int64_t sv = g.sv;
+  const int64_t cb = column_base(g, col);
+  double* S = b.vic + col;
+  double* Z = S + (int64_t)nl * ES * ncol;
+  auto Sat = [&](int i, int e) -> double& { return S[((int64_t)i * ES + e) * ncol]; };
+  const double* T = b.vicT + col;
+  auto Tat = [&](int t, int e) { return T + ((int64_t)t * 2 * NN + e) * ncol; };
+  extern __shared__ double vic_ring[];
+  const int nt = blockDim.x, lane = threadIdx.x;
+  auto fring = [&](int slot, int e) { return vic_ring + ((size_t)(slot * FE + e) * nt + lane); };
+  auto ffetch = [&](int i, int slot) {  // layer i: A_{i+1}, J_{i+2}, du rows and rho of cell i
+    if (i < nl) {
+#pragma unroll
+      for (int e = 0; e < NN; ++e) cp_async_bytes8(fring(slot, e), Tat(i + 1, e));
+#pragma unroll
+      for (int e = 0; e < NN; ++e) cp_async_bytes8(fring(slot, NN + e), Tat(i + 2, NN + e));
+#pragma unroll
+      for (int r = 0; r < N; ++r)
+        cp_async_bytes8(fring(slot, 2 * NN + r), b.D + sel<N>(r) * sv + cb + i);
+      cp_async_bytes8(fring(slot, 2 * NN + N), b.w + IDN * sv + cb + i);
     }
     cp_async_commit();
   };
-  double dn[N];
 #pragma unroll
-  for (int r = 0; r < N; ++r) dn[r] = dp[r];
-  double b_dry = (vic_d(b, IDN * sv + cb + nl - 1) - dn[0]) * 1. * V;
+  for (int k = 0; k < DF; ++k) ffetch(k, k);
+  const double dt = *b.dt;
+  const double Aa = g.A1, hiv = 0.5 / g.vol, idt = 1. / dt, grav = p.grav1, V = g.vol;
+  double Am[N][N], Jp[N][N], Jc[N][N], ap[N][N], dp[N];
 #pragma unroll
-  for (int k = 0; k < DB; ++k) fetch(nl - 2 - k, k);
-  for (int i = nl - 2, slot = 0; i >= 0; --i) {
-    cp_async_wait<DB - 1>();  // the group of layer i has landed
-    double cur[ES];
+  for (int r = 0; r < N; ++r)
 #pragma unroll
-    for (int e = 0; e < ES; ++e) cur[e] = *ring(slot, e);
-    const double dcur = ring_elem(ring(slot, ES), b.D);
-    double d[N];
+    for (int q = 0; q < N; ++q) {
+      Am[r][q] = *Tat(0, r * N + q);
+      Jp[r][q] = *Tat(0, NN + r * N + q);
+      Jc[r][q] = *Tat(1, NN + r * N + q);
+      ap[r][q] = 0.;
+    }
+#pragma unroll
+  for (int r = 0; r < N; ++r) dp[r] = 0.;
+  double sum_a2 = 0.;
+  for (int i = 0, fslot = 0; i < nl; ++i) {
+    double Ap[N][N], Jn[N][N], rhs[N];
+    cp_async_wait<DF - 1>();  // the group of layer i has landed
 #pragma unroll
     for (int r = 0; r < N; ++r) {
-      double t = 0.;
+      rhs[r] = *fring(fslot, 2 * NN + r) / dt;
 #pragma unroll
-      for (int q = 0; q < N; ++q) t += cur[r * N + q] * dn[q];
-      d[r] = cur[N * N + r] - t;
+      for (int q = 0; q < N; ++q) {
+        Ap[r][q] = *fring(fslot, r * N + q);
+        Jn[r][q] = *fring(fslot, NN + r * N + q);
+      }
     }
-    b_dry += (dcur - d[0]) * 1. * V;
-    fetch(i - DB, slot);  // the slot's values are consumed: refill it
-    slot = slot + 1 == DB ? 0 : slot + 1;
+    const double ai = *fring(fslot, 2 * NN + N) * V;
+    sum_a2 += ai * ai;
+    double c[N][N];
+    vic_layer<N>(Am, Ap, Jp, Jn, ap, dp, rhs, c, i, nl, Aa, hiv, idt, grav);
+    ffetch(i + DF, fslot);  // the slot's values are consumed: refill it
+    fslot = fslot + 1 == DF ? 0 : fslot + 1;
 #pragma unroll
     for (int r = 0; r < N; ++r) {
-      dn[r] = d[r];
-      Sat(i, N * N + r) = d[r];
+      dp[r] = rhs[r];
+      __stcs(&Sat(i, NN + r), rhs[r]);
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        ap[r][q] = c[r][q];
+        __stcs(&Sat(i, r * N + q), c[r][q]);
+      }
     }
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        Am[r][q] = Ap[r][q];
+        Jp[r][q] = Jc[r][q];
+        Jc[r][q] = Jn[r][q];
+      }
   }
-  cp_async_wait<0>();
-  Z[0] = sum_a2;
-  Z[ncol] = b_dry;
+  vic_back<N>(b, S, Z, ncol, sv, cb, nl, dp, sum_a2, V);
 }
 
 // the ring of a 128-thread CTA exceeds the default 48 KB of dynamic shared
@@ -533,9 +695,22 @@ static cudaError_t launch_vic_n(const Geo& g, const Phys& p, const B& b, cudaStr
   const int nl = g.nx1;
   // small column counts: narrower CTAs spread the sequential sweeps over more SMs
   int bs = ncol >= 148 * 128 ? 128 : (ncol >= 148 * 64 ? 64 : 32);
-  allow_ring_smem(k_vic_column<N, B>, back_ring_bytes<N>(128));
-  k_vic_column<N, B><<<(unsigned)((ncol + bs - 1) / bs), bs, back_ring_bytes<N>(bs), st>>>(g, p,
-                                                                                      b);
+  bool split = false;
+  if constexpr (std::is_same_v<B, StageBufs>) split = b.vicT != nullptr;
+  if constexpr (std::is_same_v<B, StageBufs>) {
+    if (split) {
+      const int64_t nb = ncol * (nl + 2);
+      k_vic_blocks<N><<<(unsigned)((nb + 255) / 256), 256, 0, st>>>(g, p, b);
+      allow_ring_smem(k_vic_column_pre<N>, pre_ring_bytes<N>(128));
+      k_vic_column_pre<N><<<(unsigned)((ncol + bs - 1) / bs), bs, pre_ring_bytes<N>(bs), st>>>(
+          g, p, b);
+    }
+  }
+  if (!split) {
+    allow_ring_smem(k_vic_column<N, B>, back_ring_bytes<N>(128));
+    k_vic_column<N, B><<<(unsigned)((ncol + bs - 1) / bs), bs, back_ring_bytes<N>(bs), st>>>(
+        g, p, b);
+  }
   dim3 gf((unsigned)((ncol + kTC - 1) / kTC), (unsigned)((nl + kTL - 1) / kTL));
   switch (p.nscalar) {
     case 0: k_vic_finish<N, 0, B><<<gf, kFinThreads, 0, st>>>(g, p, b); break;
