@@ -783,6 +783,9 @@ def run_adjoint_check(args):
             ad = float((grad * v).sum())
             errs.append(abs(fd - ad) / max(abs(fd), abs(ad), 1e-300))
     cells = interior_cells(cfg)
+    # one step's reverse (from kept stage inputs) against one forward step
+    stream = torch.cuda.current_stream()
+    per_step = run_adjoint_timing(args, opts, (w, None), cells, stream, torch.cuda.synchronize)
     line = {
         "metric": METRIC, "value": cells * 3 * nsteps / (bwd_ms / 1e3) / 1e6, "unit": UNIT,
         "n_gpus": 1, "steps": nsteps, "warmup": 1, "ms_per_step": bwd_ms / nsteps,
@@ -793,6 +796,11 @@ def run_adjoint_check(args):
                    "value_is": "reverse (checkpointed backward) cell-updates per second"},
         "adjoint": {"forward_ms": fwd_ms, "backward_ms": bwd_ms,
                     "backward_over_forward": bwd_ms / fwd_ms,
+                    "step": {"forward_ms": per_step["forward_ms_per_step"],
+                             "reverse_ms": per_step["reverse_ms_per_step"],
+                             "reverse_over_forward": per_step["adjoint_over_forward"],
+                             "reverse_kernel_ms_per_stage":
+                                 per_step["reverse_kernel_ms_per_stage"]},
                     "fd_directions": len(errs), "fd_rel_err_max": max(errs),
                     "fd_rel_err_median": float(np.median(errs)),
                     "fd_within_1e-6": int(sum(e < 1e-6 for e in errs)),

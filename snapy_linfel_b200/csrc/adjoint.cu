@@ -994,7 +994,7 @@ __global__ void __launch_bounds__(128) k_vadj_sweep(Geo g, Phys p, AdjBufs b) {
   const double Aa = g.A1, hiv = 0.5 / g.vol, idt = 1. / dt, grav = p.grav1, V = g.vol;
 
   // (1) forward elimination, as the forward column sweep, keeping ahat_i
-  constexpr int E_1 = 2 * NN + N + 1;
+  constexpr int E_1 = 2 * NN + N + 2;
   Ring r1{vadj_ring, E_1, nt, lane};
   auto fetch1 = [&](int i, int slot) {
     if (i < nl) {
@@ -1005,6 +1005,7 @@ __global__ void __launch_bounds__(128) k_vadj_sweep(Geo g, Phys p, AdjBufs b) {
 #pragma unroll
       for (int r = 0; r < N; ++r) cp_async_bytes8(r1.at(slot, 2 * NN + r), Tp(i, tDU + r));
       cp_async_bytes8(r1.at(slot, 2 * NN + N), Tp(i, tRHO));
+      cp_async_bytes8(r1.at(slot, 2 * NN + N + 1), Tp(i, tG));  // cotangent of du_out[IDN]
     }
     cp_async_commit();
   };
@@ -1018,7 +1019,9 @@ __global__ void __launch_bounds__(128) k_vadj_sweep(Geo g, Phys p, AdjBufs b) {
       Jp[r][q] = *Tp(0, tJ + r * N + q);
       Jc[r][q] = *Tp(1, tJ + r * N + q);
     }
-  double sum_a2 = 0.;
+  // sum (rho V)^2 and Q = sum g_out[IDN] rho (rho V): the redistribution's
+  // cotangents are g_B = Q / S and g_S = -Q B_dry / S^2
+  double sum_a2 = 0., qg = 0.;
   for (int i = 0, slot = 0; i < nl; ++i) {
     double Ap[N][N], Jn[N][N], rhs[N];
     cp_async_wait<D - 1>();
@@ -1031,8 +1034,9 @@ __global__ void __launch_bounds__(128) k_vadj_sweep(Geo g, Phys p, AdjBufs b) {
         Jn[r][q] = *r1.at(slot, NN + r * N + q);
       }
     }
-    const double ai = *r1.at(slot, 2 * NN + N) * V;
+    const double rho = *r1.at(slot, 2 * NN + N), ai = rho * V;
     sum_a2 += ai * ai;
+    qg += *r1.at(slot, 2 * NN + N + 1) * rho * ai;
     double a[N][N], bb[N][N], c[N][N];
 #pragma unroll
     for (int r = 0; r < N; ++r)
@@ -1148,25 +1152,7 @@ __global__ void __launch_bounds__(128) k_vadj_sweep(Geo g, Phys p, AdjBufs b) {
   cp_async_wait<0>();
 
   // (3) cotangents of the redistribution's B_dry and S
-  Ring r3{vadj_ring, 2, nt, lane};
-  auto fetch3 = [&](int i, int slot) {
-    if (i < nl) {
-      cp_async_bytes8(r3.at(slot, 0), Tp(i, tRHO));
-      cp_async_bytes8(r3.at(slot, 1), Tp(i, tG));  // cotangent of du_out[IDN]
-    }
-    cp_async_commit();
-  };
-  prologue(fetch3, 0, 1, D);
-  double gb = 0., gS = 0.;
-  for (int i = 0, slot = 0; i < nl; ++i) {
-    cp_async_wait<D - 1>();
-    const double rho = *r3.at(slot, 0), go = *r3.at(slot, 1);
-    gb += go * rho * (rho * V) / sum_a2;
-    gS -= go * rho * (rho * V) * b_dry / (sum_a2 * sum_a2);
-    fetch3(i + D, slot);
-    slot = slot + 1 == D ? 0 : slot + 1;
-  }
-  cp_async_wait<0>();
+  const double gb = qg / sum_a2, gS = -qg * b_dry / (sum_a2 * sum_a2);
   Z[0] = b_dry / sum_a2;
   Z[ncol] = gS;
   Z[2 * ncol] = gb;
