@@ -107,6 +107,19 @@ __device__ __forceinline__ bool queue_next(const WorkQueue& q, int& m, int64_t& 
   return true;
 }
 
+// Copy member m's descriptor into shared memory, whole CTA, then barrier.  Call
+// it right after queue_next (whose leading barrier ends the previous tile).
+// Kernels then read the fields as they need them instead of holding the
+// ~50-word struct in registers for the whole tile.
+__device__ __forceinline__ void load_member(Member32& dst, const Member32* mem, int m) {
+  static_assert(sizeof(Member32) % sizeof(int) == 0, "member descriptor copy");
+  const int* src = reinterpret_cast<const int*>(mem + m);
+  int* d = reinterpret_cast<int*>(&dst);
+  for (int k = threadIdx.x; k < (int)(sizeof(Member32) / sizeof(int)); k += blockDim.x)
+    d[k] = src[k];
+  __syncthreads();
+}
+
 // Persistent grid of a batched launch: as many CTAs as fit on the GPU at once
 // (the occupancy calculator's blocks per SM, optionally capped), never more
 // than there are work items.

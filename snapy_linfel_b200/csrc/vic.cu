@@ -749,17 +749,13 @@ template <int N, int V>
 __global__ void __launch_bounds__(128, V == 0 ? 1 : (V == 1 ? 3 : 4))
     k_vic_column_batch(const Member32* __restrict__ mem, Phys p, WorkQueue q, int stage) {
   // The member's descriptor is read from shared memory as the sweep needs its
-  // fields instead of being copied into registers (~50 of them) for the tile.
+  // fields instead of being copied into registers (~50 of them) for the tile
+  // (for the sweeps of stage32.cu the compiler hoists those reads and spills).
   __shared__ Member32 s_mem;
-  static_assert(sizeof(Member32) % sizeof(int) == 0, "member descriptor copy");
   int m;
   int64_t tile;
   while (queue_next(q, m, tile)) {  // (starts with a barrier: the last tile is done)
-    const int* src = reinterpret_cast<const int*>(mem + m);
-    int* dst = reinterpret_cast<int*>(&s_mem);
-    for (int k = threadIdx.x; k < (int)(sizeof(Member32) / sizeof(int)); k += blockDim.x)
-      dst[k] = src[k];
-    __syncthreads();
+    load_member(s_mem, mem, m);
     const int64_t col = tile * s_mem.vic_cols + threadIdx.x;
     if ((int)threadIdx.x < s_mem.vic_cols) vic_column<N, StageBufs32>(s_mem.g, p, s_mem.b, col);
   }
@@ -773,11 +769,7 @@ __global__ void __launch_bounds__(kFinThreads, 2) k_vic_finish_batch(const Membe
   int m;
   int64_t tile;
   while (queue_next(q, m, tile)) {  // (starts with a barrier: the last tile is done)
-    const int* src = reinterpret_cast<const int*>(mem + m);
-    int* dst = reinterpret_cast<int*>(&s_mem);
-    for (int k = threadIdx.x; k < (int)(sizeof(Member32) / sizeof(int)); k += blockDim.x)
-      dst[k] = src[k];
-    __syncthreads();
+    load_member(s_mem, mem, m);
     if (threadIdx.x == 0) set_stage_vic32(s_mem.b, stage);
     __syncthreads();
     const int nlb = (s_mem.g.nx1 + kTL - 1) / kTL;
