@@ -158,7 +158,7 @@ size_t x1_smem32_per_column(const Geo& g, int nvt);
 StageBufs32 bufs32_of(const snapb_hydro_config& c, void* ws);
 size_t workspace_size_f32_of(const snapb_hydro_config& c);
 constexpr int kVicFinishCols = 32;    // columns per implicit-finish tile
-constexpr int kVicFinishLayers = 32;  // layers per implicit-finish tile
+constexpr int kVicFinishLayers = 16;  // layers per implicit-finish tile
 
 // RK3 (Shu-Osher) stage weights: u = wgt0*u0 + wgt1*u + wgt2*du
 inline void rk3_weights(int stage, double& a, double& b, double& c) {

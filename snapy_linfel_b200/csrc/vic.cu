@@ -77,7 +77,7 @@ size_t vic_blocks_bytes(const Geo& g, const Phys& p) {
 }
 
 constexpr int kTC = 32;  // columns per tile
-constexpr int kTL = 32;  // layers per tile (redistribution)
+constexpr int kTL = 16;  // layers per tile (redistribution)
 
 // Back substitution: the reduced block, partial solution and du[IDN] of a
 // layer are fetched kBackDepth<N> layers ahead into a per-thread ring in
@@ -85,7 +85,6 @@ constexpr int kTL = 32;  // layers per tile (redistribution)
 // does not wait a memory latency per layer and holds no extra registers.
 // Ring layout [slot][element][thread] (element ES = du[IDN]), doubles.
 constexpr int kFinThreads = 256;                // threads of a finish CTA
-constexpr int kFinItems = kTC * kTL / kFinThreads;  // cells per finish thread
 constexpr int kFwdDepth = 4;  // layers of the forward sweep in flight
 
 template <int N>
@@ -552,14 +551,14 @@ __global__ void __launch_bounds__(128) k_vic_column_pre(Geo g, Phys p, StageBufs
 template <class K>
 static void allow_ring_smem(K kernel, size_t bytes) {
   static std::mutex mu;
-  static const void* done[32];
+  static const void* done[64];
   static int ndone = 0;
   std::lock_guard<std::mutex> lock(mu);
   const void* f = reinterpret_cast<const void*>(kernel);
   for (int k = 0; k < ndone; ++k)
     if (done[k] == f) return;
   cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  if (ndone < 32) done[ndone++] = f;
+  if (ndone < 64) done[ndone++] = f;
 }
 
 template <int N, class B>
@@ -571,94 +570,114 @@ __global__ void __launch_bounds__(128) k_vic_column(Geo g, Phys p, B b) {
 // layers: delta is transposed through shared memory so that the state
 // arrays are read and written along x1.
 // one tile: columns col0 .. col0+kTC-1, layers i0 .. i0+kTL-1 (whole CTA)
+// Shared memory of one finish tile: the back-substituted solution rows
+// [N][kTC][kTL+1] (doubles), the column sums and offsets, then the tile's cell
+// inputs [element][kTC][kTL] in the stored precision T: w'[IDN], the du rows
+// the solve does not replace, and (RK update) u, u0, and per scalar s, s0, r
+// and its du row.
+template <int N, int NS>
+struct FinSmem {
+  static constexpr int du_rows = N == 3 ? 3 : 1;           // IDN (+ IVY, IVZ)
+  static constexpr int elems = 1 + du_rows + 10 + 4 * NS;  // upper bound
+  static constexpr size_t head = ((size_t)N * kTC * (kTL + 1) + 3 * kTC) * sizeof(double);
+};
+template <int N, int NS, class T>
+constexpr size_t finish_smem_bytes() {
+  return FinSmem<N, NS>::head + (size_t)FinSmem<N, NS>::elems * kTC * kTL * sizeof(T);
+}
+
+// One tile: columns col0 .. col0+kTC-1, layers i0 .. i0+kTL-1 (whole CTA).
+// Every input of the tile is fetched with cp.async (coalesced: the solution
+// rows along columns, the cell values along x1) and waited for once, so all
+// of a tile's loads are in flight together without holding registers; the
+// threads then finish the tile's cells from shared memory.
 template <int N, int NS, class B>
 __device__ __forceinline__ void vic_finish_tile(const Geo& g, const Phys& p, const B& b,
                                                 int64_t col0, int i0) {
-  constexpr int ES = VicDims<N>::ES;
+  constexpr int ES = VicDims<N>::ES, DR = FinSmem<N, NS>::du_rows;
+  using T = std::remove_pointer_t<decltype(b.u)>;  // stored precision (FP32 / FP64)
   const int nl = g.nx1;
   const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
   const int64_t sv = g.sv;
   const double* S = b.vic;
   const double* Z = S + (int64_t)nl * ES * ncol;
-  __shared__ double dl[N][kTC][kTL + 1];
-  __shared__ double zs[2][kTC];
-  __shared__ int64_t cbs[kTC];  // (k, j, il) offsets of the tile's columns
+  extern __shared__ double fin_smem[];
+  double* dl = fin_smem;                                     // [N][kTC][kTL+1]
+  double* zs = dl + (size_t)N * kTC * (kTL + 1);             // [2][kTC]
+  int64_t* cbs = reinterpret_cast<int64_t*>(zs + 2 * kTC);   // [kTC]
+  T* cell = reinterpret_cast<T*>(cbs + kTC);                 // [element][kTC][kTL]
+  auto DL = [&](int r, int c, int s) -> double& {
+    return dl[((size_t)r * kTC + c) * (kTL + 1) + s];
+  };
+  auto CE = [&](int e, int c, int s) -> T* { return cell + ((size_t)e * kTC + c) * kTL + s; };
+  const bool du_only = b.vic_du_only, first = b.stage == 0;
+  // element slots; per scalar n: s, s0, r, its du row at eS + 4 n
+  const int eRHO = 0, eDU = 1, eU = 1 + DR, eU0 = eU + 5, eS = eU0 + 5;
   const int tid = threadIdx.x;
+  if (tid < 2 * kTC) {
+    int c = tid % kTC, k = tid / kTC;
+    zs[k * kTC + c] = col0 + c < ncol ? Z[k * ncol + col0 + c] : 1.;
+    if (k == 0) cbs[c] = col0 + c < ncol ? column_base(g, col0 + c) : 0;
+  }
+  __syncthreads();
   for (int idx = tid; idx < N * kTC * kTL; idx += blockDim.x) {
     int c = idx % kTC, rest = idx / kTC;
     int s = rest % kTL, r = rest / kTL;
     int64_t col = col0 + c;
     int i = i0 + s;
-    dl[r][c][s] = (col < ncol && i < nl) ? S[((int64_t)i * ES + N * N + r) * ncol + col] : 0.;
+    if (col < ncol && i < nl)
+      cp_async_bytes8(&DL(r, c, s), S + ((int64_t)i * ES + N * N + r) * ncol + col);
   }
-  if (tid < 2 * kTC) {
-    int c = tid % kTC, k = tid / kTC;
-    zs[k][c] = col0 + c < ncol ? Z[k * ncol + col0 + c] : 1.;
-    if (k == 0) cbs[c] = col0 + c < ncol ? column_base(g, col0 + c) : 0;
-  }
-  __syncthreads();
-  // (2) each thread's kFinItems cells: every load first (no store in
-  // between, so they are all in flight together), then the arithmetic and
-  // the stores.  Cells are distinct, so the order is the sequential one's.
-  constexpr int IT = kFinItems, NSA = NS > 0 ? NS : 1;
-  using T = std::remove_pointer_t<decltype(b.u)>;  // stored precision (FP32 / FP64)
-  T rho[IT], et[IT], dvy[IT], dvz[IT], uo[IT][5], u0o[IT][5];
-  T so[IT][NSA], s0o[IT][NSA], ro[IT][NSA], dso[IT][NSA];
-  int64_t offs[IT];
-  bool ok[IT];
-  const bool du_only = b.vic_du_only, first = b.stage == 0;
-#pragma unroll
-  for (int k = 0; k < IT; ++k) {
-    const int idx = tid + k * kFinThreads;
-    const int s = idx % kTL, c = idx / kTL;
-    const int64_t col = col0 + c;
+  const int ne = du_only ? eU : (first ? eU0 : eS);  // u0 is the stage input at stage 0
+  for (int idx = tid; idx < ne * kTC * kTL; idx += blockDim.x) {
+    const int s = idx % kTL, rest = idx / kTL;
+    const int c = rest % kTC, e = rest / kTC;
     const int i = i0 + s;
-    ok[k] = col < ncol && i < nl;
-    if (!ok[k]) continue;
+    if (col0 + c >= ncol || i >= nl) continue;
     const int64_t off = cbs[c] + i;
-    offs[k] = off;
-    rho[k] = b.w[IDN * sv + off];
-    et[k] = b.D[IDN * sv + off];
-    if constexpr (N == 3) {
-      dvy[k] = b.D[IVY * sv + off];
-      dvz[k] = b.D[IVZ * sv + off];
-    }
-    if (!du_only) {
-#pragma unroll
-      for (int v = 0; v < 5; ++v) {
-        uo[k][v] = b.u[v * sv + off];
-        if (!first) u0o[k][v] = b.u0[v * sv + off];
-      }
-#pragma unroll
-      for (int n = 0; n < NS; ++n) {
-        const int64_t o = n * sv + off;
-        so[k][n] = b.s[o];
-        if (!first) s0o[k][n] = b.s0[o];
-        ro[k][n] = b.r[o];
-        dso[k][n] = b.D[(5 + n) * sv + off];
-      }
+    const T* src;
+    if (e == eRHO) src = b.w + IDN * sv + off;
+    else if (e < eU) src = b.D + (e == eDU ? IDN : (e == eDU + 1 ? IVY : IVZ)) * sv + off;
+    else if (e < eU0) src = b.u + (e - eU) * sv + off;
+    else src = b.u0 + (e - eU0) * sv + off;
+    cp_async_elem(CE(e, c, s), src);
+  }
+  if (!du_only) {
+    for (int idx = tid; idx < 4 * NS * kTC * kTL; idx += blockDim.x) {
+      const int s = idx % kTL, rest = idx / kTL;
+      const int c = rest % kTC, q = rest / kTC;
+      const int n = q / 4, kind = q % 4;
+      const int i = i0 + s;
+      if (col0 + c >= ncol || i >= nl || (kind == 1 && first)) continue;
+      const int64_t o = n * sv + cbs[c] + i;
+      const T* src = kind == 0 ? b.s + o
+                               : (kind == 1 ? b.s0 + o : (kind == 2 ? b.r + o : b.D + 5 * sv + o));
+      cp_async_elem(CE(eS + q, c, s), src);
     }
   }
-#pragma unroll
-  for (int k = 0; k < IT; ++k) {
-    if (!ok[k]) continue;
-    const int idx = tid + k * kFinThreads;
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+  for (int idx = tid; idx < kTC * kTL; idx += blockDim.x) {
     const int s = idx % kTL, c = idx / kTL;
-    const int64_t off = offs[k];
-    const int xi = g.il + i0 + s;
-    const double rhok = vic_full(b, (double)rho[k], IDN, xi), etk = et[k];
+    const int i = i0 + s;
+    if (col0 + c >= ncol || i >= nl) continue;
+    const int64_t off = cbs[c] + i;
+    const int xi = g.il + i;
+    const double rhok = vic_full(b, (double)*CE(eRHO, c, s), IDN, xi);
+    const double etk = *CE(eDU, c, s);
     double ai = rhok * g.vol;
-    double fix = dl[0][c][s] - etk;
+    double fix = DL(0, c, s) - etk;
     double du[5];
-    du[IDN] = etk + fix * 1. + rhok * ai * zs[1][c] / zs[0][c];
+    du[IDN] = etk + fix * 1. + rhok * ai * zs[kTC + c] / zs[c];
     if constexpr (N == 3) {
-      du[IVX] = dl[1][c][s];
-      du[IVY] = dvy[k];
-      du[IVZ] = dvz[k];
-      du[IPR] = dl[2][c][s];
+      du[IVX] = DL(1, c, s);
+      du[IVY] = *CE(eDU + 1, c, s);
+      du[IVZ] = *CE(eDU + 2, c, s);
+      du[IPR] = DL(2, c, s);
     } else {
 #pragma unroll
-      for (int v = 1; v < 5; ++v) du[v] = dl[v][c][s];
+      for (int v = 1; v < 5; ++v) du[v] = DL(v, c, s);
     }
     if (b.M) b.M[IDN * sv + off] = fix;
     if (du_only) {
@@ -669,16 +688,19 @@ __device__ __forceinline__ void vic_finish_tile(const Geo& g, const Phys& p, con
     double unew_rho = 0.;
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
-      double un = vic_rk_from(b.u, b.u0, v * sv + off, first, uo[k][v], u0o[k][v], b.wgt0,
-                              b.wgt1, b.wgt2, du[v]);
+      const double uo = *CE(eU + v, c, s), u0o = first ? 0. : (double)*CE(eU0 + v, c, s);
+      double un = vic_rk_from(b.u, b.u0, v * sv + off, first, uo, u0o, b.wgt0, b.wgt1, b.wgt2,
+                              du[v]);
       if (v == IDN) unew_rho = vic_full_rho(b, un, xi);
     }
 #pragma unroll
     for (int n = 0; n < NS; ++n) {
       const int64_t o = n * sv + off;
-      double ds = (double)dso[k][n] + fix * (double)ro[k][n];
-      double sn = vic_rk_from(b.s, b.s0, o, first, so[k][n], s0o[k][n], b.wgt0, b.wgt1,
-                              b.wgt2, ds);
+      const double so = *CE(eS + 4 * n, c, s);
+      const double s0o = first ? 0. : (double)*CE(eS + 4 * n + 1, c, s);
+      const double ro = *CE(eS + 4 * n + 2, c, s), dso = *CE(eS + 4 * n + 3, c, s);
+      double ds = dso + fix * ro;
+      double sn = vic_rk_from(b.s, b.s0, o, first, so, s0o, b.wgt0, b.wgt1, b.wgt2, ds);
       b.r[o] = sn / unew_rho;
     }
   }
@@ -712,13 +734,21 @@ static cudaError_t launch_vic_n(const Geo& g, const Phys& p, const B& b, cudaStr
         g, p, b);
   }
   dim3 gf((unsigned)((ncol + kTC - 1) / kTC), (unsigned)((nl + kTL - 1) / kTL));
+  using T = std::remove_pointer_t<decltype(b.u)>;
+#define SNAPB_VF(NS)                                              \
+  case NS: {                                                      \
+    constexpr size_t sm = finish_smem_bytes<N, NS, T>();          \
+    allow_ring_smem(k_vic_finish<N, NS, B>, sm);                  \
+    k_vic_finish<N, NS, B><<<gf, kFinThreads, sm, st>>>(g, p, b); \
+  } break;
   switch (p.nscalar) {
-    case 0: k_vic_finish<N, 0, B><<<gf, kFinThreads, 0, st>>>(g, p, b); break;
-    case 1: k_vic_finish<N, 1, B><<<gf, kFinThreads, 0, st>>>(g, p, b); break;
-    case 2: k_vic_finish<N, 2, B><<<gf, kFinThreads, 0, st>>>(g, p, b); break;
-    case 3: k_vic_finish<N, 3, B><<<gf, kFinThreads, 0, st>>>(g, p, b); break;
+    SNAPB_VF(0)
+    SNAPB_VF(1)
+    SNAPB_VF(2)
+    SNAPB_VF(3)
     default: return cudaErrorInvalidValue;
   }
+#undef SNAPB_VF
   return cudaGetLastError();
 }
 
@@ -763,7 +793,7 @@ __global__ void __launch_bounds__(128, V == 0 ? 1 : (V == 1 ? 3 : 4))
 }
 
 template <int N, int NS>
-__global__ void __launch_bounds__(kFinThreads, 2) k_vic_finish_batch(const Member32* __restrict__ mem,
+__global__ void __launch_bounds__(kFinThreads, 4) k_vic_finish_batch(const Member32* __restrict__ mem,
                                                           Phys p, WorkQueue q, int stage) {
   __shared__ Member32 s_mem;  // the member's descriptor, read as needed (see the column kernel)
   int m;
@@ -806,10 +836,14 @@ cudaError_t launch_vic_column_batch(const Member32* mem, const Phys& p, const Wo
 cudaError_t launch_vic_finish_batch(const Member32* mem, const Phys& p, const WorkQueue& q,
                                     int stage, const PersistGrid& pg, cudaStream_t st) {
   static_assert(kTC == kVicFinishCols && kTL == kVicFinishLayers, "finish tile shape");
-#define SNAPB_VFB(N, NS)                                                                 \
-  k_vic_finish_batch<N, NS><<<persistent_grid(k_vic_finish_batch<N, NS>, kFinThreads, 0, pg), \
-                              kFinThreads, 0, \
-                              st>>>(mem, p, q, stage)
+#define SNAPB_VFB(N, NS)                                                                  \
+  {                                                                                       \
+    constexpr size_t sm = finish_smem_bytes<N, NS, float>();                              \
+    allow_ring_smem(k_vic_finish_batch<N, NS>, sm);                                       \
+    k_vic_finish_batch<N, NS><<<persistent_grid(k_vic_finish_batch<N, NS>, kFinThreads, sm, \
+                                                pg),                                      \
+                                kFinThreads, sm, st>>>(mem, p, q, stage);                 \
+  }
   if (vic_n(p) == 5) {
     switch (p.nscalar) {
       case 0: SNAPB_VFB(5, 0); break;
