@@ -158,7 +158,6 @@ size_t x1_smem32_per_column(const Geo& g, int nvt);
 StageBufs32 bufs32_of(const snapb_hydro_config& c, void* ws);
 size_t workspace_size_f32_of(const snapb_hydro_config& c);
 constexpr int kVicFinishCols = 32;    // columns per implicit-finish tile
-constexpr int kVicFinishLayers = 16;  // layers per implicit-finish tile
 
 // RK3 (Shu-Osher) stage weights: u = wgt0*u0 + wgt1*u + wgt2*du
 inline void rk3_weights(int stage, double& a, double& b, double& c) {
@@ -181,6 +180,7 @@ cudaError_t launch_vic(const Geo& g, const Phys& p, const StageBufs& b, cudaStre
 cudaError_t launch_vic32(const Geo& g, const Phys& p, const StageBufs32& b, cudaStream_t st);
 size_t vic_scratch_bytes(const Geo& g, const Phys& p);
 size_t vic_blocks_bytes(const Geo& g, const Phys& p);
+int vic_finish_layers32(int nscalar);  // layers per implicit-finish tile, FP32 form
 
 cudaError_t launch_cons2prim(const Geo& g, const Phys& p, const double* u, double* w,
                              cudaStream_t st);

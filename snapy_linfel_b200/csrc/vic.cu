@@ -26,6 +26,7 @@
 #include <cstring>
 #include <mutex>
 #include <type_traits>
+#include <utility>
 #include <string>
 
 #include "kernels.cuh"
@@ -77,14 +78,12 @@ size_t vic_blocks_bytes(const Geo& g, const Phys& p) {
 }
 
 constexpr int kTC = 32;  // columns per tile
-constexpr int kTL = 16;  // layers per tile (redistribution)
 
 // Back substitution: the reduced block, partial solution and du[IDN] of a
 // layer are fetched kBackDepth<N> layers ahead into a per-thread ring in
 // shared memory by asynchronous copies (cp.async), so the short recurrence
 // does not wait a memory latency per layer and holds no extra registers.
 // Ring layout [slot][element][thread] (element ES = du[IDN]), doubles.
-constexpr int kFinThreads = 256;                // threads of a finish CTA
 constexpr int kFwdDepth = 4;  // layers of the forward sweep in flight
 
 template <int N>
@@ -381,8 +380,49 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
     jac_of<N>(b, gm1c, wn, Jn);
     double ai = wc[IDN] * V;
     sum_a2 += ai * ai;
-    double c[N][N];
-    vic_layer<N>(Am, Ap, Jp, Jn, ap, dp, rhs, c, i, nl, Aa, hiv, idt, grav);
+    double a[N][N], bb[N][N], c[N][N];
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        double phi = 0.;
+        if (r == 1 && q == 0) phi = grav;
+        if (N == 3 && r == 2 && q == 1) phi = grav;
+        if (N == 5 && r == IPR && q == IVX) phi = grav;
+        a[r][q] = (Am[r][q] * Aa + Ap[r][q] * Aa) * hiv - phi;
+        bb[r][q] = -(Am[r][q] + Jp[r][q]) * Aa * hiv;
+        c[r][q] = -(Ap[r][q] - Jn[r][q]) * Aa * hiv;
+      }
+#pragma unroll
+    for (int r = 0; r < N; ++r) a[r][r] += idt;
+    if (i == 0) {
+#pragma unroll
+      for (int r = 0; r < N; ++r)
+#pragma unroll
+        for (int q = 0; q < N; ++q) a[r][q] += bb[r][q] * (q == 1 ? -1. : 1.);
+    }
+    if (i == nl - 1) {
+#pragma unroll
+      for (int r = 0; r < N; ++r)
+#pragma unroll
+        for (int q = 0; q < N; ++q) a[r][q] += c[r][q] * (q == 1 ? -1. : 1.);
+    }
+    if (i > 0) {
+#pragma unroll
+      for (int r = 0; r < N; ++r) {
+        double bd = 0.;
+#pragma unroll
+        for (int q = 0; q < N; ++q) {
+          double t = 0.;
+#pragma unroll
+          for (int kk = 0; kk < N; ++kk) t += bb[r][kk] * ap[kk][q];
+          a[r][q] -= t;
+          bd += bb[r][q] * dp[q];
+        }
+        rhs[r] = rhs[r] - bd;
+      }
+    }
+    block_solve<N>(a, c, rhs);
     // the slot's values are consumed (the solve depends on them): refill it
     ffetch(i + 1 + DF, fslot);
     fslot = fslot + 1 == DF ? 0 : fslot + 1;
@@ -407,7 +447,51 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
 #pragma unroll
     for (int v = 0; v < 5; ++v) wc[v] = wn[v];
   }
-  vic_back<N>(b, S, Z, ncol, sv, cb, nl, dp, sum_a2, V);
+  // back substitution: delta_i -= a'_i delta_{i+1}; B_dry accumulated on the
+  // way, the inputs of each layer arriving through the shared-memory ring.
+  constexpr int DB = BackRing<N>::depth, RE = BackRing<N>::elems;
+  cp_async_wait<0>();  // the forward ring is drained before its memory is reused
+  auto ring = [&](int slot, int e) { return vic_ring + ((size_t)(slot * RE + e) * nt + lane); };
+  auto fetch = [&](int i, int slot) {
+    if (i >= 0) {
+#pragma unroll
+      for (int e = 0; e < ES; ++e) cp_async_bytes8(ring(slot, e), &Sat(i, e));
+      cp_async_elem(ring(slot, ES), b.D + IDN * sv + cb + i);
+    }
+    cp_async_commit();
+  };
+  double dn[N];
+#pragma unroll
+  for (int r = 0; r < N; ++r) dn[r] = dp[r];
+  double b_dry = (vic_d(b, IDN * sv + cb + nl - 1) - dn[0]) * 1. * V;
+#pragma unroll
+  for (int k = 0; k < DB; ++k) fetch(nl - 2 - k, k);
+  for (int i = nl - 2, slot = 0; i >= 0; --i) {
+    cp_async_wait<DB - 1>();  // the group of layer i has landed
+    double cur[ES];
+#pragma unroll
+    for (int e = 0; e < ES; ++e) cur[e] = *ring(slot, e);
+    const double dcur = ring_elem(ring(slot, ES), b.D);
+    double d[N];
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      double t = 0.;
+#pragma unroll
+      for (int q = 0; q < N; ++q) t += cur[r * N + q] * dn[q];
+      d[r] = cur[N * N + r] - t;
+    }
+    b_dry += (dcur - d[0]) * 1. * V;
+    fetch(i - DB, slot);  // the slot's values are consumed: refill it
+    slot = slot + 1 == DB ? 0 : slot + 1;
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      dn[r] = d[r];
+      Sat(i, N * N + r) = d[r];
+    }
+  }
+  cp_async_wait<0>();
+  Z[0] = sum_a2;
+  Z[ncol] = b_dry;
 }
 
 // ---- split sweep (few columns): blocks first, then the elimination ----
@@ -577,13 +661,14 @@ __global__ void __launch_bounds__(128) k_vic_column(Geo g, Phys p, B b) {
 // and its du row.
 template <int N, int NS>
 struct FinSmem {
+  static constexpr int TL = 16;  // layers per staged tile
   static constexpr int du_rows = N == 3 ? 3 : 1;           // IDN (+ IVY, IVZ)
   static constexpr int elems = 1 + du_rows + 10 + 4 * NS;  // upper bound
-  static constexpr size_t head = ((size_t)N * kTC * (kTL + 1) + 3 * kTC) * sizeof(double);
+  static constexpr size_t head = ((size_t)N * kTC * (TL + 1) + 3 * kTC) * sizeof(double);
 };
 template <int N, int NS, class T>
 constexpr size_t finish_smem_bytes() {
-  return FinSmem<N, NS>::head + (size_t)FinSmem<N, NS>::elems * kTC * kTL * sizeof(T);
+  return FinSmem<N, NS>::head + (size_t)FinSmem<N, NS>::elems * kTC * FinSmem<N, NS>::TL * sizeof(T);
 }
 
 // One tile: columns col0 .. col0+kTC-1, layers i0 .. i0+kTL-1 (whole CTA).
@@ -592,9 +677,9 @@ constexpr size_t finish_smem_bytes() {
 // of a tile's loads are in flight together without holding registers; the
 // threads then finish the tile's cells from shared memory.
 template <int N, int NS, class B>
-__device__ __forceinline__ void vic_finish_tile(const Geo& g, const Phys& p, const B& b,
+__device__ __forceinline__ void vic_finish_tile_staged(const Geo& g, const Phys& p, const B& b,
                                                 int64_t col0, int i0) {
-  constexpr int ES = VicDims<N>::ES, DR = FinSmem<N, NS>::du_rows;
+  constexpr int ES = VicDims<N>::ES, DR = FinSmem<N, NS>::du_rows, kTL = FinSmem<N, NS>::TL;
   using T = std::remove_pointer_t<decltype(b.u)>;  // stored precision (FP32 / FP64)
   const int nl = g.nx1;
   const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
@@ -706,9 +791,158 @@ __device__ __forceinline__ void vic_finish_tile(const Geo& g, const Phys& p, con
   }
 }
 
+// Register variant (scalars, or FP64 state: the staged inputs would not fit
+// in 48 KB of shared memory and would cut the resident CTAs): each thread
+// issues the loads of its cells before any store.
+template <int N, int NS, class B, int NT, int kTL>
+__device__ __forceinline__ void vic_finish_tile_regs(const Geo& g, const Phys& p, const B& b,
+                                                int64_t col0, int i0) {
+  constexpr int ES = VicDims<N>::ES;
+  const int nl = g.nx1;
+  const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
+  const int64_t sv = g.sv;
+  const double* S = b.vic;
+  const double* Z = S + (int64_t)nl * ES * ncol;
+  __shared__ double dl[N][kTC][kTL + 1];
+  __shared__ double zs[2][kTC];
+  __shared__ int64_t cbs[kTC];  // (k, j, il) offsets of the tile's columns
+  const int tid = threadIdx.x;
+  for (int idx = tid; idx < N * kTC * kTL; idx += blockDim.x) {
+    int c = idx % kTC, rest = idx / kTC;
+    int s = rest % kTL, r = rest / kTL;
+    int64_t col = col0 + c;
+    int i = i0 + s;
+    dl[r][c][s] = (col < ncol && i < nl) ? S[((int64_t)i * ES + N * N + r) * ncol + col] : 0.;
+  }
+  if (tid < 2 * kTC) {
+    int c = tid % kTC, k = tid / kTC;
+    zs[k][c] = col0 + c < ncol ? Z[k * ncol + col0 + c] : 1.;
+    if (k == 0) cbs[c] = col0 + c < ncol ? column_base(g, col0 + c) : 0;
+  }
+  __syncthreads();
+  // (2) each thread's kTC kTL / NT cells: every load first (no store in
+  // between, so they are all in flight together), then the arithmetic and
+  // the stores.  Cells are distinct, so the order is the sequential one's.
+  constexpr int IT = kTC * kTL / NT, NSA = NS > 0 ? NS : 1;
+  using T = std::remove_pointer_t<decltype(b.u)>;  // stored precision (FP32 / FP64)
+  T rho[IT], et[IT], dvy[IT], dvz[IT], uo[IT][5], u0o[IT][5];
+  T so[IT][NSA], s0o[IT][NSA], ro[IT][NSA], dso[IT][NSA];
+  int64_t offs[IT];
+  bool ok[IT];
+  const bool du_only = b.vic_du_only, first = b.stage == 0;
+#pragma unroll
+  for (int k = 0; k < IT; ++k) {
+    const int idx = tid + k * NT;
+    const int s = idx % kTL, c = idx / kTL;
+    const int64_t col = col0 + c;
+    const int i = i0 + s;
+    ok[k] = col < ncol && i < nl;
+    if (!ok[k]) continue;
+    const int64_t off = cbs[c] + i;
+    offs[k] = off;
+    rho[k] = b.w[IDN * sv + off];
+    et[k] = b.D[IDN * sv + off];
+    if constexpr (N == 3) {
+      dvy[k] = b.D[IVY * sv + off];
+      dvz[k] = b.D[IVZ * sv + off];
+    }
+    if (!du_only) {
+#pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        uo[k][v] = b.u[v * sv + off];
+        if (!first) u0o[k][v] = b.u0[v * sv + off];
+      }
+#pragma unroll
+      for (int n = 0; n < NS; ++n) {
+        const int64_t o = n * sv + off;
+        so[k][n] = b.s[o];
+        if (!first) s0o[k][n] = b.s0[o];
+        ro[k][n] = b.r[o];
+        dso[k][n] = b.D[(5 + n) * sv + off];
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < IT; ++k) {
+    if (!ok[k]) continue;
+    const int idx = tid + k * NT;
+    const int s = idx % kTL, c = idx / kTL;
+    const int64_t off = offs[k];
+    const int xi = g.il + i0 + s;
+    const double rhok = vic_full(b, (double)rho[k], IDN, xi), etk = et[k];
+    double ai = rhok * g.vol;
+    double fix = dl[0][c][s] - etk;
+    double du[5];
+    du[IDN] = etk + fix * 1. + rhok * ai * zs[1][c] / zs[0][c];
+    if constexpr (N == 3) {
+      du[IVX] = dl[1][c][s];
+      du[IVY] = dvy[k];
+      du[IVZ] = dvz[k];
+      du[IPR] = dl[2][c][s];
+    } else {
+#pragma unroll
+      for (int v = 1; v < 5; ++v) du[v] = dl[v][c][s];
+    }
+    if (b.M) b.M[IDN * sv + off] = fix;
+    if (du_only) {
+#pragma unroll
+      for (int v = 0; v < 5; ++v) vic_set_d(b, v * sv + off, du[v]);
+      continue;
+    }
+    double unew_rho = 0.;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      double un = vic_rk_from(b.u, b.u0, v * sv + off, first, uo[k][v], u0o[k][v], b.wgt0,
+                              b.wgt1, b.wgt2, du[v]);
+      if (v == IDN) unew_rho = vic_full_rho(b, un, xi);
+    }
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+      const int64_t o = n * sv + off;
+      double ds = (double)dso[k][n] + fix * (double)ro[k][n];
+      double sn = vic_rk_from(b.s, b.s0, o, first, so[k][n], s0o[k][n], b.wgt0, b.wgt1,
+                              b.wgt2, ds);
+      b.r[o] = sn / unew_rho;
+    }
+  }
+}
+
+// Which finish variant a form takes, and its launch shape.
+template <int N, int NS, class T>
+struct FinCfg {
+  static constexpr bool staged = finish_smem_bytes<N, NS, T>() <= 48 * 1024;
+  static constexpr int threads = 256;
+  static constexpr int layers = staged ? FinSmem<N, NS>::TL : 32;  // tile height
+  static constexpr int min_ctas = staged ? 4 : 2;  // register budget of the batched kernel
+  // one-block kernel: two resident CTAs for FP32 state (its register
+  // variant sits just above 128 registers uncapped, which would leave one);
+  // FP64 state keeps the compiler's budget (capping it spills)
+  static constexpr int min_ctas_single = staged ? 4 : (sizeof(T) == 4 ? 2 : 1);
+  static constexpr size_t smem = staged ? finish_smem_bytes<N, NS, T>() : 0;
+};
+// the FP32 form stages exactly when it carries no scalars (the batched plan
+// sizes its tiles with vic_finish_layers32)
+static_assert(FinCfg<3, 0, float>::staged && FinCfg<5, 0, float>::staged &&
+                  !FinCfg<3, 1, float>::staged && !FinCfg<5, 1, float>::staged,
+              "finish variant of the FP32 form");
+template <class B>
+using StoredT = std::remove_pointer_t<decltype(std::declval<B>().u)>;
+
 template <int N, int NS, class B>
-__global__ void __launch_bounds__(kFinThreads) k_vic_finish(Geo g, Phys p, B b) {
-  vic_finish_tile<N, NS, B>(g, p, b, (int64_t)blockIdx.x * kTC, (int)blockIdx.y * kTL);
+__device__ __forceinline__ void vic_finish_tile(const Geo& g, const Phys& p, const B& b,
+                                                int64_t col0, int i0) {
+  using C = FinCfg<N, NS, StoredT<B>>;
+  if constexpr (C::staged)
+    vic_finish_tile_staged<N, NS, B>(g, p, b, col0, i0);
+  else
+    vic_finish_tile_regs<N, NS, B, C::threads, C::layers>(g, p, b, col0, i0);
+}
+
+template <int N, int NS, class B>
+__global__ void __launch_bounds__(FinCfg<N, NS, StoredT<B>>::threads,
+                                  FinCfg<N, NS, StoredT<B>>::min_ctas_single) k_vic_finish(Geo g, Phys p, B b) {
+  vic_finish_tile<N, NS, B>(g, p, b, (int64_t)blockIdx.x * kTC,
+                            (int)blockIdx.y * FinCfg<N, NS, StoredT<B>>::layers);
 }
 
 template <int N, class B>
@@ -733,13 +967,14 @@ static cudaError_t launch_vic_n(const Geo& g, const Phys& p, const B& b, cudaStr
     k_vic_column<N, B><<<(unsigned)((ncol + bs - 1) / bs), bs, back_ring_bytes<N>(bs), st>>>(
         g, p, b);
   }
-  dim3 gf((unsigned)((ncol + kTC - 1) / kTC), (unsigned)((nl + kTL - 1) / kTL));
   using T = std::remove_pointer_t<decltype(b.u)>;
-#define SNAPB_VF(NS)                                              \
-  case NS: {                                                      \
-    constexpr size_t sm = finish_smem_bytes<N, NS, T>();          \
-    allow_ring_smem(k_vic_finish<N, NS, B>, sm);                  \
-    k_vic_finish<N, NS, B><<<gf, kFinThreads, sm, st>>>(g, p, b); \
+#define SNAPB_VF(NS)                                                   \
+  case NS: {                                                           \
+    using FC = FinCfg<N, NS, T>;                                       \
+    dim3 gf((unsigned)((ncol + kTC - 1) / kTC),                        \
+            (unsigned)((nl + FC::layers - 1) / FC::layers));           \
+    if (FC::smem) allow_ring_smem(k_vic_finish<N, NS, B>, FC::smem);   \
+    k_vic_finish<N, NS, B><<<gf, FC::threads, FC::smem, st>>>(g, p, b); \
   } break;
   switch (p.nscalar) {
     SNAPB_VF(0)
@@ -793,7 +1028,8 @@ __global__ void __launch_bounds__(128, V == 0 ? 1 : (V == 1 ? 3 : 4))
 }
 
 template <int N, int NS>
-__global__ void __launch_bounds__(kFinThreads, 4) k_vic_finish_batch(const Member32* __restrict__ mem,
+__global__ void __launch_bounds__(FinCfg<N, NS, float>::threads,
+                                  FinCfg<N, NS, float>::min_ctas) k_vic_finish_batch(const Member32* __restrict__ mem,
                                                           Phys p, WorkQueue q, int stage) {
   __shared__ Member32 s_mem;  // the member's descriptor, read as needed (see the column kernel)
   int m;
@@ -802,10 +1038,11 @@ __global__ void __launch_bounds__(kFinThreads, 4) k_vic_finish_batch(const Membe
     load_member(s_mem, mem, m);
     if (threadIdx.x == 0) set_stage_vic32(s_mem.b, stage);
     __syncthreads();
-    const int nlb = (s_mem.g.nx1 + kTL - 1) / kTL;
+    constexpr int TLY = FinCfg<N, NS, float>::layers;
+    const int nlb = (s_mem.g.nx1 + TLY - 1) / TLY;
     const int64_t cb = tile / nlb;
     const int lb = (int)(tile - cb * nlb);
-    vic_finish_tile<N, NS, StageBufs32>(s_mem.g, p, s_mem.b, cb * kTC, lb * kTL);
+    vic_finish_tile<N, NS, StageBufs32>(s_mem.g, p, s_mem.b, cb * kTC, lb * TLY);
   }
 }
 
@@ -833,16 +1070,20 @@ cudaError_t launch_vic_column_batch(const Member32* mem, const Phys& p, const Wo
   return cudaGetLastError();
 }
 
+int vic_finish_layers32(int nscalar) {
+  return nscalar == 0 ? FinCfg<3, 0, float>::layers : FinCfg<3, 1, float>::layers;
+}
+
 cudaError_t launch_vic_finish_batch(const Member32* mem, const Phys& p, const WorkQueue& q,
                                     int stage, const PersistGrid& pg, cudaStream_t st) {
-  static_assert(kTC == kVicFinishCols && kTL == kVicFinishLayers, "finish tile shape");
+  static_assert(kTC == kVicFinishCols, "finish tile shape");
 #define SNAPB_VFB(N, NS)                                                                  \
   {                                                                                       \
-    constexpr size_t sm = finish_smem_bytes<N, NS, float>();                              \
-    allow_ring_smem(k_vic_finish_batch<N, NS>, sm);                                       \
-    k_vic_finish_batch<N, NS><<<persistent_grid(k_vic_finish_batch<N, NS>, kFinThreads, sm, \
-                                                pg),                                      \
-                                kFinThreads, sm, st>>>(mem, p, q, stage);                 \
+    using FC = FinCfg<N, NS, float>;                                                      \
+    if (FC::smem) allow_ring_smem(k_vic_finish_batch<N, NS>, FC::smem);                   \
+    k_vic_finish_batch<N, NS><<<persistent_grid(k_vic_finish_batch<N, NS>, FC::threads,   \
+                                                FC::smem, pg),                            \
+                                FC::threads, FC::smem, st>>>(mem, p, q, stage);           \
   }
   if (vic_n(p) == 5) {
     switch (p.nscalar) {
