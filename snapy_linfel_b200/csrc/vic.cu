@@ -209,7 +209,8 @@ __device__ __forceinline__ void jac_of(const StageBufs32&, double gm1, const dou
 // at the layer's lower / upper faces (Am, Ap) and J of the cells below /
 // above (Jp, Jn); the previous reduced block and partial solution (ap, dp)
 // are eliminated, and c (reduced block) and rhs (partial solution) return the
-// new ones.  The same arithmetic for the fused and the split sweeps.
+// new ones.  Used by the split sweep; the fused sweep (vic_column) spells out
+// the same arithmetic inline.
 template <int N, class BT>
 __device__ __forceinline__ void vic_layer(const BT (&Am)[N][N], const BT (&Ap)[N][N],
                                           const BT (&Jp)[N][N], const BT (&Jn)[N][N],
