@@ -1,9 +1,9 @@
 """Multi-GPU plumbing of the replica runs: one process per GPU, no exchange on
 the data path.
 
-The single-domain step would shard by domain decomposition with a halo
-exchange per stage (reference src/layout/layout.cpp:361-634), which is not
-built; an ensemble shards trivially by whole members.  These helpers give the
+The single-domain step shards by slab decomposition with a ghost exchange per
+stage (layout.py); an ensemble shards trivially by whole members.  These
+helpers give the
 rank geometry, the max-over-ranks device timing every multi-rank number uses,
 and a size-balanced assignment of ensemble members to ranks.
 """

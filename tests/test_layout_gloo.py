@@ -1,0 +1,171 @@
+"""Slab decomposition host logic on CPU: the Morton rank order and neighbours
+of the reference's SlabLayout, the local block configurations, and the ghost
+exchange itself between gloo ranks (127.0.0.1) and between blocks held by one
+process, checked against the undivided array with its periodic wraps."""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+from snapy_linfel_b200.config import BC, make_config
+from snapy_linfel_b200.layout import SlabLayout, zorder_coords
+
+torch = pytest.importorskip("torch")
+mp = pytest.importorskip("torch.multiprocessing")
+
+
+def test_zorder_order():
+    # codes 0..7 decode to (x, y) = (0,0) (1,0) (0,1) (1,1) (2,0) (3,0) (2,1) (3,1)
+    assert zorder_coords(2, 2) == [(0, 0), (1, 0), (0, 1), (1, 1)]
+    assert zorder_coords(4, 2) == [(0, 0), (1, 0), (0, 1), (1, 1), (2, 0), (3, 0), (2, 1), (3, 1)]
+    # codes outside a 3 x 2 grid are skipped
+    assert zorder_coords(3, 2) == [(0, 0), (1, 0), (0, 1), (1, 1), (2, 0), (2, 1)]
+    assert zorder_coords(1, 3) == [(0, 0), (0, 1), (0, 2)]
+
+
+def test_neighbours():
+    lay = SlabLayout(4, 2, periodic_x=True, periodic_y=False)
+    r = lay.rank_at[(0, 0)]
+    assert lay.neighbor_rank(r, -1, 0) == lay.rank_at[(3, 0)]  # wraps in x2
+    assert lay.neighbor_rank(r, 1, 0) == lay.rank_at[(1, 0)]
+    assert lay.neighbor_rank(r, 0, -1) == -1                   # x3 edge
+    assert lay.neighbor_rank(r, 0, 1) == lay.rank_at[(0, 1)]
+    assert lay.loc_of(8) == (-1, -1)
+
+
+def test_local_config():
+    cfg = make_config(nx1=8, nx2=12, nx3=8, x2=(0.0, 1200.0), x3=(0.0, 800.0),
+                      bc=("reflecting", "reflecting", "reflecting", "outflow", "periodic",
+                          "periodic"))
+    lay = SlabLayout(3, 2, periodic_x=False, periodic_y=True)
+    seen = np.zeros((cfg.nx3, cfg.nx2), dtype=int)
+    for r in range(lay.world_size):
+        x, y = lay.loc_of(r)
+        c = lay.local_config(cfg, r)
+        assert (c.nx1, c.nx2, c.nx3) == (8, 4, 4)
+        assert c.x2min == pytest.approx(400.0 * x) and c.x2max == pytest.approx(400.0 * (x + 1))
+        assert c.x3min == pytest.approx(400.0 * y) and c.x3max == pytest.approx(400.0 * (y + 1))
+        assert c.bc[0] == BC["reflecting"] and c.bc[1] == BC["reflecting"]
+        assert c.bc[2] == (BC["reflecting"] if x == 0 else BC["custom"])
+        assert c.bc[3] == (BC["outflow"] if x == 2 else BC["custom"])
+        assert c.bc[4] == c.bc[5] == BC["custom"]  # periodic decomposed axis
+        j, k = lay.local_slices(cfg, r)
+        seen[k.start - 3:k.stop - 3, j.start - 3:j.stop - 3] += 1
+    assert (seen == 1).all()
+    with pytest.raises(ValueError):
+        SlabLayout(5, 1).local_config(cfg, 0)  # 12 cells do not split into 5
+
+
+def _global_with_wraps(cfg, lay, seed):
+    """a seeded global array [nv, nc3, nc2, nc1], and the same array with the
+    decomposed periodic axes wrapped (x2 first, then x3)"""
+    rng = np.random.default_rng(seed)
+    g = rng.standard_normal((2,) + cfg.shape[1:])
+    gx = g.copy()
+    ng = cfg.nghost
+    if lay.periodic[0] and lay.px > 1:
+        n = cfg.nx2
+        gx[:, :, :ng, :] = gx[:, :, n:n + ng, :]
+        gx[:, :, n + ng:, :] = gx[:, :, ng:2 * ng, :]
+    if lay.periodic[1] and lay.py > 1:
+        n = cfg.nx3
+        gx[:, :ng] = gx[:, n:n + ng]
+        gx[:, n + ng:] = gx[:, ng:2 * ng]
+    return g, gx
+
+
+def _local(arr, cfg, lay, r):
+    j, k = lay.local_slices(cfg, r)
+    ng = cfg.nghost
+    jj = slice(j.start - ng, j.stop + ng) if cfg.nx2 > 1 else j
+    kk = slice(k.start - ng, k.stop + ng) if cfg.nx3 > 1 else k
+    return np.ascontiguousarray(arr[:, kk, jj, :])
+
+
+def _poison(t, cfg, lay, r):
+    """NaN into the ghost cells the exchange must write"""
+    c = lay.local_config(cfg, r)
+    ng = cfg.nghost
+    for face, dim in ((2, 2), (3, 2), (4, 1), (5, 1)):
+        if c.bc[face] != BC["custom"]:
+            continue
+        idx = [slice(None)] * 4
+        n = t.shape[dim]
+        idx[dim] = slice(0, ng) if face % 2 == 0 else slice(n - ng, n)
+        t[tuple(idx)] = float("nan")
+
+
+CASES = [
+    (dict(nx1=6, nx2=12, nx3=1), (2, 1, True, False)),
+    (dict(nx1=6, nx2=12, nx3=1), (3, 1, False, False)),
+    (dict(nx1=5, nx2=8, nx3=12), (2, 2, True, False)),
+    (dict(nx1=5, nx2=8, nx3=12), (2, 2, False, True)),
+]
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, world, port, case, out):
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        kw, (px, py, perx, pery) = CASES[case]
+        cfg = make_config(**kw)
+        lay = SlabLayout(px, py, perx, pery)
+        g, gx = _global_with_wraps(cfg, lay, 7)
+        lc = lay.local_config(cfg, rank)
+        t = torch.from_numpy(_local(g, cfg, lay, rank))
+        s = torch.from_numpy(_local(g, cfg, lay, rank) * 2.0)
+        _poison(t, cfg, lay, rank)
+        _poison(s, cfg, lay, rank)
+        lay.exchange(lc, rank, [t, s])
+        want = _local(gx, cfg, lay, rank)
+        ok = bool(np.array_equal(t.numpy(), want)) and bool(np.array_equal(s.numpy(), 2.0 * want))
+        dt = torch.tensor([1.0 + rank])
+        lay.min_dt(dt)
+        out.put((rank, ok, float(dt)))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
+def test_exchange_between_gloo_ranks(case):
+    _, (px, py, _, _) = CASES[case]
+    world = px * py
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, case, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for r, ok, dt in res:
+        assert ok, f"rank {r}: ghost cells differ from the undivided array"
+        assert dt == 1.0  # MIN over ranks
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
+def test_exchange_in_one_process(case):
+    kw, (px, py, perx, pery) = CASES[case]
+    cfg = make_config(**kw)
+    lay = SlabLayout(px, py, perx, pery)
+    g, gx = _global_with_wraps(cfg, lay, 11)
+    lc = lay.local_config(cfg, 0)
+    fields = []
+    for r in range(lay.world_size):
+        t = torch.from_numpy(_local(g, cfg, lay, r))
+        _poison(t, cfg, lay, r)
+        fields.append([t])
+    lay.exchange_local(lc, fields)
+    for r in range(lay.world_size):
+        assert np.array_equal(fields[r][0].numpy(), _local(gx, cfg, lay, r)), r
