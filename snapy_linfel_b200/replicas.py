@@ -3,9 +3,9 @@ the data path.
 
 The single-domain step shards by slab decomposition with a ghost exchange per
 stage (layout.py); an ensemble shards trivially by whole members.  These
-helpers give the
-rank geometry, the max-over-ranks device timing every multi-rank number uses,
-and a size-balanced assignment of ensemble members to ranks.
+helpers give the rank geometry, the max-over-ranks device timing every
+multi-rank number uses, and a size-balanced assignment of ensemble members to
+ranks.
 """
 from __future__ import annotations
 
