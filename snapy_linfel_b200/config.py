@@ -156,10 +156,24 @@ class Integration:
 
 
 @dataclass
+class LayoutOptions:
+    """distribute.* keys (LayoutOptionsImpl::from_yaml,
+    src/layout/layout.cpp:165-185); the periodic flags follow the external
+    boundary types of x2 / x3 (src/mesh/meshblock_options.cpp:132-146)."""
+    type: str = "slab"
+    px: int = 1  # nb2
+    py: int = 1  # nb3
+    pz: int = 1  # nb1
+    periodic_x: bool = False
+    periodic_y: bool = False
+
+
+@dataclass
 class MeshBlockOptions:
     hydro: HydroConfig
     integration: Integration = field(default_factory=Integration)
     scalar_names: list = field(default_factory=list)
+    layout: LayoutOptions = field(default_factory=LayoutOptions)
 
     @staticmethod
     def from_yaml(path_or_dict) -> "MeshBlockOptions":
@@ -247,4 +261,8 @@ def _from_dict(cfg: dict) -> MeshBlockOptions:
                      nlim=int(integ.get("nlim", -1)), tlim=float(integ.get("tlim", 1.0e9)))
     if it.type != "rk3":
         raise ValueError(f"integrator {it.type!r} is not on this path (rk3 only)")
-    return MeshBlockOptions(hydro=hc, integration=it, scalar_names=names)
+    dist = cfg.get("distribute", {}) or {}
+    lay = LayoutOptions(type=str(dist.get("layout", "slab")), px=int(dist.get("nb2", 1)),
+                        py=int(dist.get("nb3", 1)), pz=int(dist.get("nb1", 1)),
+                        periodic_x="periodic" in bcs[2:4], periodic_y="periodic" in bcs[4:6])
+    return MeshBlockOptions(hydro=hc, integration=it, scalar_names=names, layout=lay)

@@ -68,6 +68,16 @@ class SlabLayout:
         self.coords = zorder_coords(px, py)
         self.rank_at = {xy: r for r, xy in enumerate(self.coords)}
 
+    @staticmethod
+    def from_options(options) -> "SlabLayout":
+        """from MeshBlockOptions.layout (the YAML 'distribute' section)"""
+        lo = options.layout
+        if lo.type != "slab":
+            raise ValueError(f"layout {lo.type!r} is not on this path (slab only)")
+        if lo.pz != 1:
+            raise ValueError("a slab layout keeps whole x1 columns: nb1 must be 1")
+        return SlabLayout(lo.px, lo.py, lo.periodic_x, lo.periodic_y)
+
     @property
     def world_size(self) -> int:
         return self.px * self.py
@@ -109,10 +119,11 @@ class SlabLayout:
             n = nx // p
             if n < cfg.nghost:
                 raise ValueError(f"x{a + 2}: blocks of {n} cells are thinner than the ghost zone")
-            dx = (hi - lo) / nx
+            # CoordinateOptionsImpl::repartition (src/coord/coordinate.cpp:167-191)
+            bmin = lo + l * (hi - lo) / p
             setattr(c, f"nx{a + 2}", n)
-            setattr(c, f"x{a + 2}min", lo + l * n * dx)
-            setattr(c, f"x{a + 2}max", lo + (l + 1) * n * dx)
+            setattr(c, f"x{a + 2}min", bmin)
+            setattr(c, f"x{a + 2}max", bmin + (hi - lo) / p)
             if self.periodic[a] or l > 0:
                 c.bc[face] = CUSTOM
             if self.periodic[a] or l < p - 1:

@@ -169,3 +169,36 @@ def test_exchange_in_one_process(case):
     lay.exchange_local(lc, fields)
     for r in range(lay.world_size):
         assert np.array_equal(fields[r][0].numpy(), _local(gx, cfg, lay, r)), r
+
+
+def test_yaml_distribute_section(tmp_path):
+    from snapy_linfel_b200.config import MeshBlockOptions
+
+    text = """
+geometry:
+  type: cartesian
+  bounds: {x1min: 0., x1max: 1000., x2min: 0., x2max: 1200., x3min: 0., x3max: 800.}
+  cells: {nx1: 8, nx2: 12, nx3: 8, nghost: 3}
+dynamics:
+  equation-of-state: {type: ideal-gas, gammad: 1.4}
+  reconstruct:
+    vertical: {type: weno5}
+    horizontal: {type: weno5}
+  riemann-solver: {type: lmars}
+boundary-condition:
+  external: {x1-inner: reflecting, x1-outer: reflecting, x2-inner: reflecting,
+             x2-outer: reflecting, x3-inner: periodic, x3-outer: periodic}
+integration: {type: rk3, cfl: 0.8}
+distribute: {layout: slab, nb2: 3, nb3: 2}
+"""
+    p = tmp_path / "dist.yaml"
+    p.write_text(text)
+    o = MeshBlockOptions.from_yaml(str(p))
+    lay = SlabLayout.from_options(o)
+    assert (lay.px, lay.py, lay.periodic) == (3, 2, (False, True))
+    c = lay.local_config(o.hydro, lay.rank_at[(2, 1)])
+    assert (c.nx2, c.nx3) == (4, 4)
+    assert (c.x2min, c.x2max, c.x3min, c.x3max) == (800.0, 1200.0, 400.0, 800.0)
+    p.write_text(text.replace("layout: slab", "layout: cubed-sphere"))
+    with pytest.raises(ValueError):
+        SlabLayout.from_options(MeshBlockOptions.from_yaml(str(p)))
