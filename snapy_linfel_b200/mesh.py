@@ -162,6 +162,43 @@ class MeshBlock:
         self.current_redo = 0
         return 0
 
+    # ---- restart files (snapy_linfel_b200/restart.py) ----
+    def write_restart(self, output_dir, basename, file_number, current_time, rank=0,
+                      final=False, output_file_numbers=(), output_next_times=()):
+        """this block's restart part (RestartOutput::write_output_file)"""
+        from . import restart
+
+        v = {"hydro_u": self.hydro_u, "hydro_w": self.hydro_w, "scalar_s": self.scalar_s,
+             "scalar_r": self.scalar_r}
+        return restart.write_part(v, output_dir, basename, rank, file_number, current_time,
+                                  self.cycle, final, output_file_numbers, output_next_times)
+
+    def restore(self, variables):
+        """state from restart variables (restart.load_restart): hydro_u,
+        hydro_w and scalar_s as stored (hydro_w derived from hydro_u when the
+        file has none: it is the last stage's input primitive state, which the
+        next CFL step reads), scalar_r = scalar_s / rho; returns the restart's
+        last_time"""
+        import torch
+
+        c = self.cfg
+        u = variables["hydro_u"]
+        if tuple(u.shape) != tuple(c.shape):
+            raise _lib.SnapbError(f"restart hydro_u has shape {tuple(u.shape)}, the block "
+                                  f"{tuple(c.shape)}")
+        self.hydro_u.copy_(u.to(self.device, torch.float64))
+        if "hydro_w" in variables:
+            self.hydro_w.copy_(variables["hydro_w"].to(self.device, torch.float64))
+        else:
+            self._call("snapb_cons2prim", ctypes.byref(c), _lib.ptr(self.hydro_u),
+                       _lib.ptr(self.hydro_w), self._stream())
+        if c.nscalar:
+            self.scalar_s.copy_(variables["scalar_s"].to(self.device, torch.float64))
+            self.scalar_r.copy_(self.scalar_s / self.hydro_u[0:1])
+        if "last_cycle" in variables:
+            self.cycle = int(variables["last_cycle"].reshape(-1)[0])
+        return float(variables["last_time"].reshape(-1)[0]) if "last_time" in variables else 0.0
+
     # ---- diagnostics ----
     def interior(self, t):
         return t[(slice(None),) + self.cfg.interior()]
