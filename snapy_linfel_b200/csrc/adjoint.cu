@@ -1497,7 +1497,7 @@ static cudaError_t launch_sweeps_adj_ns(const Geo& g, const Phys& p, const AdjBu
     int C = (int)std::max<size_t>(1, (48 * 1024) / per);
     C = std::min(C, 8);
     size_t smem = per * C;
-    cudaFuncSetAttribute(k_x1_adj<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    raise_smem_limit(k_x1_adj<NS>, 200 * 1024);
     int64_t ncol = (int64_t)g.nc2 * g.nc3;
     k_x1_adj<NS><<<(unsigned)((ncol + C - 1) / C), 256, smem, st>>>(g, p, b, C);
   } else {

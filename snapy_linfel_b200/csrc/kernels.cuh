@@ -1,6 +1,10 @@
 // kernels.cuh — launchers shared between the translation units of libsnapb.
 #pragma once
 
+#include <mutex>
+#include <utility>
+#include <vector>
+
 #include <string>
 
 #include "common.cuh"
@@ -105,6 +109,24 @@ __device__ __forceinline__ bool queue_next(const WorkQueue& q, int& m, int64_t& 
   m = lo;
   tile = item - q.prefix[lo];
   return true;
+}
+
+// Raise a kernel's dynamic shared-memory limit above the default 48 KB, once
+// per (device, kernel): the attribute belongs to the current device's
+// context.  The first launch of each kernel on a device should come before
+// any stream capture.
+template <class K>
+inline void raise_smem_limit(K kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::vector<std::pair<int, const void*>> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const void* f = reinterpret_cast<const void*>(kernel);
+  std::lock_guard<std::mutex> lock(mu);
+  for (auto& d : done)
+    if (d.first == dev && d.second == f) return;
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  done.emplace_back(dev, f);
 }
 
 // Copy member m's descriptor into shared memory, whole CTA, then barrier.  Call

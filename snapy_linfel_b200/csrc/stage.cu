@@ -492,11 +492,7 @@ static cudaError_t launch_x1_t(const Geo& g, const Phys& p, const StageBufs& b, 
   int C = x1_columns_per_cta(g, nvt);
   size_t smem = (size_t)C * x1_smem_per_column(g, nvt);
   if (smem > 200 * 1024) return cudaErrorInvalidConfiguration;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(k_x1<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_set = true;
-  }
+  raise_smem_limit(k_x1<NS>, 200 * 1024);
   int64_t ncol = (int64_t)g.nc2 * g.nc3;
   int64_t grid = (ncol + C - 1) / C;
   k_x1<NS><<<(unsigned)grid, 256, smem, st>>>(g, p, b, C, last ? 1 : 0);

@@ -637,12 +637,7 @@ cudaError_t launch_x1_32_batch(const Member32* mem, const Phys& p, const WorkQue
                                cudaStream_t st) {
 #define SNAPB_X1B(NS)                                                                         \
   case NS: {                                                                                  \
-    static bool attr = false;                                                                 \
-    if (!attr) {                                                                              \
-      cudaFuncSetAttribute(k_x1_32_batch<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,    \
-                           200 * 1024);                                                       \
-      attr = true;                                                                            \
-    }                                                                                         \
+    raise_smem_limit(k_x1_32_batch<NS>, 200 * 1024);                                        \
     int grid = persistent_grid(k_x1_32_batch<NS>, 256, smem, pg);                             \
     k_x1_32_batch<NS><<<grid, 256, smem, st>>>(mem, p, q, stage, last ? 1 : 0);               \
     break;                                                                                    \
@@ -711,11 +706,7 @@ static cudaError_t launch_x1_32t(const Geo& g, const Phys& p, const StageBufs32&
   int C = x1_columns_per_cta32(g, nvt);
   size_t smem = (size_t)C * x1_smem32_per_column(g, nvt);
   if (smem > 200 * 1024) return cudaErrorInvalidConfiguration;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(k_x1_32<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_set = true;
-  }
+  raise_smem_limit(k_x1_32<NS>, 200 * 1024);
   int64_t ncol = (int64_t)g.nc2 * g.nc3;
   k_x1_32<NS><<<(unsigned)((ncol + C - 1) / C), 256, smem, st>>>(g, p, b, C, last ? 1 : 0);
   return cudaGetLastError();

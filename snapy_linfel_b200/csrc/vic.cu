@@ -632,18 +632,10 @@ __global__ void __launch_bounds__(128) k_vic_column_pre(Geo g, Phys p, StageBufs
 }
 
 // the ring of a 128-thread CTA exceeds the default 48 KB of dynamic shared
-// memory; raise the kernel's limit once (before any graph capture)
+// memory (raise_smem_limit, kernels.cuh)
 template <class K>
 static void allow_ring_smem(K kernel, size_t bytes) {
-  static std::mutex mu;
-  static const void* done[64];
-  static int ndone = 0;
-  std::lock_guard<std::mutex> lock(mu);
-  const void* f = reinterpret_cast<const void*>(kernel);
-  for (int k = 0; k < ndone; ++k)
-    if (done[k] == f) return;
-  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  if (ndone < 64) done[ndone++] = f;
+  raise_smem_limit(kernel, bytes);
 }
 
 template <int N, class B>
