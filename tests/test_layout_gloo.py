@@ -202,3 +202,54 @@ distribute: {layout: slab, nb2: 3, nb3: 2}
     p.write_text(text.replace("layout: slab", "layout: cubed-sphere"))
     with pytest.raises(ValueError):
         SlabLayout.from_options(MeshBlockOptions.from_yaml(str(p)))
+
+
+@pytest.mark.parametrize("split", [(2, 1, False, False), (2, 2, True, True)])
+def test_oracle_blocks_reproduce_the_undivided_step(oracle, split):
+    """the oracle's own stage on each block, with the exchange after every
+    stage, against the oracle stepping the whole domain (CPU)"""
+    from snapy_linfel_b200 import problems
+    from snapy_linfel_b200.config import CONSERVED, PRIMITIVE
+
+    px, py, perx, pery = split
+    if py == 1:
+        opts, w, _ = problems.straka(nx2=16, nx1=12, implicit_scheme=1)
+    else:
+        opts, w, _ = problems.large_3d(nx3=8, nx2=8, nx1=12, nscalar=0)
+    c = opts.hydro
+    lay = SlabLayout(px, py, perx, pery)
+
+    def conserved(cfg, wp):
+        wp = np.ascontiguousarray(wp)
+        oracle.bc_apply(cfg, wp, PRIMITIVE)
+        u = oracle.prim2cons(cfg, wp)
+        oracle.bc_apply(cfg, u, CONSERVED)
+        return u
+
+    u = conserved(c, w.copy())
+    parts = []
+    for r in range(lay.world_size):
+        lc = lay.local_config(c, r)
+        parts.append((lc, conserved(lc, _local(w, c, lay, r))))
+    lay.exchange_local(parts[0][0], [[torch.from_numpy(p[1])] for p in parts])
+    whole = oracle.block(c)
+    blocks = [oracle.block(lc) for lc, _ in parts]
+    u0 = np.empty_like(u)
+    u0s = [np.empty_like(p[1]) for p in parts]
+    ww = np.empty_like(u)
+    wws = [np.empty_like(p[1]) for p in parts]
+    for _ in range(2):
+        for st in range(3):
+            whole.stage(st, 0.4, u, u0, ww)
+            for (lc, up), b, u0p, wp in zip(parts, blocks, u0s, wws):
+                b.stage(st, 0.4, up, u0p, wp)
+            lay.exchange_local(parts[0][0], [[torch.from_numpy(p[1])] for p in parts])
+    for r, (lc, up) in enumerate(parts):
+        j, k = lay.local_slices(c, r)
+        ng = c.nghost
+        lj = slice(ng, ng + j.stop - j.start) if c.nx2 > 1 else j
+        lk = slice(ng, ng + k.stop - k.start) if c.nx3 > 1 else k
+        a = up[:, lk, lj, ng:ng + c.nx1]
+        b = u[:, k, j, ng:ng + c.nx1]
+        for v in range(5):
+            assert np.abs(a[v] - b[v]).max() <= 1e-12 * np.abs(b[v]).max() + 1e-300, (r, v)
