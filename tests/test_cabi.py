@@ -166,3 +166,27 @@ int main() {{
     py = [ctypes.sizeof(MemberF32), MemberF32.u.offset, MemberF32.workspace.offset,
           MemberF32.workspace_bytes.offset, ctypes.sizeof(Tuning), Tuning.vic_regs.offset]
     assert vals == py
+
+
+def test_module_surface_rejects_cpu_tensors():
+    """the module classes have no CPU path: CPU tensors are refused before any
+    device call"""
+    torch = pytest.importorskip("torch")
+    from snapy_linfel_b200 import _lib
+    from snapy_linfel_b200.modules import (EquationOfState, Hydro, ImplicitHydro, Reconstruct,
+                                           RiemannSolver)
+
+    c = make_config(nx1=8, nx2=6)
+    x = torch.zeros(c.shape, dtype=torch.float64)
+    with pytest.raises(_lib.SnapbError):
+        EquationOfState(c).compute("U->W", [x])
+    with pytest.raises(_lib.SnapbError):
+        Hydro(c).forward(0.1, x)
+    with pytest.raises(_lib.SnapbError):
+        Reconstruct(c).forward(x, 3)
+    with pytest.raises(_lib.SnapbError):
+        RiemannSolver(c, "hllc").forward(x, x, 3, x)
+    with pytest.raises(_lib.SnapbError):
+        ImplicitHydro(c).forward(x, x, 0.1)
+    with pytest.raises(KeyError):
+        RiemannSolver(c, "exact")
