@@ -31,7 +31,7 @@ def _grids(cfg):
 
 
 def sod(nx1=1024):
-    """1-D Sod shock tube on x1 in [0, 1]."""
+    """1-D Sod shock tube on x1 in [0, 1] (1024 cells, WENO5 + HLLC, outflow)."""
     cfg = make_config(nx1=nx1, x1=(0.0, 1.0), gammad=1.4, recon1="weno5", shock1=True,
                       recon23="weno5", shock23=True, riemann="hllc",
                       bc=("outflow",) * 6)
@@ -50,7 +50,7 @@ def _isentropic(X1, p0, theta0, grav, rd, cp):
 
 
 def straka(nx2=1024, nx1=128, implicit_scheme=1, riemann="lmars"):
-    """2-D Straka cold-bubble density current.
+    """2-D Straka cold-bubble density current (1024 x 128 cells, WENO5 + LMARS).
 
     x2 in [-25.6, 25.6] km (bubble centred at x2 = 0), x1 in [0, 6.4] km,
     R = 287, cp = 1004, g = 9.81, T' = -15 K (cos(pi L) + 1)/2 for L <= 1 as
@@ -73,7 +73,7 @@ def straka(nx2=1024, nx1=128, implicit_scheme=1, riemann="lmars"):
 
 def warm_bubble_3d(nx3, nx2, nx1, amp, radius, center, dx=100.0, dz=100.0,
                    riemann="lmars", implicit_scheme=1):
-    """One 3-D dry warm-bubble member, doubly periodic."""
+    """One 3-D dry warm-bubble member of the 48-member ensemble, doubly periodic."""
     rd, cp, g = 287.0, 1004.0, 9.81
     cfg = make_config(nx1=nx1, nx2=nx2, nx3=nx3, x1=(0.0, nx1 * dz), x2=(0.0, nx2 * dx),
                       x3=(0.0, nx3 * dx), gammad=cp / (cp - rd), rgas=rd, recon1="weno5",
@@ -133,7 +133,7 @@ def gaussian_random_field(shape, dx, corr, sigma, seed):
 
 
 def adjoint_bubble(nx2=512, nx1=256, seed=7):
-    """2-D warm bubble of BASELINE config 4 (20 km x 10 km, HLLC)."""
+    """2-D warm bubble of the adjoint workload (512 x 256 cells, 20 km x 10 km, HLLC)."""
     rd, cp, g = 287.0, 1004.0, 9.81
     cfg = make_config(nx1=nx1, nx2=nx2, x1=(0.0, 10.0e3), x2=(0.0, 20.0e3),
                       gammad=cp / (cp - rd), rgas=rd, recon1="weno5", recon23="weno5",
@@ -154,7 +154,7 @@ def adjoint_bubble(nx2=512, nx1=256, seed=7):
 
 
 def large_3d(nx3=384, nx2=384, nx1=192, seed=11, nscalar=2, implicit_scheme=1):
-    """Large H2-He 3-D domain.
+    """Large H2-He 3-D domain (384 x 384 x 192 cells, WENO5 + Roe, two tracers).
 
     R = 3777, cp = 13000, g = 24.8; dry-adiabatic below 2/3 of the height,
     isothermal above; T0 = 166 K and p0 = 1e5 Pa at the bottom (chosen here,

@@ -8,7 +8,7 @@ as the FP64 target states it: the error in the state change is divided by
 the magnitude of the state itself (density, energy, sqrt(rho E) for the
 momenta, the scalar's own range), bound 1e-12 per step.  A tendency that is
 a cancellation of large fluxes (e.g. du[IVY] of a horizontally uniform
-pressure, exactly 0 on the CPU and ~1e-15 on the GPU) is judged against the
+pressure, exactly 0 on the CPU and ~1e-15 on the GPU) is measured against the
 state it changes, not against its own near-zero size.
 """
 import ctypes
