@@ -174,7 +174,10 @@ int snapb_implicit_correction(const snapb_hydro_config* cfg, const double* dt,
  * exits, so problems needing more (nx1 * columns * (N*N+N) * 8 bytes, N = 3
  * or 5) are rejected with SNAPB_ERR_ARG.  The first call on a device looks up
  * that array's address (once per device), so make it before any stream
- * capture.  All calls share the one array: calls whose kernels overlap on the
+ * capture.  The looked-up address is kept for the life of the process: after
+ * cudaDeviceReset (or any teardown of the device's primary context) in the
+ * same process it is stale, so do not call this entry point again after such
+ * a reset.  All calls share the one array: calls whose kernels overlap on the
  * GPU (different streams, or different host threads) race on it; serialize
  * them.  The solve writes every scratch entry before reading it, so nothing
  * is carried over from the previous call. */

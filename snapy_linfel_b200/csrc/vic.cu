@@ -1122,7 +1122,9 @@ static __device__ __align__(256) double
 // Device address of g_noalloc_vic_scratch on the current device.  In host code
 // the array's name only stands in for the symbol, so the address is looked up
 // with cudaGetSymbolAddress once per device (with that device current) and
-// cached.
+// cached for the life of the process.  The cache is not invalidated by
+// cudaDeviceReset; the header tells callers not to use this entry point after
+// resetting a device in the same process.
 cudaError_t noalloc_scratch(double** out) {
   static std::mutex mu;
   static double* addr[64] = {};

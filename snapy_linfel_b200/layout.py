@@ -166,9 +166,15 @@ class SlabLayout:
     def exchange(self, cfg: HydroConfig, rank: int, tensors, group=None):
         """Fill the exchange faces' ghost cells of each [nv, nc3, nc2, nc1]
         tensor (local block, after its local boundary fill) from the
-        neighbours' interiors."""
+        neighbours' interiors.  `rank` and the layout's ranks are ranks of
+        `group` (the default group when None); a subgroup may hold any set of
+        global ranks."""
         import torch
         import torch.distributed as dist
+
+        def peer_of(r):
+            # layout ranks are ranks of `group`; P2POp names global ranks
+            return r if group is None else dist.get_global_rank(group, r)
 
         for dim, sends, recvs in self._face_plan(cfg, rank):
             ops, bufs = [], []
@@ -180,7 +186,7 @@ class SlabLayout:
                     idx[dim] = sl
                     buf = t[tuple(idx)].contiguous()
                     bufs.append(buf)
-                    ops.append(dist.P2POp(dist.isend, buf, peer, group, 4 * ti + tag))
+                    ops.append(dist.P2POp(dist.isend, buf, peer_of(peer), group, 4 * ti + tag))
                 for peer, sl, tag in recvs:
                     if peer < 0:
                         continue
@@ -189,7 +195,7 @@ class SlabLayout:
                     shape = list(t.shape)
                     shape[dim] = sl.stop - sl.start
                     buf = torch.empty(shape, dtype=t.dtype, device=t.device)
-                    ops.append(dist.P2POp(dist.irecv, buf, peer, group, 4 * ti + tag))
+                    ops.append(dist.P2POp(dist.irecv, buf, peer_of(peer), group, 4 * ti + tag))
                     bufs.append((t, tuple(idx), buf))
             if not ops:
                 continue

@@ -13,18 +13,15 @@ import pytest
 
 from snapy_linfel_b200 import problems
 
+from errnorm import rel_l1_linf
+
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
 
 def _errors(a, b, it):
-    out = []
-    for v in range(a.shape[0]):
-        x, y = a[v][it], b[v][it]
-        l1 = float(np.abs(x - y).sum() / max(np.abs(y).sum(), 1e-300))
-        linf = float(np.abs(x - y).max() / max(np.abs(y).max(), 1e-300))
-        out.append((l1, linf))
-    return out
+    return rel_l1_linf(np.stack([a[v][it] for v in range(a.shape[0])]),
+                       np.stack([b[v][it] for v in range(b.shape[0])]))
 
 
 def _run_pair(opts, w, r, dts, reference="mean"):

@@ -8,6 +8,8 @@ import pytest
 
 from snapy_linfel_b200 import problems
 
+from errnorm import assert_finite
+
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
@@ -30,12 +32,14 @@ def _compare(opts, w, r, layout, steps=3):
     it = (slice(None),) + opts.hydro.interior()
     a = parts.gather()[it].cpu().numpy()
     b = whole.hydro_u[it].cpu().numpy()
+    assert_finite(a, b)
     for v in range(a.shape[0]):
         scale = max(np.abs(b[v]).max(), 1e-300)
         assert np.abs(a[v] - b[v]).max() / scale < 1e-12, v
     if whole.scalar_s is not None:
         sa = parts.gather("scalar_s")[it].cpu().numpy()
         sb = whole.scalar_s[it].cpu().numpy()
+        assert_finite(sa, sb)
         assert np.abs(sa - sb).max() / np.abs(sb).max() < 1e-12
 
 

@@ -8,13 +8,14 @@ import pytest
 from snapy_linfel_b200 import problems
 from snapy_linfel_b200.config import CONSERVED, PRIMITIVE
 
+from errnorm import assert_finite, relerr
+
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
 
 def _rel(a, b):
-    return max(float(np.abs(a[v] - b[v]).max() / max(np.abs(b[v]).max(), 1e-300))
-               for v in range(a.shape[0]))
+    return relerr(a, b)
 
 
 @pytest.fixture(scope="module")
@@ -84,6 +85,7 @@ def test_hydro_and_implicit_modules(case, oracle):
     du_ref = oracle.block(c).hydro_forward(0.5, u, w_ref)
     it = (slice(None),) + c.interior()
     scale = np.abs(u[it]).max(axis=(1, 2, 3), keepdims=True)
+    assert_finite(du)
     assert (np.abs(du.cpu().numpy()[it] - du_ref[it]) / scale).max() < 1e-12
     # CFL limit of the primitive state
     dt = hyd.max_time_step(torch.from_numpy(w_ref).cuda())
@@ -97,4 +99,5 @@ def test_hydro_and_implicit_modules(case, oracle):
                                0.5)
     ref = du_e.copy()
     oracle.implicit_correction(c, 0.5, ref, w_full)
+    assert_finite(corr)
     assert (np.abs(corr.cpu().numpy()[it] - (ref - du_e)[it]) / scale).max() < 1e-12

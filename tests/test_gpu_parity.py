@@ -19,6 +19,8 @@ import pytest
 from snapy_linfel_b200 import problems
 from snapy_linfel_b200.config import CONSERVED, PRIMITIVE, SCALAR, make_config
 
+from errnorm import assert_finite, relerr, state_err, state_scale  # noqa: F401
+
 pytestmark = pytest.mark.gpu
 
 torch = pytest.importorskip("torch")
@@ -35,35 +37,6 @@ def L():
 
 def dev(a):
     return torch.from_numpy(np.ascontiguousarray(a)).cuda()
-
-
-def relerr(a, b):
-    """per-variable relative max error"""
-    a = np.asarray(a)
-    b = np.asarray(b)
-    if a.ndim <= 1:
-        return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
-    out = []
-    for v in range(a.shape[0]):
-        den = max(np.max(np.abs(b[v])), 1e-300)
-        out.append(float(np.max(np.abs(a[v] - b[v])) / den))
-    return max(out)
-
-
-def state_scale(u):
-    """per-variable magnitude of a conserved state [nvar, ...]"""
-    u = np.asarray(u)
-    rho = np.max(np.abs(u[0]))
-    en = np.max(np.abs(u[4]))
-    mom = max(np.sqrt(rho * en), np.max(np.abs(u[1:4])))
-    return np.array([rho, mom, mom, mom, en])
-
-
-def state_err(a, b, u):
-    """max over variables of max|a_v - b_v| / scale_v(u)"""
-    sc = state_scale(u)
-    a, b = np.asarray(a), np.asarray(b)
-    return max(float(np.max(np.abs(a[v] - b[v])) / sc[v]) for v in range(a.shape[0]))
 
 
 def random_prim(rng, shape):

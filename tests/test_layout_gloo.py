@@ -154,6 +154,52 @@ def test_exchange_between_gloo_ranks(case):
         assert dt == 1.0  # MIN over ranks
 
 
+def _subgroup_worker(rank, world, port, out):
+    """global ranks 1 and 2 form a subgroup holding a 2 x 1 layout; global
+    rank 0 only takes part in creating the group"""
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        sub = dist.new_group([1, 2])
+        if rank == 0:
+            out.put((rank, True, 0.0))
+            return
+        lrank = dist.get_group_rank(sub, rank)
+        kw, (px, py, perx, pery) = CASES[0]
+        cfg = make_config(**kw)
+        lay = SlabLayout(px, py, perx, pery)
+        g, gx = _global_with_wraps(cfg, lay, 5)
+        lc = lay.local_config(cfg, lrank)
+        t = torch.from_numpy(_local(g, cfg, lay, lrank))
+        _poison(t, cfg, lay, lrank)
+        lay.exchange(lc, lrank, [t], group=sub)
+        ok = bool(np.array_equal(t.numpy(), _local(gx, cfg, lay, lrank)))
+        dt = torch.tensor([3.0 + rank])
+        lay.min_dt(dt, group=sub)
+        out.put((rank, ok, float(dt)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_exchange_in_a_subgroup_of_nonzero_ranks():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_subgroup_worker, args=(r, 3, port, q)) for r in range(3)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in range(3))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for r, ok, dt in res:
+        assert ok, f"rank {r}: ghost cells differ from the undivided array"
+        if r:
+            assert dt == 4.0  # MIN over the subgroup (global ranks 1 and 2)
+
+
 @pytest.mark.parametrize("case", range(len(CASES)))
 def test_exchange_in_one_process(case):
     kw, (px, py, perx, pery) = CASES[case]
