@@ -54,6 +54,11 @@
 #include <snap/riemann/hllc_impl.h>
 #include <snap/riemann/lmars_impl.h>
 #include <snap/riemann/roe_impl.h>
+// the implicit solve, compiled against the Eigen subset in ref_shim/Eigen
+#include <snap/implicit/forward_sweep_impl.h>
+#include <snap/implicit/vic_assemble_full_impl.h>
+#include <snap/implicit/vic_assemble_partial_impl.h>
+#include <snap/implicit/vic_redistribute_impl.h>
 #endif
 
 namespace orc {
@@ -1152,6 +1157,54 @@ inline void vic_column(double* du, const double* w, double* mass, int nlayer, in
   vic_reduce_redistribute(du, w, mass, dflat.data(), &vol, 0, nlayer, sv, 0, N);
 }
 
+#ifdef ORC_REFERENCE_KERNELS
+// One column through the reference's own implicit code, called the way
+// vic_{assemble,solve,redistribute}_{partial,full}_cpu call it
+// (src/implicit/implicit_dispatch.cpp:22-180): du/w/mass point at the
+// column's first interior cell with variable stride sv and layer stride 1, so
+// index -1 and nlayer reach the x1 ghost cells as the interior views do in
+// ImplicitHydroImpl::forward (src/implicit/implicit_hydro.cpp:141-176).
+template <int N>
+inline void vic_column_reference(double* du, const double* w, double* mass, int nlayer,
+                                 int64_t sv, double area, double vol, double dt, double grav,
+                                 double gamma) {
+  using Mat = Eigen::Matrix<double, N, N>;
+  using Vec = Eigen::Matrix<double, N, 1>;
+  std::vector<Mat> a(nlayer), b(nlayer), c(nlayer);
+  std::vector<Vec> delta(nlayer);
+  std::vector<double> gam(nlayer + 2, gamma), ar(nlayer + 1, area), vl(nlayer, vol);
+  std::vector<double> mfix;
+  if (!mass) {
+    mfix.assign((size_t)(IDN + 1) * sv, 0.0);
+    mass = mfix.data();
+  }
+  double* wp = const_cast<double*>(w);
+  const int il = 0, iu = nlayer - 1, dir = 0, ny = 0, nvapor = 0;
+  const int stride1 = (int)sv, stride2 = 1;
+  if (N == 5) {
+    snap::vic_assemble_full_impl<double>(du, wp, gam.data() + 1, ar.data(), vl.data(), dt, grav,
+                                         il, iu, dir, ny, stride1, stride2, true, true, false,
+                                         reinterpret_cast<Eigen::Matrix<double, 5, 5>*>(a.data()),
+                                         reinterpret_cast<Eigen::Matrix<double, 5, 5>*>(b.data()),
+                                         reinterpret_cast<Eigen::Matrix<double, 5, 5>*>(c.data()));
+  } else {
+    for (int i = 0; i < nlayer; ++i)
+      snap::vic_assemble_partial_impl<double>(
+          reinterpret_cast<Eigen::Matrix<double, 3, 3>*>(a.data()),
+          reinterpret_cast<Eigen::Matrix<double, 3, 3>*>(b.data()),
+          reinterpret_cast<Eigen::Matrix<double, 3, 3>*>(c.data()), wp, gam.data() + 1,
+          ar.data(), vl.data(), i, il, iu, dt, grav, dir, ny, stride1, stride2, true, true);
+  }
+  snap::ForwardSweep<double, N>(a.data(), b.data(), c.data(), delta.data(), du, dt, il, iu, dir,
+                                ny, stride1, stride2, true, true);
+  snap::vic_backward_reduce<double, N>(du, wp, a.data(), delta.data(), vl.data(), c[0].data(),
+                                       il, iu, dir, ny, stride1, stride2);
+  for (int i = il; i <= iu; ++i)
+    snap::vic_redistribute_cell<double, N>(du, wp, mass, delta.data(), vl.data(), c[0].data(), i,
+                                           dir, ny, nvapor, stride1, stride2);
+}
+#endif
+
 inline void implicit_correction(const Grid& g, double dt, double* du, const double* w,
                                 double* mass) {
   int scheme = g.c.implicit_scheme;
@@ -1165,12 +1218,21 @@ inline void implicit_correction(const Grid& g, double dt, double* du, const doub
     int j = g.jl + (int)(col % nj);
     int k = g.kl + (int)(col / nj);
     int64_t off = g.idx(k, j, g.il);
+#ifdef ORC_REFERENCE_KERNELS
+    if (full)
+      vic_column_reference<5>(du + off, w + off, mass ? mass + off : nullptr, nlayer, sv,
+                              g.area1(), g.vol(), dt, g.c.grav1, g.c.gammad);
+    else
+      vic_column_reference<3>(du + off, w + off, mass ? mass + off : nullptr, nlayer, sv,
+                              g.area1(), g.vol(), dt, g.c.grav1, g.c.gammad);
+#else
     if (full)
       vic_column<5>(du + off, w + off, mass ? mass + off : nullptr, nlayer, sv, g.area1(),
                     g.area1(), g.vol(), dt, g.c.grav1, g.c.gammad);
     else
       vic_column<3>(du + off, w + off, mass ? mass + off : nullptr, nlayer, sv, g.area1(),
                     g.area1(), g.vol(), dt, g.c.grav1, g.c.gammad);
+#endif
   });
 }
 

@@ -236,6 +236,7 @@ class MeshBlock {
                              stream()),
               "snapb_bc_apply");
       }
+      --cycle;  // the rejected step does not count (step() counted it)
       return 1;
     }
     current_redo = 0;
@@ -272,6 +273,8 @@ PYBIND11_MODULE(_snapb_host, m) {
       .def("check_redo", &MeshBlock::check_redo, pybind11::arg("max_redo") = 5)
       .def_readonly("hydro_u", &MeshBlock::hydro_u)
       .def_readonly("hydro_w", &MeshBlock::hydro_w)
+      .def_readonly("hydro_u0", &MeshBlock::hydro_u0)
+      .def_readonly("current_redo", &MeshBlock::current_redo)
       .def_readonly("scalar_s", &MeshBlock::scalar_s)
       .def_readonly("scalar_r", &MeshBlock::scalar_r)
       .def_readonly("dt", &MeshBlock::dt)

@@ -158,6 +158,7 @@ class MeshBlock:
             if c.nscalar:
                 self._call("snapb_bc_apply", ctypes.byref(c), _lib.ptr(self.scalar_s),
                            c.nscalar, SCALAR, st)
+            self.cycle -= 1  # the rejected step does not count (step() counted it)
             return 1
         self.current_redo = 0
         return 0

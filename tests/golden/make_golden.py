@@ -8,12 +8,14 @@ Run in a container that has the reference sources:
     python tests/golden/make_golden.py
 
 ``oracle/_ref/libsnapref.so`` evaluates WENO5/WENO3/cp5/cp3 (interp_impl.h),
-HLLC/LMARS/Roe (hllc_impl.h, lmars_impl.h, roe_impl.h) and the ideal-gas
-cons2prim (ideal_gas_impl.h) with the reference's code; the orchestration
-around them (reconstruction grouping and edge fills, PLM, divergence,
-forcing, boundary fills, RK3 and the implicit solve, which needs Eigen and is
-restated) is the oracle's.  Inputs are seeded, so the fixtures are
-reproducible.
+HLLC/LMARS/Roe (hllc_impl.h, lmars_impl.h, roe_impl.h), the ideal-gas
+cons2prim (ideal_gas_impl.h) and the vertically implicit solve
+(vic_assemble_{partial,full}_impl.h, forward_sweep_impl.h,
+vic_redistribute_impl.h, math/{ludcmp,lubksb}.h, compiled against the Eigen
+subset in oracle/ref_shim/Eigen) with the reference's code; the
+orchestration around them (reconstruction grouping and edge fills, PLM,
+divergence, forcing, boundary fills, RK3) is the oracle's.  Inputs are
+seeded, so the fixtures are reproducible.
 """
 import os
 import sys
@@ -117,6 +119,32 @@ def main():
                 blk.stage(s, dt, u, u0, w0)
         out[f"straka{scheme}_dts"] = np.array(dts)
         out[f"straka{scheme}_u_final"] = u
+    # ---- the implicit correction alone (schemes 1 and 9): a Straka column
+    # set with a seeded flow and a noisy explicit tendency, and a 3-D box ----
+    for scheme in (1, 9):
+        for case in ("straka", "box"):
+            if case == "straka":
+                opts, w0, _ = problems.straka(nx2=16, nx1=20, implicit_scheme=scheme)
+            else:
+                opts, w0, _ = problems.warm_bubble_3d(4, 5, 12, amp=2.0, radius=500.0,
+                                                       center=(200.0, 250.0, 500.0),
+                                                       implicit_scheme=scheme)
+            c = opts.hydro
+            w0[1:4] += 0.3 * rng.standard_normal(w0[1:4].shape)
+            R.bc_apply(c, w0, 0)
+            u = R.prim2cons(c, w0)
+            R.bc_apply(c, u, 1)
+            ce = c.copy()
+            ce.implicit_scheme = 0
+            wf = np.empty_like(u)
+            du = R.block(ce).hydro_forward(2.0, u, wf)
+            du += 1e-3 * rng.standard_normal(du.shape) * np.abs(du).max(axis=(1, 2, 3),
+                                                                      keepdims=True)
+            key = f"vic{scheme}_{case}"
+            out[key + "_w"], out[key + "_du_in"] = wf, du.copy()
+            mass = np.zeros_like(u)
+            R.implicit_correction(c, 2.0, du, wf, mass)
+            out[key + "_du_out"], out[key + "_mass"] = du, mass
     path = os.path.join(HERE, "ref_kernels.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, os.path.getsize(path), "bytes,", len(out), "arrays")
