@@ -23,8 +23,13 @@ Arms:
                     oracle/_ref build (the reference's own *_impl.h kernels
                     under the restated orchestration), all host threads, on a
                     bounded sub-domain of the same workload.
-Multi-GPU: the hydro step is run as independent replicas (one domain per
-rank, no exchange) — ``scaling: weak``.
+Multi-GPU (one process per GPU): the ensemble's members are sharded over
+the ranks by size (no data-path exchange; the step is the whole ensemble,
+``scaling: strong``); a single-domain workload is split into x2 slabs with
+the ghost exchange after every stage and a MIN all-reduce of dt
+(``--decomp slab``, ``scaling: strong``) or run as replicas
+(``--decomp replicas``, ``scaling: weak``).  Every time is the maximum over
+the ranks of CUDA-event durations.
 """
 from __future__ import annotations
 
@@ -86,20 +91,24 @@ def algo_bytes_per_cell_update(cfg, elem=8) -> int:
     return 3 * (cfg.nvar + cfg.nscalar) * elem
 
 
-def kernel_algo_bytes_per_cell(name, cfg, elem=8) -> int:
-    """Compulsory HBM bytes per interior cell of one launch of a stage kernel.
+def kernel_io_bytes_per_cell(name, cfg, elem=8) -> int:
+    """The bytes a stage kernel must move per interior cell given the
+    kernel split (its inputs and outputs, each once), reported beside the
+    roofline; the roofline itself uses the fused-stage bytes of
+    algo_bytes_per_cell_update.
 
     x1 sweep: read u, s; write w, r and the x1 flux sums (3 NV values).
     x2/x3 sweep: read w, r and the running sums; write the sums (3 NV values).
-    implicit_vic (assemble + sweep + finish, timed together): read w, du,
-    u, u0, s, s0, r; write u, s, r and the FP64 mass correction.
+    implicit_vic (one fused kernel: blocks, elimination, redistribution, RK
+    update): read w, du, u, u0, and per scalar s, s0, r, ds; write u, s, r;
+    the FP64 plain form also writes the FP64 mass correction.
     """
     nv = cfg.nvar + cfg.nscalar
     ns = cfg.nscalar
     if name in ("x1_sweep", "x2_sweep", "x3_sweep"):
         return 3 * nv * elem
     if name == "implicit_vic":
-        return (5 + nv + 10 + 3 * ns + 5 + 2 * ns) * elem + 8
+        return (5 + 5 + 5 + 5 + 4 * ns + 5 + 2 * ns) * elem + (8 if elem == 8 else 0)
     return 0
 
 
@@ -294,32 +303,38 @@ def rel_errors(a, b, it):
 
 
 # DRAM bytes per interior cell of one launch (dram__bytes_read.sum +
-# dram__bytes_write.sum) from the ncu captures summarised in profiles/, scaled
-# to a launch by the cells it processes (traffic grows with the cells): the
-# batched FP32 kernels of the 12-member ensemble capture.
+# dram__bytes_write.sum) of the batched FP32 kernels, from one-kernel ncu
+# captures of the first 12 ensemble members, scaled to a launch by the cells
+# it processes (their traffic grows in proportion to the cells).  None: not
+# captured for the current build.
 NCU_TRAFFIC_PER_CELL_F32 = {"x1_sweep": 68.2, "x2_sweep": 63.2, "x3_sweep": 63.2,
-                            "implicit_vic": 243.9 + 104.1}
+                            "implicit_vic": None}
 
 
 def dominant_roofline(kern, cfg, cells, elem, peak, peak_src):
-    """Roofline line of the kernel with the largest share of the timed region."""
+    """Roofline line of the kernel with the largest share of the timed region:
+    achieved = the fused stage's algorithmic bytes per cell update (read u,
+    read u0, write u: 3 (nvar + nscalar) values) x the cells of one launch,
+    over the launch's CUDA-event duration."""
     if not kern:
         return None
     name, (tot_ms, n) = max(kern.items(), key=lambda kv: kv[1][0])
     per_launch_s = tot_ms / n / 1e3
-    per_cell = kernel_algo_bytes_per_cell(name, cfg, elem)
+    per_cell = algo_bytes_per_cell_update(cfg, elem)
     ach = per_cell * cells / per_launch_s / 1e9
     share = tot_ms / sum(v[0] for v in kern.values())
     traffic = None
-    if elem == 4 and name in NCU_TRAFFIC_PER_CELL_F32:
+    if elem == 4 and NCU_TRAFFIC_PER_CELL_F32.get(name) is not None:
         traffic = NCU_TRAFFIC_PER_CELL_F32[name] * cells
+    io = kernel_io_bytes_per_cell(name, cfg, elem)
     return {"kernel": name, "bound": "hbm", "achieved": ach, "peak": peak,
             "peak_source": peak_src, "unit": "GB/s", "frac": ach / peak,
             "traffic": traffic,
-            "traffic_source": ("ncu capture of the 12-member ensemble, bytes per cell x cells "
-                               "(profiles/batched_fp32_kernels_warm_bubble_ensemble.md)"
-                               if traffic is not None else None),
+            "traffic_source": ("one-kernel ncu capture of the first 12 ensemble members, "
+                               "DRAM bytes per cell x cells" if traffic is not None else None),
             "algorithmic_bytes_per_cell": per_cell,
+            "kernel_io_bytes_per_cell": io,
+            "kernel_io_frac": io * cells / per_launch_s / 1e9 / peak,
             "cells_per_launch": cells, "ms_per_launch": per_launch_s * 1e3,
             "share_of_timed_kernels": share}
 
@@ -485,9 +500,81 @@ def run_adjoint_timing(args, opts, state, cells, stream, barrier):
 
 def ensemble_launches_per_step(cfg) -> int:
     """kernels of one batched step: CFL fill + reduce + final, then per stage
-    x1, x2, x3 sweeps, implicit column + finish, boundary fill(s)"""
-    per_stage = 3 + (2 if cfg.implicit_scheme else 0) + 1 + (1 if cfg.nscalar else 0)
+    x1, x2, x3 sweeps, the implicit solve, boundary fill(s)"""
+    per_stage = 3 + (1 if cfg.implicit_scheme else 0) + 1 + (1 if cfg.nscalar else 0)
     return 3 + 3 * per_stage
+
+
+def cpu_baseline_block(workload_name):
+    """the reference CPU path on the host cores (all threads, and one
+    thread), on a bounded sample of the workload"""
+    try:
+        from oracle.pyoracle import lib_path
+
+        kind = "reference" if os.path.exists(lib_path("reference")) else "port"
+        v, per_step, cores, sample, _ = cpu_sample_run(kind, 1, 0, workload_name=workload_name)
+        v1, per1, _, sample1, _ = cpu_sample_run(kind, 1, 0, threads=1,
+                                                 workload_name=workload_name, nx_h=32)
+        return {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample,
+                "single_core": {"value": v1, "unit": UNIT, "cores": 1, "sample": sample1}}
+    except Exception as e:  # the baseline is reported, never required
+        return {"value": None, "unit": UNIT, "cores": None, "kind": None,
+                "sample": f"failed: {e}"}
+
+
+def run_single_domain_forms(args, stream, barrier, nx=(384, 384, 192), acc_steps=10):
+    """The 384 x 384 x 192 H2-He domain (WENO5 + Roe + VIC, two tracers):
+    the FP64 plain form and the FP32 perturbation form timed on the same
+    state, and compared per field after acc_steps steps with the same dt."""
+    import torch
+
+    from snapy_linfel_b200 import problems
+    from snapy_linfel_b200.mesh import MeshBlock, MeshBlockF32
+
+    opts, w, r = problems.large_3d(nx3=nx[0], nx2=nx[1], nx1=nx[2])
+    cells = interior_cells(opts.hydro)
+    steps = max(1, min(args.steps, 5))
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = {"workload": WORKLOAD_DESC["c5"], "steps": steps}
+    for name, cls in (("fp64_plain", MeshBlock), ("fp32_perturbation", MeshBlockF32)):
+        mb = cls(opts, device="cuda")
+        mb.initialize(w, r)
+        for _ in range(args.warmup):
+            mb.step()
+        barrier()
+        ev0.record(stream)
+        for _ in range(steps):
+            mb.step()
+        ev1.record(stream)
+        barrier()
+        ms = ev0.elapsed_time(ev1)
+        out[name] = {"value": cells * 3 * steps / (ms / 1e3) / 1e6,
+                     "ms_per_step": ms / steps}
+        del mb
+        torch.cuda.empty_cache()
+    out["fp32_over_fp64"] = out["fp32_perturbation"]["value"] / out["fp64_plain"]["value"]
+    a64 = MeshBlock(opts, device="cuda")
+    a64.initialize(w, r)
+    a32 = MeshBlockF32(opts, device="cuda")
+    a32.initialize(w, r)
+    for _ in range(acc_steps):
+        dt = a64.max_time_step().clone()
+        a64.step(dt)
+        a32.step(dt)
+    torch.cuda.synchronize()
+    it = (slice(None),) + opts.hydro.interior()
+    acc = rel_errors(a32.state64(), a64.hydro_u, it[1:])
+    acc["steps"] = acc_steps
+    sacc = rel_errors(a32.scalar_s.double(), a64.scalar_s, it[1:])
+    acc["scalar_rel_l1"] = sacc["rel_l1"]
+    rb = a32.ref_rho.view(1, 1, -1)
+    rp32 = (a32.state64()[0] - rb)[it[1:]]
+    rp64 = (a64.hydro_u[0] - rb)[it[1:]]
+    acc["rho_prime_rel_l1"] = float((rp32 - rp64).abs().sum() / rp64.abs().sum())
+    out["accuracy_fp32_vs_fp64"] = acc
+    del a64, a32
+    torch.cuda.empty_cache()
+    return out
 
 
 def perturbation_fields(u, cfg, rb, pb):
@@ -534,11 +621,22 @@ def run_ensemble(args):
 
         return max_over_ranks(ms, dev)
 
-    members = problems.ensemble_members(n=48, seed=2024)
+    everyone = problems.ensemble_members(n=48, seed=2024)
     if args.workload == "c3s":  # a quarter of the ensemble, for profiling captures
-        members = members[:12]
+        everyone = everyone[:12]
+    sizes = [o.hydro.nx1 * o.hydro.nx2 * o.hydro.nx3 for o, _, _ in everyone]
+    # the members are independent: on N GPUs each rank advances its share
+    # (size-balanced), no data-path exchange; the step is the whole ensemble
+    if world > 1:
+        from snapy_linfel_b200.replicas import shard_members
+
+        mine = shard_members(sizes, world)[rank]
+    else:
+        mine = list(range(len(everyone)))
+    members = [everyone[k] for k in mine]
     cfg0 = members[0][0].hydro
-    cells = sum(o.hydro.nx1 * o.hydro.nx2 * o.hydro.nx3 for o, _, _ in members)
+    cells = sum(sizes[k] for k in mine)          # this rank's cells
+    cells_total = sum(sizes)                     # the whole ensemble
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
     # ---- batched FP32: autotune, capture, replay ----
@@ -565,7 +663,7 @@ def run_ensemble(args):
         barrier()
         clk.mark_end()
     ms32 = max_ms(ev0.elapsed_time(ev1))
-    value32 = world * cells * 3 * args.steps / (ms32 / 1e3) / 1e6
+    value32 = cells_total * 3 * args.steps / (ms32 / 1e3) / 1e6
     _lib.timing_enable(True)
     for _ in range(2):
         ens.step_eager()
@@ -587,10 +685,12 @@ def run_ensemble(args):
             h.copy_(b.hydro_u, non_blocking=True)
     ev1.record(stream)
     barrier()
-    e2e = world * cells * 3 * args.steps / (max_ms(ev0.elapsed_time(ev1)) / 1e3) / 1e6
+    e2e = cells_total * 3 * args.steps / (max_ms(ev0.elapsed_time(ev1)) / 1e3) / 1e6
     del hus
 
-    # ---- plain FP64: member after member through snapb_stage ----
+    # ---- plain FP64: member after member through snapb_stage, the whole
+    # step (every member's CFL and three stages) replayed from one CUDA graph
+    # like the batched form, and eagerly for reference ----
     blocks = []
     for opts, w, r in members:
         mb = MeshBlock(opts, device=dev)
@@ -606,8 +706,23 @@ def run_ensemble(args):
             mb.step()
     ev1.record(stream)
     barrier()
+    ms64_eager = max_ms(ev0.elapsed_time(ev1))
+    g64 = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g64):
+        for mb in blocks:
+            mb.step()
+    for _ in range(args.warmup):
+        g64.replay()
+    barrier()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        g64.replay()
+    ev1.record(stream)
+    barrier()
     ms64 = max_ms(ev0.elapsed_time(ev1))
-    value64 = world * cells * 3 * args.steps / (ms64 / 1e3) / 1e6
+    del g64
+    value64 = cells_total * 3 * args.steps / (ms64 / 1e3) / 1e6
+    value64_eager = cells_total * 3 * args.steps / (ms64_eager / 1e3) / 1e6
 
     # ---- accuracy: both forms from the same state with the same dt ----
     ens.restore(init32)
@@ -659,45 +774,47 @@ def run_ensemble(args):
                                  barrier)
         adj["workload"] = "adjoint_bubble_2d_512x256_weno5_hllc_vic3"
 
+    # ---- the single 384 x 384 x 192 domain: FP32 form vs FP64 form ----
+    single = None
+    if world == 1 and not args.no_single_domain:
+        single = run_single_domain_forms(args, stream, barrier)
+
     # ---- roofline of the dominant batched kernel ----
     peak, peak_src = measured_peaks()
     roof = dominant_roofline(kern32, cfg0, cells, 4, peak, peak_src)
     st32 = ms32 / 1e3 / (3 * args.steps)
-    bw32 = algo_bytes_per_cell_update(cfg0, 4) * cells / st32 / 1e9
+    bw32 = algo_bytes_per_cell_update(cfg0, 4) * cells_total / st32 / 1e9
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        try:
-            from oracle.pyoracle import lib_path
-
-            kind = "reference" if os.path.exists(lib_path("reference")) else "port"
-            v, per_step, cores, sample, _ = cpu_sample_run(kind, 1, 0, workload_name="c3")
-            cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
-        except Exception as e:  # the baseline is reported, never required
-            cpu = {"value": None, "unit": UNIT, "cores": None, "kind": None,
-                   "sample": f"failed: {e}"}
+        cpu = cpu_baseline_block("c3")
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value32, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms32 / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": "f32 (perturbation over f64 reference)", "data": "synthetic",
-            "config": {"workload": WORKLOAD_DESC[args.workload], "members": len(members),
-                       "cells_per_gpu": cells, "rk_stages_per_step": 3,
+            "config": {"workload": WORKLOAD_DESC[args.workload], "members": len(everyone),
+                       "cells": cells_total, "cells_rank0": cells, "rk_stages_per_step": 3,
                        "form": "batched_fp32_perturbation (persistent work queue, CUDA graph)",
                        "tuning": tune["best"],
                        "l2_policy": "inputs larger than L2 (ensemble state > 126 MB)",
-                       "parallelism": f"replicas x{world}"},
+                       "parallelism": (f"members sharded over {world} ranks" if world > 1
+                                       else "one GPU")},
             "forms": {
                 "batched_fp32": {"value": value32, "ms_per_step": ms32 / args.steps,
                                  "kernel_ms_per_launch": {k: round(v[0] / v[1], 4)
                                                           for k, v in kern32.items()},
                                  "stage_roofline": {"achieved": bw32, "peak": peak,
                                                     "unit": "GB/s", "frac": bw32 / peak}},
-                "plain_fp64_member_by_member": {"value": value64,
-                                                "ms_per_step": ms64 / args.steps},
+                "plain_fp64_member_by_member_graph": {"value": value64,
+                                                      "ms_per_step": ms64 / args.steps},
+                "plain_fp64_member_by_member_eager": {"value": value64_eager,
+                                                      "ms_per_step": ms64_eager / args.steps},
                 "batched_fp32_over_plain_fp64": value32 / value64,
+                "batched_fp32_over_plain_fp64_eager": value32 / value64_eager,
+                "single_domain_384x384x192": single,
                 "accuracy_fp32_vs_fp64": acc,
                 "autotuner": tune,
             },
@@ -707,6 +824,7 @@ def run_ensemble(args):
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes},
             "gpu_launches": ensemble_launches_per_step(cfg0) * args.steps,
+            "gpu_launches_counts": "this rank's kernels in the timed region",
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
@@ -830,9 +948,29 @@ def run_ours(args):
     opts, w, r, desc = workload(args.workload)
     _STATE_CACHE[args.workload] = (w, r)
     cfg = opts.hydro
-    mb = MeshBlock(opts, device=f"cuda:{local}")
-    mb.initialize(w, r)
-    cells = interior_cells(cfg)
+    cells = interior_cells(cfg)  # the whole domain
+    # on N GPUs the domain is split into N x2 slabs (whole vertical columns),
+    # one per rank, with the ghost exchange after every stage and the MIN
+    # all-reduce of dt: the total work is fixed
+    decomposed = world > 1 and args.decomp == "slab"
+    if decomposed:
+        from snapy_linfel_b200.config import BC
+        from snapy_linfel_b200.layout import SlabBlock, SlabLayout
+
+        if cfg.nx2 < 2 or cfg.nx2 % world:
+            raise SystemExit(f"{args.workload}: {cfg.nx2} x2 cells do not split into {world} slabs")
+        lay = SlabLayout(world, 1, periodic_x=cfg.bc[2] == BC["periodic"])
+        slab = SlabBlock(opts, lay, rank, device=f"cuda:{local}")
+        slab.initialize(w, r)
+        mb = slab.block
+        stepper = slab.step
+        args.no_fp32 = True     # the exchange moves the FP64 state
+        args.no_adjoint = True
+    else:
+        mb = MeshBlock(opts, device=f"cuda:{local}")
+        mb.initialize(w, r)
+        stepper = mb.step
+    mult = 1 if decomposed else world  # replicas multiply the work
     stream = torch.cuda.current_stream()
 
     def barrier():
@@ -844,13 +982,13 @@ def run_ours(args):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         for _ in range(args.warmup):
-            mb.step()
+            stepper()
         barrier()
         _lib.timing_enable(True)
         clk.mark_start()
         ev0.record(stream)
         for _ in range(args.steps):
-            mb.step()
+            stepper()
         ev1.record(stream)
         barrier()
         clk.mark_end()
@@ -861,7 +999,7 @@ def run_ours(args):
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_max = t.item()
-    value = world * cells * 3 * args.steps / (ms_max / 1e3) / 1e6
+    value = mult * cells * 3 * args.steps / (ms_max / 1e3) / 1e6
 
     # ---- end to end through the public API with host buffers ----
     hu = torch.empty(cfg.shape, dtype=torch.float64).pin_memory()
@@ -879,7 +1017,7 @@ def run_ours(args):
         mb.hydro_u.copy_(hu, non_blocking=True)
         if hs is not None:
             mb.scalar_s.copy_(hs, non_blocking=True)
-        mb.step()
+        stepper()
         hu.copy_(mb.hydro_u, non_blocking=True)
         if hs is not None:
             hs.copy_(mb.scalar_s, non_blocking=True)
@@ -888,13 +1026,14 @@ def run_ours(args):
     t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e = world * cells * 3 * args.steps / (t.item() / 1e3) / 1e6
+    e2e = mult * cells * 3 * args.steps / (t.item() / 1e3) / 1e6
 
     # ---- roofline of the dominant kernel (live CUDA-event durations) ----
     peak, peak_src = measured_peaks()
-    roof64 = dominant_roofline(kern, cfg, cells, 8, peak, peak_src)
+    local_cells = interior_cells(mb.cfg)
+    roof64 = dominant_roofline(kern, cfg, local_cells, 8, peak, peak_src)
     stage_s = ms_max / 1e3 / (3 * args.steps)
-    stage_bw = algo_bytes_per_cell_update(cfg) * cells / stage_s / 1e9
+    stage_bw = algo_bytes_per_cell_update(cfg) * local_cells / stage_s / 1e9
     kern_ms = {k: round(v[0] / v[1], 4) for k, v in kern.items()}
     roof = roof64
 
@@ -916,16 +1055,7 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        try:
-            from oracle.pyoracle import lib_path
-
-            kind = "reference" if os.path.exists(lib_path("reference")) else "port"
-            v, per_step, cores, sample, _ = cpu_sample_run(kind, 1, 0,
-                                                           workload_name=args.workload)
-            cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
-        except Exception as e:  # the baseline is reported, never required
-            cpu = {"value": None, "unit": UNIT, "cores": None, "kind": None,
-                   "sample": f"failed: {e}"}
+        cpu = cpu_baseline_block(args.workload)
 
     if rank == 0:
         forms = {"fp64_plain": {"value": value, "ms_per_step": ms_max / args.steps}}
@@ -951,13 +1081,15 @@ def run_ours(args):
         line = {
             "metric": METRIC, "value": head_value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": head_ms, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": head_ms, "higher_is_better": True,
+            "scaling": "strong" if decomposed else "weak",
             "vs_baseline": None, "dtype": head_dtype, "data": "synthetic",
             "forms": forms,
             "config": {"workload": desc, "form": head_form,
                        "cells_per_gpu": cells, "rk_stages_per_step": 3,
                        "l2_policy": "inputs larger than L2 (state > 126 MB)",
-                       "parallelism": f"replicas x{world}"},
+                       "parallelism": (f"x2 slabs x{world} (ghost exchange per stage)"
+                                       if decomposed else f"replicas x{world}")},
             "roofline": roof,
             "stage_roofline_fp64": {"achieved": stage_bw, "peak": peak, "unit": "GB/s",
                                     "frac": stage_bw / peak,
@@ -984,10 +1116,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c3")
+    ap.add_argument("--decomp", default="slab", choices=["slab", "replicas"],
+                    help="single-domain workloads on N > 1 GPUs: x2 slabs with the ghost "
+                         "exchange (total work fixed) or independent replicas")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--acc-steps", type=int, default=100)
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-single-domain", action="store_true",
+                    help="skip the 384 x 384 x 192 FP32/FP64 comparison of the ensemble line")
     ap.add_argument("--tuning", default="",
                     help="fixed ensemble tile shapes instead of the autotuner, "
                          "e.g. x1_columns=8,march_segment=16,vic_block=32,vic_regs=0")

@@ -224,6 +224,23 @@ int snapb_scale_dt(const double* dt_in, double cfl, int redo, double* dt_out,
 int snapb_check_positive(const snapb_hydro_config* cfg, const double* u,
                          int* flags, void* stream);
 
+/* ---- slab domain decomposition: ghost-zone messages ----
+ * A slab is `width` consecutive indices along x2 (axis 2) or x3 (axis 3) of
+ * var[nv, nc3, nc2, nc1], from `start`, with the full extent of the other
+ * axes.  snapb_pack_slab copies it into buf in the row-major order of
+ * var[:, slab] ([nv][nc3][width][nc1] or [nv][width][nc2][nc1]);
+ * snapb_unpack_slab writes such a buffer into a slab.  The exchange of a
+ * decomposed block packs the ng interior layers next to each internal face
+ * into a send buffer in the sender's memory, moves it as one message and
+ * unpacks it into the receiver's ghost layers.  Replaces the face copies of
+ * LayoutImpl's exchange (src/layout/layout.cpp:361-634). */
+int snapb_pack_slab(const snapb_hydro_config* cfg, int axis, int start,
+                    int width, const double* var, int nv, double* buf,
+                    void* stream);
+int snapb_unpack_slab(const snapb_hydro_config* cfg, int axis, int start,
+                      int width, double* var, int nv, const double* buf,
+                      void* stream);
+
 /* ---- FP32 perturbation form ----
  * The state is stored in FP32 as perturbations about an FP64 reference
  * profile rho_bar(x1), p_bar(x1) (x1 = vertical, [nc1] device arrays, ghosts
@@ -279,9 +296,9 @@ typedef struct snapb_member_f32 {
 } snapb_member_f32;
 
 /* tile shapes; 0 = default.  x1_columns: columns per x1 tile; march_segment:
- * faces per x2/x3 segment; ctas_per_sm: persistent CTAs per SM cap; vic_block:
- * columns per implicit-column tile (32, 64 or 128); vic_regs: register budget
- * of the implicit-column kernel (0 compiler's choice, 1 ~168, 2 128). */
+ * faces per x2/x3 segment; ctas_per_sm: persistent CTAs per SM cap; vic_block
+ * and vic_regs: ignored (the implicit solve runs in fixed tiles of 32
+ * columns; the fields keep the struct layout). */
 typedef struct snapb_ensemble_tuning {
   int32_t x1_columns, march_segment, ctas_per_sm, vic_block, vic_regs;
 } snapb_ensemble_tuning;

@@ -53,6 +53,8 @@ def lib():
         "snapb_max_time_step": (i, [cp, vp, vp, vp, sz, vp]),
         "snapb_scale_dt": (i, [vp, d, i, vp, vp]),
         "snapb_check_positive": (i, [cp, vp, vp, vp]),
+        "snapb_pack_slab": (i, [cp, i, i, i, vp, i, vp, vp]),
+        "snapb_unpack_slab": (i, [cp, i, i, i, vp, i, vp, vp]),
         "snapb_workspace_size_f32": (sz, [cp]),
         "snapb_reference_f32": (i, [cp, vp, vp, vp, sz, vp]),
         "snapb_to_perturbation": (i, [cp, i, vp, vp, vp, sz, vp]),
@@ -93,7 +95,8 @@ def exported_symbols():
             "snapb_prim2cons", "snapb_reconstruct", "snapb_riemann", "snapb_hydro_forward",
             "snapb_implicit_correction", "snapb_implicit_correction_noalloc", "snapb_stage",
             "snapb_bc_apply", "snapb_max_time_step", "snapb_scale_dt",
-            "snapb_check_positive", "snapb_timing_enable", "snapb_timing_query",
+            "snapb_check_positive", "snapb_pack_slab", "snapb_unpack_slab",
+            "snapb_timing_enable", "snapb_timing_query",
             "snapb_workspace_size_f32", "snapb_reference_f32", "snapb_to_perturbation",
             "snapb_from_perturbation", "snapb_stage_f32", "snapb_bc_apply_f32",
             "snapb_max_time_step_f32", "snapb_adjoint_workspace_size", "snapb_stage_adjoint",

@@ -163,6 +163,52 @@ class SlabLayout:
             plans.append((dim, sends, recvs))
         return plans
 
+    # ---- slab buffers: the message format of the exchange ----
+    @staticmethod
+    def pack(cfg: HydroConfig, t, dim: int, sl: slice):
+        """the slab t[:, .., sl, ..] along tensor dim (2: x2, 1: x3) as a
+        contiguous buffer in row-major order; device tensors are packed by the
+        snapb_pack_slab kernel, host tensors (CPU ranks) by a tensor copy of
+        the same layout"""
+        import torch
+
+        shape = list(t.shape)
+        shape[dim] = sl.stop - sl.start
+        if not t.is_cuda:
+            idx = [slice(None)] * 4
+            idx[dim] = sl
+            return t[tuple(idx)].contiguous()
+        if t.dtype != torch.float64 or not t.is_contiguous():
+            raise ValueError("device slabs are packed from contiguous float64 arrays")
+        import ctypes
+
+        from . import _lib
+
+        buf = torch.empty(shape, dtype=t.dtype, device=t.device)
+        _lib.check(_lib.lib().snapb_pack_slab(ctypes.byref(cfg), 2 if dim == 2 else 3, sl.start,
+                                              sl.stop - sl.start, _lib.ptr(t), int(t.shape[0]),
+                                              _lib.ptr(buf), _lib.stream_ptr()),
+                   "snapb_pack_slab")
+        return buf
+
+    @staticmethod
+    def unpack(cfg: HydroConfig, t, dim: int, sl: slice, buf):
+        """write a buffer made by pack() into the slab t[:, .., sl, ..]"""
+        if not t.is_cuda:
+            idx = [slice(None)] * 4
+            idx[dim] = sl
+            t[tuple(idx)].copy_(buf)
+            return
+        import ctypes
+
+        from . import _lib
+
+        _lib.check(_lib.lib().snapb_unpack_slab(ctypes.byref(cfg), 2 if dim == 2 else 3,
+                                                sl.start, sl.stop - sl.start, _lib.ptr(t),
+                                                int(t.shape[0]), _lib.ptr(buf),
+                                                _lib.stream_ptr()),
+                   "snapb_unpack_slab")
+
     def exchange(self, cfg: HydroConfig, rank: int, tensors, group=None):
         """Fill the exchange faces' ghost cells of each [nv, nc3, nc2, nc1]
         tensor (local block, after its local boundary fill) from the
@@ -177,34 +223,29 @@ class SlabLayout:
             return r if group is None else dist.get_global_rank(group, r)
 
         for dim, sends, recvs in self._face_plan(cfg, rank):
-            ops, bufs = [], []
+            ops, keep, unpacks = [], [], []
             for ti, t in enumerate(tensors):
                 for peer, sl, tag in sends:
                     if peer < 0:
                         continue
-                    idx = [slice(None)] * 4
-                    idx[dim] = sl
-                    buf = t[tuple(idx)].contiguous()
-                    bufs.append(buf)
+                    buf = self.pack(cfg, t, dim, sl)
+                    keep.append(buf)
                     ops.append(dist.P2POp(dist.isend, buf, peer_of(peer), group, 4 * ti + tag))
                 for peer, sl, tag in recvs:
                     if peer < 0:
                         continue
-                    idx = [slice(None)] * 4
-                    idx[dim] = sl
                     shape = list(t.shape)
                     shape[dim] = sl.stop - sl.start
                     buf = torch.empty(shape, dtype=t.dtype, device=t.device)
                     ops.append(dist.P2POp(dist.irecv, buf, peer_of(peer), group, 4 * ti + tag))
-                    bufs.append((t, tuple(idx), buf))
+                    unpacks.append((t, sl, buf))
             if not ops:
                 continue
             for req in dist.batch_isend_irecv(ops):
                 req.wait()
-            for b in bufs:
-                if isinstance(b, tuple):
-                    t, idx, buf = b
-                    t[idx].copy_(buf)
+            for t, sl, buf in unpacks:
+                self.unpack(cfg, t, dim, sl, buf)
+            del keep
 
     def exchange_local(self, cfg: HydroConfig, fields_by_rank):
         """The same exchange between blocks held by one process (a list, per
@@ -222,12 +263,10 @@ class SlabLayout:
                     _, psends, _ = plans[peer][a]
                     ssl = next(sl for q, sl, tg in psends if q == r and tg == tag)
                     for t_dst, t_src in zip(fields_by_rank[r], fields_by_rank[peer]):
-                        src = [slice(None)] * 4
-                        dst = [slice(None)] * 4
-                        src[dim], dst[dim] = ssl, rsl
-                        moves.append((t_dst, tuple(dst), t_src[tuple(src)].clone()))
-            for t, idx, val in moves:
-                t[idx].copy_(val)
+                        # the message the sender would post, unpacked by the receiver
+                        moves.append((t_dst, dim, rsl, self.pack(cfg, t_src, dim, ssl)))
+            for t, dim, sl, buf in moves:
+                self.unpack(cfg, t, dim, sl, buf)
 
     @staticmethod
     def min_dt(dt, group=None):

@@ -25,12 +25,70 @@ from . import _lib
 from .config import CONSERVED, PRIMITIVE, RIEMANN, HydroConfig, MeshBlockOptions
 
 
-def _cfg(options) -> HydroConfig:
+def _block_cfg(block) -> HydroConfig:
+    """the configuration (geometry, boundaries, scalars) of a parent block"""
+    if isinstance(block, HydroConfig):
+        return block
+    if isinstance(block, MeshBlockOptions):
+        return block.hydro
+    if hasattr(block, "cfg") and isinstance(block.cfg, HydroConfig):  # a MeshBlock
+        return block.cfg
+    raise TypeError("block: a MeshBlock, MeshBlockOptions or HydroConfig")
+
+
+def _cfg(options, block=None) -> HydroConfig:
+    """options: MeshBlockOptions / HydroConfig, or the snapy options classes
+    (HydroOptions; the geometry then comes from `block`, as the reference's
+    modules take their coordinates from the parent mesh block)"""
+    from .options import CoordinateOptions, HydroOptions, InterpOptions
+
     if isinstance(options, MeshBlockOptions):
         return options.hydro
     if isinstance(options, HydroConfig):
         return options
-    raise TypeError("options: MeshBlockOptions or HydroConfig")
+    if isinstance(options, HydroOptions):
+        if block is None:
+            raise TypeError("HydroOptions need a block for the geometry")
+        b = _block_cfg(block)
+        coord = CoordinateOptions(nx1=b.nx1, nx2=b.nx2, nx3=b.nx3, nghost=b.nghost,
+                                  x1min=b.x1min, x1max=b.x1max, x2min=b.x2min,
+                                  x2max=b.x2max, x3min=b.x3min, x3max=b.x3max)
+        from .config import BC, RECON
+
+        names = {v: k for k, v in BC.items()}
+        rnames = {v: k for k, v in RECON.items()}
+        return options.config(coord, bc=tuple(names[int(x)] for x in b.bc), nscalar=b.nscalar,
+                              scalar_recon=InterpOptions(rnames[b.scalar_recon_type])
+                              .scale(bool(b.scalar_recon_scale)))
+    from .config import RECON, RGAS
+    from .options import (EquationOfStateOptions, ImplicitOptions, ReconstructOptions,
+                          RiemannSolverOptions)
+
+    if isinstance(options, (ReconstructOptions, RiemannSolverOptions, ImplicitOptions,
+                            EquationOfStateOptions)):
+        # one module's options on the parent block's configuration
+        if block is None:
+            raise TypeError(f"{type(options).__name__} need a block for the geometry")
+        c = _block_cfg(block).copy()
+        if isinstance(options, ReconstructOptions):
+            it = options.interp() or InterpOptions()
+            c.recon1_type = c.recon23_type = RECON[it.type()]
+            c.recon1_shock = c.recon23_shock = int(bool(options.shock()))
+            c.recon1_scale = c.recon23_scale = int(bool(it.scale()))
+        elif isinstance(options, RiemannSolverOptions):
+            if options.type() not in ("roe", "lmars", "hllc"):
+                raise ValueError(f"unsupported hydro riemann solver {options.type()!r}")
+            c.riemann = RIEMANN[options.type()]
+        elif isinstance(options, ImplicitOptions):
+            options.type()  # rejects unsupported schemes
+            c.implicit_scheme = int(options.scheme())
+        else:
+            if options.type() != "ideal-gas":
+                raise ValueError(f"equation of state {options.type()!r} is not on this path")
+            c.gammad = float(options.gammad())
+            c.rgas = RGAS / float(options.weight())
+        return c
+    raise TypeError("options: the snapy options classes, MeshBlockOptions or HydroConfig")
 
 
 def _cuda64(*ts):
@@ -52,8 +110,9 @@ def _dt_tensor(dt, device):
 
 
 class _Module:
-    def __init__(self, options):
-        self.cfg = _cfg(options)
+    def __init__(self, options, block=None):
+        self.cfg = _cfg(options, block)
+        self.options = options
         self.lib = _lib.lib()
 
     def __call__(self, *args, **kw):
@@ -66,8 +125,8 @@ class _Module:
 class Hydro(_Module):
     """the stage tendency du = -dt div F + forcing (+ implicit correction)"""
 
-    def __init__(self, options):
-        super().__init__(options)
+    def __init__(self, options, block=None):
+        super().__init__(options, block)
         self._ws = None
 
     def _workspace(self, device):
@@ -111,8 +170,8 @@ class Hydro(_Module):
 class Reconstruct(_Module):
     """interface states along one axis; group 0 = hydro, 1 = scalars"""
 
-    def __init__(self, options, group: int = 0):
-        super().__init__(options)
+    def __init__(self, options, block=None, group: int = 0):
+        super().__init__(options, block)
         self.group = group
 
     def forward(self, w, dim: int):
@@ -133,8 +192,10 @@ class RiemannSolver(_Module):
     """face fluxes of a hydro solver ('roe', 'lmars', 'hllc'; default the
     configuration's)"""
 
-    def __init__(self, options, solver: str | None = None):
-        super().__init__(options)
+    def __init__(self, options, block=None, solver: str | None = None):
+        if isinstance(block, str):  # RiemannSolver(options, "hllc")
+            block, solver = None, block
+        super().__init__(options, block)
         self.solver = RIEMANN[solver] if solver is not None else int(self.cfg.riemann)
 
     def forward(self, wl, wr, dim: int, flx, face_pressure=None):
@@ -149,8 +210,8 @@ class RiemannSolver(_Module):
 class ImplicitHydro(_Module):
     """vertically implicit correction of a stage tendency"""
 
-    def __init__(self, options):
-        super().__init__(options)
+    def __init__(self, options, block=None):
+        super().__init__(options, block)
         self._ws = None
 
     def forward(self, du, w, dt, mass_corr=None):
