@@ -80,3 +80,42 @@ def test_bundle_and_single(tmp_path):
     single = restart.combine(d, "solo", 0, final=True)
     assert os.path.basename(single) == "solo.final.restart" and not restart.is_bundle(single)
     assert torch.equal(restart.load_restart(single, 0)["hydro_w"], vs[0]["hydro_w"])
+
+
+def _ref_fixture():
+    import sys
+
+    here = os.path.join(os.path.dirname(__file__), "golden")
+    sys.path.insert(0, here)
+    try:
+        import make_restart_fixture as m
+    finally:
+        sys.path.remove(here)
+    return os.path.join(here, "ref_restart.block0.00003.part"), m.fixture_tensors()
+
+
+def test_reads_a_part_written_by_the_reference(tmp_path):
+    """a restart part written by the reference's own save_tensors
+    (python/write_init.py:12-22) is read back exactly, as a single part and
+    from a bundle, and restores like one written here"""
+    path, want = _ref_fixture()
+    back = restart.load_restart(path, 0)
+    assert set(back) == set(want)
+    for k, v in want.items():
+        assert back[k].dtype == v.dtype and torch.equal(back[k], v), k
+    # bundled with two parts written here, it is found by its block rank
+    d = str(tmp_path)
+    import shutil
+
+    shutil.copy(path, os.path.join(d, "ref.block0.00003.part"))
+    for r in (1, 2):
+        restart.write_part(_vars(20 + r), d, "ref", rank=r, file_number=3, current_time=1.0,
+                           cycle=2)
+    out = restart.combine(d, "ref", 3)
+    got = restart.load_restart(out, 0)
+    assert torch.equal(got["hydro_u"], want["hydro_u"]) and int(got["last_cycle"][0]) == 77
+    # the same variables written here give the same buffers
+    mine = str(tmp_path / "mine.part")
+    restart.save_tensors(want, mine)
+    again = restart.load_tensors(mine)
+    assert all(torch.equal(again[k], want[k]) for k in want)
