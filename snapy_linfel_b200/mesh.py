@@ -174,6 +174,21 @@ class MeshBlock:
         return restart.write_part(v, output_dir, basename, rank, file_number, current_time,
                                   self.cycle, final, output_file_numbers, output_next_times)
 
+    def write_netcdf(self, output_dir, basename, file_number, current_time, file_id="out1",
+                     variables=("prim",), rank=0, block_loc=(0, 0, 0), blocks=(1, 1, 1)):
+        """this block's NetCDF output (NetcdfOutput::write_output_file,
+        src/output/netcdf.cpp:34-508; snapy_linfel_b200/netcdf.py), the
+        scalars written as mixing ratios with 'prim' and densities with
+        'cons'"""
+        from . import netcdf
+
+        sc = None
+        if self.cfg.nscalar:
+            sc = self.scalar_s if "cons" in variables else self.scalar_r
+        return netcdf.write_block(self.cfg, self.hydro_w, self.hydro_u, output_dir, basename,
+                                  file_number, current_time, file_id, variables, rank,
+                                  block_loc, blocks, sc)
+
     def restore(self, variables):
         """state from restart variables (restart.load_restart): hydro_u,
         hydro_w and scalar_s as stored (hydro_w derived from hydro_u when the
