@@ -172,12 +172,6 @@ __device__ __forceinline__ void x1_32_tile(const Geo& g, const Phys& p, const St
   const float gm1 = (float)(p.gammad - 1.);
   const float gamma = (float)p.gammad;
 
-  // U' -> W' of every cell of the tile's columns.  With gravity the x1 ghost
-  // cells take the isentropic revision on full values, in FP64, computed by
-  // the ghost cell's own thread from the edge cell's state: the recurrence
-  // p_{n+1} = (p_n^a + c)^(1/a) has h_n = p_n^a = p_e^a + n c, so every ghost
-  // level is independent of the others.
-  const bool revise = p.grav1 != 0.;
   for (int idx = tid; idx < C * nc1; idx += nt) {
     int c = idx / nc1, i = idx - c * nc1;
     int64_t col = col0 + c;
@@ -187,26 +181,6 @@ __device__ __forceinline__ void x1_32_tile(const Geo& g, const Phys& p, const St
 #pragma unroll
     for (int v = 0; v < 5; ++v) uc[v] = b.u[v * sv + off];
     cons2prim_pert(uc, wc, b.rbf[i], gm1);
-    if (revise && (i < g.il || i > g.iu)) {
-      const int top = i > g.iu;
-      const int e = top ? g.iu : g.il;
-      const int n = top ? i - g.iu - 1 : g.il - i - 1;
-      float ue[5], we[5];
-#pragma unroll
-      for (int v = 0; v < 5; ++v) ue[v] = b.u[v * sv + col * nc1 + e];
-      cons2prim_pert(ue, we, b.rbf[e], gm1);
-      const double gam = p.gammad;
-      const double a = (gam - 1.) / gam, ig = 1. / gam, ia = 1. / a;
-      const double grav = -p.grav1, dz = g.dx1;
-      const double ps = b.pb[e] + we[IPR], rs = b.rb[e] + we[IDN];
-      const double K = ps / pow(rs, gam), kg = pow(K, ig);
-      const double step = (top ? -a : a) * grav * dz / kg;
-      const double h = pow(ps, a) + (n + 1) * step;
-      const double pn = pow(h, ia);
-      const double rn = pow(pn / K, ig);
-      wc[IPR] = (float)(pn - b.pb[i]);
-      wc[IDN] = (float)(rn - b.rb[i]);
-    }
 #pragma unroll
     for (int v = 0; v < 5; ++v) sw[(c * NV + v) * nc1 + i] = wc[v];
 #pragma unroll
@@ -214,6 +188,32 @@ __device__ __forceinline__ void x1_32_tile(const Geo& g, const Phys& p, const St
       float rr = b.s[n * sv + off] / (b.rbf[i] + uc[IDN]);
       sw[(c * NV + 5 + n) * nc1 + i] = rr;
       b.R[n * sv + off] = rr;
+    }
+  }
+  __syncthreads();
+
+  // isentropic x1 ghost revision on full values, in FP64.  The recurrence
+  // p_{n+1} = (p_n^a + c)^(1/a) has h_n = p_n^a = p_e^a + n c, so every ghost
+  // level is independent: one thread per (column, end, level)
+  if (p.grav1 != 0. && tid < 2 * g.ng * C) {
+    const int c = tid / (2 * g.ng), rest = tid - c * 2 * g.ng;
+    const int top = rest / g.ng, n = rest - top * g.ng;
+    if (col0 + c < ncol) {
+      float* pp = sw + (c * NV + IPR) * nc1;
+      float* rr = sw + (c * NV + IDN) * nc1;
+      const double gam = p.gammad;
+      const double a = (gam - 1.) / gam, ig = 1. / gam, ia = 1. / a;
+      const double grav = -p.grav1, dz = g.dx1;
+      const int e = top ? g.iu : g.il, dir = top ? 1 : -1;
+      const double ps = b.pb[e] + pp[e], rs = b.rb[e] + rr[e];
+      const double K = ps / pow(rs, gam), kg = pow(K, ig);
+      const double step = (top ? -a : a) * grav * dz / kg;
+      const double h = pow(ps, a) + (n + 1) * step;
+      const double pn = pow(h, ia);
+      const double rn = pow(pn / K, ig);
+      const int cell = e + dir * (n + 1);  // ghosts only; the edge cell is never written
+      pp[cell] = (float)(pn - b.pb[cell]);
+      rr[cell] = (float)(rn - b.rb[cell]);
     }
   }
   __syncthreads();
@@ -352,7 +352,9 @@ __device__ __forceinline__ void march32_line(const Geo& g, const Phys& p, const 
   const float rref = b.rbf[i], pref = b.pbf[i];
   const float gamma = (float)p.gammad;
 
-  float q[NV][6];
+  // six-cell window of the face's stencil plus one cell loaded a face ahead
+  // (slot 6), so a load's latency overlaps the previous face's arithmetic
+  float q[NV][7];
   auto load = [&](int cell, int slot) {
     cell = min(max(cell, 0), ncax - 1);
     int64_t off = base + cell * st;
@@ -362,11 +364,19 @@ __device__ __forceinline__ void march32_line(const Geo& g, const Phys& p, const 
     for (int n = 0; n < NS; ++n) q[5 + n][slot] = b.R[n * sv + off];
   };
 #pragma unroll
-  for (int t = 0; t < 5; ++t) load(f0 - 3 + t, t);
+  for (int t = 0; t < 6; ++t) load(f0 - 3 + t, t);
 
   float Fp[NV];
   for (int f = f0; f <= f1; ++f) {
-    load(f + 2, 5);
+    load(f + 3, 6);
+    // the running sums of the cell this face closes, fetched before the
+    // face's arithmetic
+    float dprev[NV];
+    if (f > f0 && !first) {
+      const int64_t off = base + (int64_t)(f - 1) * st;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) dprev[v] = b.D[v * sv + off];
+    }
     float L[NV], R[NV], F[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
@@ -398,7 +408,7 @@ __device__ __forceinline__ void march32_line(const Geo& g, const Phys& p, const 
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
         d[v] = A * F[v] - A * Fp[v];
-        if (!first) d[v] = b.D[v * sv + off] + d[v];
+        if (!first) d[v] = dprev[v] + d[v];
       }
       if (last) {
         float wc[5];
@@ -414,7 +424,7 @@ __device__ __forceinline__ void march32_line(const Geo& g, const Phys& p, const 
     for (int v = 0; v < NV; ++v) {
       Fp[v] = F[v];
 #pragma unroll
-      for (int t = 0; t < 5; ++t) q[v][t] = q[v][t + 1];
+      for (int t = 0; t < 6; ++t) q[v][t] = q[v][t + 1];
     }
   }
 }
