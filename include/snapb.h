@@ -296,9 +296,11 @@ typedef struct snapb_member_f32 {
 } snapb_member_f32;
 
 /* tile shapes; 0 = default.  x1_columns: columns per x1 tile; march_segment:
- * faces per x2/x3 segment; ctas_per_sm: persistent CTAs per SM cap; vic_block
- * and vic_regs: ignored (the implicit solve runs in fixed tiles of 32
- * columns; the fields keep the struct layout). */
+ * faces per x2/x3 segment; ctas_per_sm: persistent CTAs per SM cap; vic_block:
+ * columns per implicit-column tile (32, 64 or 128); vic_regs: variant of the
+ * implicit solve (0 column kernel with the compiler's register budget, 1
+ * ~168, 2 128; 3 the fused kernel: blocks, twisted elimination from both
+ * column ends, back substitution and finish in one launch). */
 typedef struct snapb_ensemble_tuning {
   int32_t x1_columns, march_segment, ctas_per_sm, vic_block, vic_regs;
 } snapb_ensemble_tuning;

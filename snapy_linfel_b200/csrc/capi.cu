@@ -57,7 +57,7 @@ const char* check_config(const snapb_hydro_config* c) {
 }
 
 struct Layout {
-  size_t D, RG, DD, R, M, VIC, SLOTS, DT, total;
+  size_t D, RG, DD, R, M, VIC, VICT, SLOTS, DT, total;
 };
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -81,6 +81,8 @@ Layout ws_layout(const snapb_hydro_config& c) {
   o = align256(o + (c.implicit_scheme ? sv : 0));
   L.VIC = o;
   o = align256(o + vic_scratch_bytes(g, p));
+  L.VICT = o;
+  o = align256(o + vic_blocks_bytes(g, p));
   L.SLOTS = o;
   o = align256(o + 8 * sizeof(double));
   L.DT = o;
@@ -148,6 +150,7 @@ int run_stage(const snapb_hydro_config* c, int stage, const double* dt, double* 
   b.R = at<double>(ws, L.R);
   b.M = p.implicit_scheme ? at<double>(ws, L.M) : nullptr;
   b.vic = at<double>(ws, L.VIC);
+  b.vicT = vic_blocks_bytes(g, p) ? at<double>(ws, L.VICT) : nullptr;
   b.stage = stage;
   rk3_weights(stage, b.wgt0, b.wgt1, b.wgt2);
   b.write_du = (mode == 1 || p.implicit_scheme != 0) ? 1 : 0;
@@ -331,6 +334,7 @@ int snapb_implicit_correction(const snapb_hydro_config* cfg, const double* dt, d
   b.D = du;
   b.M = mass_corr;
   b.vic = at<double>(workspace, L.VIC);
+  b.vicT = vic_blocks_bytes(g, p) ? at<double>(workspace, L.VICT) : nullptr;
   b.vic_du_only = 1;
   cudaStream_t st = (cudaStream_t)stream;
   KernelTimer t(SNAPB_K_VIC, st);

@@ -99,7 +99,12 @@ __global__ void k_fill_u64(unsigned long long* p, int n, unsigned long long v) {
 // ---------------------------------------------------------------------------
 // host plan
 // ---------------------------------------------------------------------------
-enum Phase { PH_X1 = 0, PH_X2, PH_X3, PH_VIC, PH_BCU, PH_BCS, PH_CFL, PH_COUNT };
+enum Phase {
+  PH_X1 = 0, PH_X2, PH_X3, PH_VCOL, PH_VFIN, PH_VFUSED, PH_BCU, PH_BCS, PH_CFL, PH_COUNT
+};
+
+// vic_regs value of the tuning that selects the fused implicit-solve kernel
+constexpr int kVicFusedVariant = 3;
 
 struct snapb_ensemble {
   std::vector<snapb_member_f32> in;
@@ -169,12 +174,18 @@ int plan(snapb_ensemble* e) {
     mb.seglen3 = seg;
     mb.nseg3 = (g.nx3 + seg - 1) / seg;
     int64_t ncolv = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
-    mb.vic_cols = vic_tile_columns();
+    mb.vic_cols = t.vic_block > 0 ? t.vic_block : 64;
     int64_t tiles[PH_COUNT] = {0};
     tiles[PH_X1] = e->a1 ? (ncol1 + C - 1) / C : 0;
     tiles[PH_X2] = e->a2 ? ((lines2 + 127) / 128) * mb.nseg2 : 0;
     tiles[PH_X3] = e->a3 ? ((lines3 + 127) / 128) * mb.nseg3 : 0;
-    tiles[PH_VIC] = e->p.implicit_scheme ? (ncolv + mb.vic_cols - 1) / mb.vic_cols : 0;
+    tiles[PH_VCOL] = e->p.implicit_scheme ? (ncolv + mb.vic_cols - 1) / mb.vic_cols : 0;
+    const int fl = vic_finish_layers32(e->p.nscalar);
+    tiles[PH_VFIN] = e->p.implicit_scheme
+                         ? ((ncolv + kVicFinishCols - 1) / kVicFinishCols) * ((g.nx1 + fl - 1) / fl)
+                         : 0;
+    const int fc = vicf_tile_columns();
+    tiles[PH_VFUSED] = e->p.implicit_scheme ? (ncolv + fc - 1) / fc : 0;
     // ghost-shell cells, 256 per tile (same count as bc_shell_slots)
     const int64_t nj = g.ju - g.jl + 1, nk = g.ku - g.kl + 1;
     const int64_t shell = (g.nc1 > 1 ? nj * nk * 2 * g.ng : 0) +
@@ -394,7 +405,15 @@ int snapb_ensemble_stage_f32(snapb_ensemble* e, int stage, void* stream) {
   }
   if (p.implicit_scheme) {
     ScopedTimer t(SNAPB_K_VIC, st);
-    c = launch_vic_batch(mem, p, queue(e, PH_VIC), stage, pgrid(e, PH_VIC), st);
+    if (e->tune.vic_regs == kVicFusedVariant) {
+      c = launch_vicf_batch(mem, p, queue(e, PH_VFUSED), stage, pgrid(e, PH_VFUSED), st);
+    } else {
+      int blk = e->mem.empty() ? 64 : e->mem[0].vic_cols;
+      c = launch_vic_column_batch(mem, p, queue(e, PH_VCOL), stage, pgrid(e, PH_VCOL), blk,
+                                  e->tune.vic_regs, st);
+      if (c == cudaSuccess)
+        c = launch_vic_finish_batch(mem, p, queue(e, PH_VFIN), stage, pgrid(e, PH_VFIN), st);
+    }
     if (c != cudaSuccess) return cuda_e(c, "ensemble implicit");
   }
   {

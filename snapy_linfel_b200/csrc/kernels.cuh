@@ -27,6 +27,7 @@ struct StageBufs {
   double* R;         // [nscalar][sv] scalar mixing ratio of the stage input
   double* M;         // [nvar][sv] implicit mass correction (IDN row used)
   double* vic;       // implicit-solve scratch
+  double* vicT;      // per-layer |A| and J blocks (split column sweep), or null
   int stage;
   double wgt0, wgt1, wgt2;
   int write_du;      // 1: finalize writes du into D instead of updating u
@@ -78,7 +79,7 @@ struct Member32 {
   int x1_cols;           // columns per x1 tile
   int seglen2, nseg2;    // x2 march: faces per segment, segments
   int seglen3, nseg3;    // x3 march
-  int vic_cols;          // columns per implicit-solve tile
+  int vic_cols;          // columns per implicit-column tile
   int pad;
 };
 
@@ -168,14 +169,22 @@ cudaError_t launch_x1_32_batch(const Member32* mem, const Phys& p, const WorkQue
 cudaError_t launch_march32_batch(int axis, const Member32* mem, const Phys& p,
                                  const WorkQueue& q, int stage, bool first, bool last,
                                  const PersistGrid& pg, cudaStream_t st);
-cudaError_t launch_vic_batch(const Member32* mem, const Phys& p, const WorkQueue& q, int stage,
-                             const PersistGrid& pg, cudaStream_t st);
-int vic_tile_columns();  // columns per implicit-solve tile
+cudaError_t launch_vic_column_batch(const Member32* mem, const Phys& p, const WorkQueue& q,
+                                    int stage, const PersistGrid& pg, int block, int variant,
+                                    cudaStream_t st);
+cudaError_t launch_vic_finish_batch(const Member32* mem, const Phys& p, const WorkQueue& q,
+                                    int stage, const PersistGrid& pg, cudaStream_t st);
+// the fused implicit-solve kernel (vicf.cu): one launch per solve, tiles of
+// vicf_tile_columns() columns
+cudaError_t launch_vicf_batch(const Member32* mem, const Phys& p, const WorkQueue& q, int stage,
+                              const PersistGrid& pg, cudaStream_t st);
+int vicf_tile_columns();
 cudaError_t launch_bc32_batch(const Member32* mem, const Phys& p, const WorkQueue& q, int kind,
                               double igm1, const PersistGrid& pg, cudaStream_t st);
 size_t x1_smem32_per_column(const Geo& g, int nvt);
 StageBufs32 bufs32_of(const snapb_hydro_config& c, void* ws);
 size_t workspace_size_f32_of(const snapb_hydro_config& c);
+constexpr int kVicFinishCols = 32;    // columns per implicit-finish tile
 
 // RK3 (Shu-Osher) stage weights: u = wgt0*u0 + wgt1*u + wgt2*du
 inline void rk3_weights(int stage, double& a, double& b, double& c) {
@@ -197,6 +206,13 @@ cudaError_t launch_diffusion(const Geo& g, const Phys& p, const StageBufs& b, cu
 cudaError_t launch_vic(const Geo& g, const Phys& p, const StageBufs& b, cudaStream_t st);
 cudaError_t launch_vic32(const Geo& g, const Phys& p, const StageBufs32& b, cudaStream_t st);
 size_t vic_scratch_bytes(const Geo& g, const Phys& p);
+size_t vic_column_scratch_bytes(const Geo& g, const Phys& p);
+size_t vicf_scratch_bytes(const Geo& g, const Phys& p);
+cudaError_t launch_vic_column(const Geo& g, const Phys& p, const StageBufs& b, cudaStream_t st);
+cudaError_t launch_vicf(const Geo& g, const Phys& p, const StageBufs& b, cudaStream_t st);
+cudaError_t launch_vicf32(const Geo& g, const Phys& p, const StageBufs32& b, cudaStream_t st);
+size_t vic_blocks_bytes(const Geo& g, const Phys& p);
+int vic_finish_layers32(int nscalar);  // layers per implicit-finish tile, FP32 form
 
 cudaError_t launch_cons2prim(const Geo& g, const Phys& p, const double* u, double* w,
                              cudaStream_t st);

@@ -1,30 +1,20 @@
-// vic.cu — vertically implicit correction (VIC) of one RK stage.
+// vic.cu — vertically implicit correction (VIC) of one RK stage, FP64.
 //
-// One kernel per solve: k_vic, one CTA per tile of 32 x1 columns (x1 is the
-// vertical axis; a tile's column index sits on the lanes), or its persistent
-// batched form k_vic_batch over the tiles of many ensemble members.  Per tile:
-//   (1) producer warps form the blocks of each layer from the state — a_i,
-//       b_i, c_i and the right-hand side du_i / dt, with the Roe-averaged
-//       |A| = R |Lambda| R^-1 at the layer's two faces and the flux
-//       Jacobians J of the cells below and above — into a double-buffered
-//       ring of chunks in shared memory;
-//   (2) two elimination warps work the block-tridiagonal system from both
-//       ends at once (a twisted block factorisation): warp 0 eliminates
-//       upwards from the bottom layer, as the reference's forward sweep
-//       does, warp 1 downwards from the top layer; at the middle layer
-//       m = nl / 2 the two reduced systems meet and that layer is solved
-//       first.  Each chain is half as long as one sweep over the column;
-//   (3) both warps back-substitute outwards from the middle layer and
-//       accumulate the MS-VIC column sums;
-//   (4) the whole CTA applies the mass redistribution, the scalar mass fix
-//       and the RK combination (or leaves du) to the tile's cells, its
-//       inputs staged through shared memory by cp.async.
-// (1) and (2) overlap: the producers fill chunk c+1 while the elimination
-// warps consume chunk c, with one CTA barrier per chunk (no other
-// synchronisation).  The reduced blocks and partial solutions (N*N + N
-// doubles per cell) are written by (2) and read back by (3) inside the same
-// CTA a short time later, so with a few tiles in flight per SM they are
-// served by L2 rather than HBM.  Every elimination step is FP64.
+// Two kernels per solve:
+//   k_vic_column    one thread per x1 column (x1 is the vertical axis): the
+//                   blocks are formed on the fly while the column is swept —
+//                   the Roe-averaged |A| = R |Lambda| R^-1 once per interface
+//                   (the reference forms it twice, once per neighbouring cell)
+//                   and the flux Jacobian once per cell, a layer ahead of the
+//                   elimination that consumes them — then the block-Thomas
+//                   elimination, back substitution and the MS-VIC column
+//                   sums.  Only the reduced blocks and the partial solutions
+//                   go through HBM;
+//   k_vic_finish    per cell: mass redistribution, scalar mass fix and the RK
+//                   combination (or du), with delta transposed through shared
+//                   memory.
+// Every workspace array is laid out with the column index fastest, so the
+// sequential sweep's loads and stores are coalesced across a warp's columns.
 //
 // Reference: ImplicitHydroImpl::forward (src/implicit/implicit_hydro.cpp:99-189),
 // vic_assemble_partial_impl (src/implicit/vic_assemble_partial_impl.h:29-111),
@@ -33,8 +23,7 @@
 // (src/math/ludcmp.h:24-76, src/math/lubksb.h:124-147),
 // vic_backward_reduce / vic_redistribute_cell (src/implicit/vic_redistribute_impl.h:26-106),
 // flux Jacobian and Roe eigenvectors (src/implicit/flux_decomposition_impl.h:133-245).
-// The reference eliminates each column bottom-up only; the twisted order
-// gives the same solution up to rounding.
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <type_traits>
@@ -47,66 +36,74 @@
 
 namespace snapb {
 
+// ---------------------------------------------------------------------------
+// Scratch layout (doubles, column index fastest so that the threads of a warp,
+// one column each, read consecutive addresses):
+//   S [nl][N*N+N][ncol]  the reduced blocks a'_i then the partial solutions
+//                        delta_i (back-substituted in place)
+//   Z [2][ncol]          per-column sums: sum (rho V)^2 and B_dry
+// ---------------------------------------------------------------------------
+template <int N>
+struct VicDims {
+  static constexpr int ES = N * N + N;
+};
+
 static inline int vic_n(const Phys& p) { return ((p.implicit_scheme >> 3) & 1) ? 5 : 3; }
 
-// Tile shape and shared-memory plan of the fused kernel for N x N blocks.
-template <int N>
-struct VicCfg {
-  static constexpr int TC = 32;               // columns per tile (lane = column)
-  static constexpr int K = N == 3 ? 2 : 1;    // layers per chunk at each end
-  static constexpr int PW = N == 3 ? 2 : 1;   // producer warps per end
-  static constexpr int NT = (2 + 2 * PW) * 32;
-  static constexpr int NN = N * N;
-  static constexpr int RE = 3 * NN + N;       // ring entry: a, b, c, rhs
-  static constexpr int ES = NN + N;           // scratch record: reduced block, partial solution
-  static constexpr int BD = N == 3 ? 4 : 2;   // back-substitution prefetch depth (layers)
-  static constexpr int BE = ES + 2;           // back ring entry: record, du[IDN], w[IDN]
-  static constexpr size_t ring_bytes = (size_t)2 * 2 * K * RE * TC * sizeof(double);
-  static constexpr size_t back_bytes = (size_t)2 * BD * BE * 32 * sizeof(double);
-  // fixed area after the shared region: the top chain's last reduced block and
-  // partial solution [ES][TC], the middle solution [N][TC], the column sums
-  // [4][TC] and the column offsets [TC] (int64)
-  static constexpr size_t fixed_bytes = ((size_t)(ES + N + 4) * TC + TC) * sizeof(double);
-};
-
-// Finish staging: per sub-tile of TL layers, the solution rows [N][TC][TL+1]
-// (doubles) and the cell inputs [elem][TC][TL] in the stored precision T:
-// w[IDN], the du rows the solve does not replace, u, u0, and per scalar s,
-// s0, r and its du row.
-template <int N, int NS, class T>
-struct VicFin {
-  static constexpr int TC = VicCfg<N>::TC;
-  static constexpr int DR = N == 3 ? 3 : 1;   // du rows read: IDN (+ IVY, IVZ)
-  static constexpr int elems = 1 + DR + 10 + 4 * NS;
-  static constexpr size_t bytes_for(int tl) {
-    return (size_t)N * TC * (tl + 1) * sizeof(double) + (size_t)elems * TC * tl * sizeof(T);
-  }
-  static constexpr int TL = bytes_for(16) <= 64 * 1024 ? 16 : 8;
-  static constexpr size_t bytes = bytes_for(TL);
-};
-
-template <class B>
-using StoredT = std::remove_pointer_t<decltype(std::declval<B>().u)>;
-
-template <int N, int NS, class T>
-constexpr size_t vic_smem_bytes() {
-  using C = VicCfg<N>;
-  size_t r = C::ring_bytes;
-  if (C::back_bytes > r) r = C::back_bytes;
-  if (VicFin<N, NS, T>::bytes > r) r = VicFin<N, NS, T>::bytes;
-  r = (r + 15) & ~(size_t)15;
-  return r + C::fixed_bytes;
-}
-
-// Scratch: per tile of TC columns, [nl][N*N+N][TC] doubles (column fastest,
-// so a warp's stores and loads of one element are one 256-byte line).
-size_t vic_scratch_bytes(const Geo& g, const Phys& p) {
+size_t vic_column_scratch_bytes(const Geo& g, const Phys& p) {
   if (p.implicit_scheme == 0) return 0;
-  const int N = vic_n(p);
-  const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
-  const int64_t tiles = (ncol + 31) / 32;
-  return (size_t)(tiles * 32 * (int64_t)g.nx1 * (N * N + N)) * sizeof(double);
+  int N = vic_n(p);
+  int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
+  int64_t nl = g.nx1;
+  int64_t es = N * N + N;
+  return (size_t)(nl * es * ncol + 2 * ncol) * sizeof(double);
 }
+
+// workspace share of the implicit solve: room for either variant (the column
+// + finish pair here, or the fused kernel of vicf.cu)
+size_t vic_scratch_bytes(const Geo& g, const Phys& p) {
+  const size_t a = vic_column_scratch_bytes(g, p), b = vicf_scratch_bytes(g, p);
+  return a > b ? a : b;
+}
+
+// Few columns (2-D domains, thin 3-D ones) leave most of the GPU idle with one
+// thread per column: the blocks |A| (per face) and J (per cell) are then
+// formed by a fully parallel kernel first, so the sequential sweep only
+// eliminates.  Scratch T [nl+2][2 N*N][ncol]: index t holds |A| of the face
+// between cells t-1 and t, and J of cell t-1.
+constexpr int64_t kSplitMaxCols = 8192;
+
+bool vic_split(const Geo& g, const Phys& p) {
+  const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
+  return p.implicit_scheme != 0 && ncol <= kSplitMaxCols;
+}
+
+size_t vic_blocks_bytes(const Geo& g, const Phys& p) {
+  if (!vic_split(g, p)) return 0;
+  int N = vic_n(p);
+  int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
+  return (size_t)((int64_t)(g.nx1 + 2) * 2 * N * N * ncol) * sizeof(double);
+}
+
+constexpr int kTC = 32;  // columns per tile
+
+// Back substitution: the reduced block, partial solution and du[IDN] of a
+// layer are fetched kBackDepth<N> layers ahead into a per-thread ring in
+// shared memory by asynchronous copies (cp.async), so the short recurrence
+// does not wait a memory latency per layer and holds no extra registers.
+// Ring layout [slot][element][thread] (element ES = du[IDN]), doubles.
+constexpr int kFwdDepth = 4;  // layers of the forward sweep in flight
+
+template <int N>
+struct BackRing {
+  static constexpr int depth = N == 3 ? 4 : 2;
+  static constexpr int elems = N * N + N + 1;
+};
+template <int N>
+constexpr size_t back_ring_bytes(int threads) {
+  return (size_t)threads * BackRing<N>::depth * BackRing<N>::elems * sizeof(double);
+}
+
 
 // (k, j, il) offset of interior column `col`
 __device__ __forceinline__ int64_t column_base(const Geo& g, int64_t col) {
@@ -216,44 +213,19 @@ __device__ __forceinline__ void jac_of(const StageBufs32&, double gm1, const dou
     for (int q = 0; q < N; ++q) J[r][q] = (double)F[r][q];
 }
 
-// ---------------------------------------------------------------------------
-// (1) the blocks of layer i of one column (cb: the column's (k, j, il)
-// offset), written to out[e * TC], e = a (N*N), b (N*N), c (N*N), rhs (N):
-//   a_i = (|A|_{i-1/2} + |A|_{i+1/2}) A / (2V) - Phi + I / dt,
-//   b_i = -(|A|_{i-1/2} + J_{i-1}) A / (2V),  c_i = -(|A|_{i+1/2} - J_{i+1}) A / (2V),
-// with the reflecting-wall fix a += b diag(1,-1,1,..) at the bottom layer and
-// a += c diag(..) at the top one, rhs = du_i / dt
-// (vic_assemble_partial_impl.h:29-111, forward_sweep_impl.h:31-47).
-// ---------------------------------------------------------------------------
-template <int N, class B>
-__device__ __forceinline__ void vic_layer_blocks(const Geo& g, const Phys& p, const B& b,
-                                                 int64_t cb, int i, int nl, double dt,
-                                                 double* out) {
-  constexpr int NN = N * N, TC = VicCfg<N>::TC;
-  const int64_t sv = g.sv;
-  const double gm1c = p.gammad - 1.;
-  const double gm1f = 0.5 * (p.gammad + p.gammad) - 1.;
-  const double Aa = g.A1, hiv = 0.5 / g.vol, idt = 1. / dt, grav = p.grav1;
-  double wm[5], wc[5], wp[5];
-#pragma unroll
-  for (int v = 0; v < 5; ++v) {
-    wm[v] = vic_w(b, sv, v, cb + i - 1, g.il + i - 1);
-    wc[v] = vic_w(b, sv, v, cb + i, g.il + i);
-    wp[v] = vic_w(b, sv, v, cb + i + 1, g.il + i + 1);
-  }
-  double Am[N][N], Ap[N][N], J[N][N], bb[N][N], cc[N][N];
-  absA_of<N>(b, gm1f, wm, wc, Am);
-  jac_of<N>(b, gm1c, wm, J);
-#pragma unroll
-  for (int r = 0; r < N; ++r)
-#pragma unroll
-    for (int q = 0; q < N; ++q) bb[r][q] = -(Am[r][q] + J[r][q]) * Aa * hiv;
-  absA_of<N>(b, gm1f, wc, wp, Ap);
-  jac_of<N>(b, gm1c, wp, J);
-#pragma unroll
-  for (int r = 0; r < N; ++r)
-#pragma unroll
-    for (int q = 0; q < N; ++q) cc[r][q] = -(Ap[r][q] - J[r][q]) * Aa * hiv;
+// One layer of the block-Thomas forward elimination: a_i, b_i, c_i from |A|
+// at the layer's lower / upper faces (Am, Ap) and J of the cells below /
+// above (Jp, Jn); the previous reduced block and partial solution (ap, dp)
+// are eliminated, and c (reduced block) and rhs (partial solution) return the
+// new ones.  Used by the split sweep; the fused sweep (vic_column) spells out
+// the same arithmetic inline.
+template <int N, class BT>
+__device__ __forceinline__ void vic_layer(const BT (&Am)[N][N], const BT (&Ap)[N][N],
+                                          const BT (&Jp)[N][N], const BT (&Jn)[N][N],
+                                          const double (&ap)[N][N], const double (&dp)[N],
+                                          double (&rhs)[N], double (&c)[N][N], int i, int nl,
+                                          double Aa, double hiv, double idt, double grav) {
+  double a[N][N], bb[N][N];
 #pragma unroll
   for (int r = 0; r < N; ++r)
 #pragma unroll
@@ -262,72 +234,490 @@ __device__ __forceinline__ void vic_layer_blocks(const Geo& g, const Phys& p, co
       if (r == 1 && q == 0) phi = grav;
       if (N == 3 && r == 2 && q == 1) phi = grav;
       if (N == 5 && r == IPR && q == IVX) phi = grav;
-      double a = (Am[r][q] * Aa + Ap[r][q] * Aa) * hiv - phi;
-      if (r == q) a += idt;
-      if (i == 0) a += bb[r][q] * (q == 1 ? -1. : 1.);
-      if (i == nl - 1) a += cc[r][q] * (q == 1 ? -1. : 1.);
-      out[(r * N + q) * TC] = a;
-      out[(NN + r * N + q) * TC] = bb[r][q];
-      out[(2 * NN + r * N + q) * TC] = cc[r][q];
+      a[r][q] = (Am[r][q] * Aa + Ap[r][q] * Aa) * hiv - phi;
+      bb[r][q] = -(Am[r][q] + Jp[r][q]) * Aa * hiv;
+      c[r][q] = -(Ap[r][q] - Jn[r][q]) * Aa * hiv;
     }
 #pragma unroll
-  for (int r = 0; r < N; ++r) out[(3 * NN + r) * TC] = vic_d(b, sel<N>(r) * sv + cb + i) / dt;
+  for (int r = 0; r < N; ++r) a[r][r] += idt;
+  if (i == 0) {
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+      for (int q = 0; q < N; ++q) a[r][q] += bb[r][q] * (q == 1 ? -1. : 1.);
+  }
+  if (i == nl - 1) {
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+      for (int q = 0; q < N; ++q) a[r][q] += c[r][q] * (q == 1 ? -1. : 1.);
+  }
+  if (i > 0) {
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      double bd = 0.;
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        double t = 0.;
+#pragma unroll
+        for (int kk = 0; kk < N; ++kk) t += bb[r][kk] * ap[kk][q];
+        a[r][q] -= t;
+        bd += bb[r][q] * dp[q];
+      }
+      rhs[r] = rhs[r] - bd;
+    }
+  }
+  block_solve<N>(a, c, rhs);
 }
 
-// X -= L Y (N x N) and y -= L z (N) with L, Y, z in registers
-template <int N>
-__device__ __forceinline__ void vic_eliminate(double (&X)[N][N], double (&y)[N],
-                                              const double (&L)[N][N], const double (&Y)[N][N],
-                                              const double (&z)[N]) {
+// Back substitution delta_i -= a'_i delta_{i+1} and the MS-VIC column sums
+// (sum (rho V)^2 from the forward sweep, B_dry accumulated here); the inputs
+// of each layer arrive through the thread's shared-memory ring.
+template <int N, class B>
+__device__ __forceinline__ void vic_back(const B& b, double* S, double* Z, int64_t ncol,
+                                         int64_t sv, int64_t cb, int nl, const double (&dp)[N],
+                                         double sum_a2, double V) {
+  constexpr int ES = VicDims<N>::ES;
+  constexpr int DB = BackRing<N>::depth, RE = BackRing<N>::elems;
+  extern __shared__ double vic_ring[];
+  const int nt = blockDim.x, lane = threadIdx.x;
+  auto Sat = [&](int i, int e) -> double& { return S[((int64_t)i * ES + e) * ncol]; };
+  cp_async_wait<0>();  // the forward ring is drained before its memory is reused
+  auto ring = [&](int slot, int e) { return vic_ring + ((size_t)(slot * RE + e) * nt + lane); };
+  auto fetch = [&](int i, int slot) {
+    if (i >= 0) {
 #pragma unroll
-  for (int r = 0; r < N; ++r) {
-    double bd = 0.;
+      for (int e = 0; e < ES; ++e) cp_async_bytes8(ring(slot, e), &Sat(i, e));
+      cp_async_elem(ring(slot, ES), b.D + IDN * sv + cb + i);
+    }
+    cp_async_commit();
+  };
+  double dn[N];
 #pragma unroll
-    for (int q = 0; q < N; ++q) {
+  for (int r = 0; r < N; ++r) dn[r] = dp[r];
+  double b_dry = (vic_d(b, IDN * sv + cb + nl - 1) - dn[0]) * 1. * V;
+#pragma unroll
+  for (int k = 0; k < DB; ++k) fetch(nl - 2 - k, k);
+  for (int i = nl - 2, slot = 0; i >= 0; --i) {
+    cp_async_wait<DB - 1>();  // the group of layer i has landed
+    double cur[ES];
+#pragma unroll
+    for (int e = 0; e < ES; ++e) cur[e] = *ring(slot, e);
+    const double dcur = ring_elem(ring(slot, ES), b.D);
+    double d[N];
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
       double t = 0.;
 #pragma unroll
-      for (int kk = 0; kk < N; ++kk) t += L[r][kk] * Y[kk][q];
-      X[r][q] -= t;
-      bd += L[r][q] * z[q];
+      for (int q = 0; q < N; ++q) t += cur[r * N + q] * dn[q];
+      d[r] = cur[N * N + r] - t;
     }
-    y[r] = y[r] - bd;
+    b_dry += (dcur - d[0]) * 1. * V;
+    fetch(i - DB, slot);  // the slot's values are consumed: refill it
+    slot = slot + 1 == DB ? 0 : slot + 1;
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      dn[r] = d[r];
+      Sat(i, N * N + r) = d[r];
+    }
+  }
+  cp_async_wait<0>();
+  Z[0] = sum_a2;
+  Z[ncol] = b_dry;
+}
+
+// (1) one thread per column: blocks formed a layer ahead of the
+// block-Thomas elimination, back substitution and the column sums.  Loads of
+// a layer's w and du go 32 columns apart across a warp; the next layers of
+// each column sit in the same 32-byte sectors, which stay in L1.
+template <int N, class B>
+__device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B& b, int64_t col) {
+  constexpr int ES = VicDims<N>::ES;
+  const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
+  if (col >= ncol) return;
+  const int nl = g.nx1;
+  const int64_t sv = g.sv;
+  const int64_t cb = column_base(g, col);
+  double* S = b.vic + col;
+  double* Z = S + (int64_t)nl * ES * ncol;
+  auto Sat = [&](int i, int e) -> double& { return S[((int64_t)i * ES + e) * ncol]; };
+  auto load_w = [&](int i, double* w) {
+#pragma unroll
+    for (int v = 0; v < 5; ++v) w[v] = vic_w(b, sv, v, cb + i, g.il + i);
+  };
+  const double gm1c = p.gammad - 1.;
+  const double gm1f = 0.5 * (p.gammad + p.gammad) - 1.;
+  const double dt = *b.dt;
+  const double Aa = g.A1, hiv = 0.5 / g.vol, idt = 1. / dt, grav = p.grav1, V = g.vol;
+  // Forward sweep inputs (w of cell L and the rows of du at layer L-1,
+  // 1 <= L <= nl) arrive kFwdDepth layers ahead through the same per-thread
+  // shared-memory ring as the back substitution, layout [slot][element][thread].
+  constexpr int DF = kFwdDepth, FE = 5 + N;
+  static_assert(DF * FE <= BackRing<N>::depth * BackRing<N>::elems, "ring too small");
+  extern __shared__ double vic_ring[];
+  const int nt = blockDim.x, lane = threadIdx.x;
+  auto fring = [&](int slot, int e) { return vic_ring + ((size_t)(slot * FE + e) * nt + lane); };
+  auto ffetch = [&](int L, int slot) {
+    if (L <= nl) {
+#pragma unroll
+      for (int v = 0; v < 5; ++v) cp_async_elem(fring(slot, v), b.w + v * sv + cb + L);
+#pragma unroll
+      for (int r = 0; r < N; ++r)
+        cp_async_elem(fring(slot, 5 + r), b.D + sel<N>(r) * sv + cb + L - 1);
+    }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int k = 0; k < DF; ++k) ffetch(1 + k, k);
+  double wc[5], wn[5];
+  double Am[N][N], Jp[N][N], Jc[N][N], ap[N][N], dp[N];
+  load_w(-1, wn);
+  jac_of<N>(b, gm1c, wn, Jp);
+  load_w(0, wc);
+  absA_of<N>(b, gm1f, wn, wc, Am);
+  jac_of<N>(b, gm1c, wc, Jc);
+  double sum_a2 = 0.;
+  for (int i = 0, fslot = 0; i < nl; ++i) {
+    double Ap[N][N], Jn[N][N], rhs[N];
+    cp_async_wait<DF - 1>();  // the group of cell i+1 has landed
+#pragma unroll
+    for (int v = 0; v < 5; ++v)  // cell i+1 (the ghost cell nl at the top)
+      wn[v] = vic_full(b, ring_elem(fring(fslot, v), b.w), v, g.il + i + 1);
+#pragma unroll
+    for (int r = 0; r < N; ++r) rhs[r] = ring_elem(fring(fslot, 5 + r), b.D) / dt;
+    absA_of<N>(b, gm1f, wc, wn, Ap);
+    jac_of<N>(b, gm1c, wn, Jn);
+    double ai = wc[IDN] * V;
+    sum_a2 += ai * ai;
+    double a[N][N], bb[N][N], c[N][N];
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        double phi = 0.;
+        if (r == 1 && q == 0) phi = grav;
+        if (N == 3 && r == 2 && q == 1) phi = grav;
+        if (N == 5 && r == IPR && q == IVX) phi = grav;
+        a[r][q] = (Am[r][q] * Aa + Ap[r][q] * Aa) * hiv - phi;
+        bb[r][q] = -(Am[r][q] + Jp[r][q]) * Aa * hiv;
+        c[r][q] = -(Ap[r][q] - Jn[r][q]) * Aa * hiv;
+      }
+#pragma unroll
+    for (int r = 0; r < N; ++r) a[r][r] += idt;
+    if (i == 0) {
+#pragma unroll
+      for (int r = 0; r < N; ++r)
+#pragma unroll
+        for (int q = 0; q < N; ++q) a[r][q] += bb[r][q] * (q == 1 ? -1. : 1.);
+    }
+    if (i == nl - 1) {
+#pragma unroll
+      for (int r = 0; r < N; ++r)
+#pragma unroll
+        for (int q = 0; q < N; ++q) a[r][q] += c[r][q] * (q == 1 ? -1. : 1.);
+    }
+    if (i > 0) {
+#pragma unroll
+      for (int r = 0; r < N; ++r) {
+        double bd = 0.;
+#pragma unroll
+        for (int q = 0; q < N; ++q) {
+          double t = 0.;
+#pragma unroll
+          for (int kk = 0; kk < N; ++kk) t += bb[r][kk] * ap[kk][q];
+          a[r][q] -= t;
+          bd += bb[r][q] * dp[q];
+        }
+        rhs[r] = rhs[r] - bd;
+      }
+    }
+    block_solve<N>(a, c, rhs);
+    // the slot's values are consumed (the solve depends on them): refill it
+    ffetch(i + 1 + DF, fslot);
+    fslot = fslot + 1 == DF ? 0 : fslot + 1;
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      dp[r] = rhs[r];
+      __stcs(&Sat(i, N * N + r), rhs[r]);
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        ap[r][q] = c[r][q];
+        __stcs(&Sat(i, r * N + q), c[r][q]);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        Am[r][q] = Ap[r][q];
+        Jp[r][q] = Jc[r][q];
+        Jc[r][q] = Jn[r][q];
+      }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) wc[v] = wn[v];
+  }
+  // back substitution: delta_i -= a'_i delta_{i+1}; B_dry accumulated on the
+  // way, the inputs of each layer arriving through the shared-memory ring.
+  constexpr int DB = BackRing<N>::depth, RE = BackRing<N>::elems;
+  cp_async_wait<0>();  // the forward ring is drained before its memory is reused
+  auto ring = [&](int slot, int e) { return vic_ring + ((size_t)(slot * RE + e) * nt + lane); };
+  auto fetch = [&](int i, int slot) {
+    if (i >= 0) {
+#pragma unroll
+      for (int e = 0; e < ES; ++e) cp_async_bytes8(ring(slot, e), &Sat(i, e));
+      cp_async_elem(ring(slot, ES), b.D + IDN * sv + cb + i);
+    }
+    cp_async_commit();
+  };
+  double dn[N];
+#pragma unroll
+  for (int r = 0; r < N; ++r) dn[r] = dp[r];
+  double b_dry = (vic_d(b, IDN * sv + cb + nl - 1) - dn[0]) * 1. * V;
+#pragma unroll
+  for (int k = 0; k < DB; ++k) fetch(nl - 2 - k, k);
+  for (int i = nl - 2, slot = 0; i >= 0; --i) {
+    cp_async_wait<DB - 1>();  // the group of layer i has landed
+    double cur[ES];
+#pragma unroll
+    for (int e = 0; e < ES; ++e) cur[e] = *ring(slot, e);
+    const double dcur = ring_elem(ring(slot, ES), b.D);
+    double d[N];
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      double t = 0.;
+#pragma unroll
+      for (int q = 0; q < N; ++q) t += cur[r * N + q] * dn[q];
+      d[r] = cur[N * N + r] - t;
+    }
+    b_dry += (dcur - d[0]) * 1. * V;
+    fetch(i - DB, slot);  // the slot's values are consumed: refill it
+    slot = slot + 1 == DB ? 0 : slot + 1;
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      dn[r] = d[r];
+      Sat(i, N * N + r) = d[r];
+    }
+  }
+  cp_async_wait<0>();
+  Z[0] = sum_a2;
+  Z[ncol] = b_dry;
+}
+
+// ---- split sweep (few columns): blocks first, then the elimination ----
+template <int N>
+struct PreRing {
+  static constexpr int elems = 2 * N * N + N + 1;  // A_{i+1}, J_{i+2}, du rows, rho
+};
+template <int N>
+constexpr size_t pre_ring_bytes(int threads) {
+  return (size_t)threads * sizeof(double) *
+         (kFwdDepth * PreRing<N>::elems > BackRing<N>::depth * BackRing<N>::elems
+              ? kFwdDepth * PreRing<N>::elems
+              : BackRing<N>::depth * BackRing<N>::elems);
+}
+
+// one thread per (column, t), t in [0, nl+1], column fastest (coalesced stores)
+template <int N>
+__global__ void __launch_bounds__(256) k_vic_blocks(Geo g, Phys p, StageBufs b) {
+  constexpr int NN = N * N;
+  const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
+  const int nl = g.nx1;
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= ncol * (nl + 2)) return;
+  const int64_t col = idx - (int64_t)udiv(idx, ncol) * ncol;
+  const int t = udiv(idx, ncol);
+  const int64_t sv = g.sv, cb = column_base(g, col);
+  const double gm1c = p.gammad - 1.;
+  const double gm1f = 0.5 * (p.gammad + p.gammad) - 1.;
+  double wl[5], wr[5];
+#pragma unroll
+  for (int v = 0; v < 5; ++v) wl[v] = b.w[v * sv + cb + t - 1];
+  double* out = b.vicT + (int64_t)t * 2 * NN * ncol + col;
+  double J[N][N];
+  jac_of<N>(b, gm1c, wl, J);
+#pragma unroll
+  for (int r = 0; r < N; ++r)
+#pragma unroll
+    for (int q = 0; q < N; ++q) out[(NN + r * N + q) * ncol] = J[r][q];
+  if (t <= nl) {
+#pragma unroll
+    for (int v = 0; v < 5; ++v) wr[v] = b.w[v * sv + cb + t];
+    double A[N][N];
+    absA_of<N>(b, gm1f, wl, wr, A);
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+      for (int q = 0; q < N; ++q) out[(r * N + q) * ncol] = A[r][q];
   }
 }
 
-// ---------------------------------------------------------------------------
-// (4) finish of layers [i0, i0 + TL) of the tile: redistribution, scalar mass
-// fix, RK combination (or du), all inputs of the sub-tile fetched by cp.async
-// first (the solution rows along columns, the cell values along x1).
-// ---------------------------------------------------------------------------
-template <int N, int NS, class B>
-__device__ __forceinline__ void vic_finish_subtile(const Geo& g, const B& b, const double* S,
-                                                   const double* zs, const int64_t* cbs,
-                                                   int64_t col0, int64_t ncol, int i0,
-                                                   double* sm) {
-  using C = VicCfg<N>;
-  using F = VicFin<N, NS, StoredT<B>>;
-  using T = StoredT<B>;
-  constexpr int TC = C::TC, ES = C::ES, NN = C::NN, TL = F::TL, DR = F::DR;
+// the elimination of one column from the precomputed blocks
+template <int N>
+__global__ void __launch_bounds__(128) k_vic_column_pre(Geo g, Phys p, StageBufs b) {
+  constexpr int ES = VicDims<N>::ES, NN = N * N, DF = kFwdDepth, FE = PreRing<N>::elems;
+  const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
+  const int64_t col = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= ncol) return;
   const int nl = g.nx1;
   const int64_t sv = g.sv;
-  double* dl = sm;                                             // [N][TC][TL+1]
-  T* cell = reinterpret_cast<T*>(dl + (size_t)N * TC * (TL + 1));  // [elem][TC][TL]
-  auto DL = [&](int r, int c, int s) -> double& { return dl[((size_t)r * TC + c) * (TL + 1) + s]; };
-  auto CE = [&](int e, int c, int s) -> T* { return cell + ((size_t)e * TC + c) * TL + s; };
+  const int64_t cb = column_base(g, col);
+  double* S = b.vic + col;
+  double* Z = S + (int64_t)nl * ES * ncol;
+  auto Sat = [&](int i, int e) -> double& { return S[((int64_t)i * ES + e) * ncol]; };
+  const double* T = b.vicT + col;
+  auto Tat = [&](int t, int e) { return T + ((int64_t)t * 2 * NN + e) * ncol; };
+  extern __shared__ double vic_ring[];
+  const int nt = blockDim.x, lane = threadIdx.x;
+  auto fring = [&](int slot, int e) { return vic_ring + ((size_t)(slot * FE + e) * nt + lane); };
+  auto ffetch = [&](int i, int slot) {  // layer i: A_{i+1}, J_{i+2}, du rows and rho of cell i
+    if (i < nl) {
+#pragma unroll
+      for (int e = 0; e < NN; ++e) cp_async_bytes8(fring(slot, e), Tat(i + 1, e));
+#pragma unroll
+      for (int e = 0; e < NN; ++e) cp_async_bytes8(fring(slot, NN + e), Tat(i + 2, NN + e));
+#pragma unroll
+      for (int r = 0; r < N; ++r)
+        cp_async_bytes8(fring(slot, 2 * NN + r), b.D + sel<N>(r) * sv + cb + i);
+      cp_async_bytes8(fring(slot, 2 * NN + N), b.w + IDN * sv + cb + i);
+    }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int k = 0; k < DF; ++k) ffetch(k, k);
+  const double dt = *b.dt;
+  const double Aa = g.A1, hiv = 0.5 / g.vol, idt = 1. / dt, grav = p.grav1, V = g.vol;
+  double Am[N][N], Jp[N][N], Jc[N][N], ap[N][N], dp[N];
+#pragma unroll
+  for (int r = 0; r < N; ++r)
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+      Am[r][q] = *Tat(0, r * N + q);
+      Jp[r][q] = *Tat(0, NN + r * N + q);
+      Jc[r][q] = *Tat(1, NN + r * N + q);
+      ap[r][q] = 0.;
+    }
+#pragma unroll
+  for (int r = 0; r < N; ++r) dp[r] = 0.;
+  double sum_a2 = 0.;
+  for (int i = 0, fslot = 0; i < nl; ++i) {
+    double Ap[N][N], Jn[N][N], rhs[N];
+    cp_async_wait<DF - 1>();  // the group of layer i has landed
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      rhs[r] = *fring(fslot, 2 * NN + r) / dt;
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        Ap[r][q] = *fring(fslot, r * N + q);
+        Jn[r][q] = *fring(fslot, NN + r * N + q);
+      }
+    }
+    const double ai = *fring(fslot, 2 * NN + N) * V;
+    sum_a2 += ai * ai;
+    double c[N][N];
+    vic_layer<N>(Am, Ap, Jp, Jn, ap, dp, rhs, c, i, nl, Aa, hiv, idt, grav);
+    ffetch(i + DF, fslot);  // the slot's values are consumed: refill it
+    fslot = fslot + 1 == DF ? 0 : fslot + 1;
+#pragma unroll
+    for (int r = 0; r < N; ++r) {
+      dp[r] = rhs[r];
+      __stcs(&Sat(i, NN + r), rhs[r]);
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        ap[r][q] = c[r][q];
+        __stcs(&Sat(i, r * N + q), c[r][q]);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        Am[r][q] = Ap[r][q];
+        Jp[r][q] = Jc[r][q];
+        Jc[r][q] = Jn[r][q];
+      }
+  }
+  vic_back<N>(b, S, Z, ncol, sv, cb, nl, dp, sum_a2, V);
+}
+
+// the ring of a 128-thread CTA exceeds the default 48 KB of dynamic shared
+// memory (raise_smem_limit, kernels.cuh)
+template <class K>
+static void allow_ring_smem(K kernel, size_t bytes) {
+  raise_smem_limit(kernel, bytes);
+}
+
+template <int N, class B>
+__global__ void __launch_bounds__(128) k_vic_column(Geo g, Phys p, B b) {
+  vic_column<N, B>(g, p, b, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// (3) redistribution + RK combination (or du), tiles of 32 columns x 32
+// layers: delta is transposed through shared memory so that the state
+// arrays are read and written along x1.
+// one tile: columns col0 .. col0+kTC-1, layers i0 .. i0+kTL-1 (whole CTA)
+// Shared memory of one finish tile: the back-substituted solution rows
+// [N][kTC][kTL+1] (doubles), the column sums and offsets, then the tile's cell
+// inputs [element][kTC][kTL] in the stored precision T: w'[IDN], the du rows
+// the solve does not replace, and (RK update) u, u0, and per scalar s, s0, r
+// and its du row.
+template <int N, int NS>
+struct FinSmem {
+  static constexpr int TL = 16;  // layers per staged tile
+  static constexpr int du_rows = N == 3 ? 3 : 1;           // IDN (+ IVY, IVZ)
+  static constexpr int elems = 1 + du_rows + 10 + 4 * NS;  // upper bound
+  static constexpr size_t head = ((size_t)N * kTC * (TL + 1) + 3 * kTC) * sizeof(double);
+};
+template <int N, int NS, class T>
+constexpr size_t finish_smem_bytes() {
+  return FinSmem<N, NS>::head + (size_t)FinSmem<N, NS>::elems * kTC * FinSmem<N, NS>::TL * sizeof(T);
+}
+
+// One tile: columns col0 .. col0+kTC-1, layers i0 .. i0+kTL-1 (whole CTA).
+// Every input of the tile is fetched with cp.async (coalesced: the solution
+// rows along columns, the cell values along x1) and waited for once, so all
+// of a tile's loads are in flight together without holding registers; the
+// threads then finish the tile's cells from shared memory.
+template <int N, int NS, class B>
+__device__ __forceinline__ void vic_finish_tile_staged(const Geo& g, const Phys& p, const B& b,
+                                                int64_t col0, int i0) {
+  constexpr int ES = VicDims<N>::ES, DR = FinSmem<N, NS>::du_rows, kTL = FinSmem<N, NS>::TL;
+  using T = std::remove_pointer_t<decltype(b.u)>;  // stored precision (FP32 / FP64)
+  const int nl = g.nx1;
+  const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
+  const int64_t sv = g.sv;
+  const double* S = b.vic;
+  const double* Z = S + (int64_t)nl * ES * ncol;
+  extern __shared__ double fin_smem[];
+  double* dl = fin_smem;                                     // [N][kTC][kTL+1]
+  double* zs = dl + (size_t)N * kTC * (kTL + 1);             // [2][kTC]
+  int64_t* cbs = reinterpret_cast<int64_t*>(zs + 2 * kTC);   // [kTC]
+  T* cell = reinterpret_cast<T*>(cbs + kTC);                 // [element][kTC][kTL]
+  auto DL = [&](int r, int c, int s) -> double& {
+    return dl[((size_t)r * kTC + c) * (kTL + 1) + s];
+  };
+  auto CE = [&](int e, int c, int s) -> T* { return cell + ((size_t)e * kTC + c) * kTL + s; };
   const bool du_only = b.vic_du_only, first = b.stage == 0;
+  // element slots; per scalar n: s, s0, r, its du row at eS + 4 n
   const int eRHO = 0, eDU = 1, eU = 1 + DR, eU0 = eU + 5, eS = eU0 + 5;
-  const int tid = threadIdx.x, nt = blockDim.x;
-  for (int idx = tid; idx < N * TC * TL; idx += nt) {
-    const int c = idx % TC, rest = idx / TC;
-    const int s = rest % TL, r = rest / TL;
-    const int i = i0 + s;
-    if (col0 + c < ncol && i < nl)
-      cp_async_bytes8(&DL(r, c, s), S + ((int64_t)i * ES + NN + r) * TC + c);
+  const int tid = threadIdx.x;
+  if (tid < 2 * kTC) {
+    int c = tid % kTC, k = tid / kTC;
+    zs[k * kTC + c] = col0 + c < ncol ? Z[k * ncol + col0 + c] : 1.;
+    if (k == 0) cbs[c] = col0 + c < ncol ? column_base(g, col0 + c) : 0;
+  }
+  __syncthreads();
+  for (int idx = tid; idx < N * kTC * kTL; idx += blockDim.x) {
+    int c = idx % kTC, rest = idx / kTC;
+    int s = rest % kTL, r = rest / kTL;
+    int64_t col = col0 + c;
+    int i = i0 + s;
+    if (col < ncol && i < nl)
+      cp_async_bytes8(&DL(r, c, s), S + ((int64_t)i * ES + N * N + r) * ncol + col);
   }
   const int ne = du_only ? eU : (first ? eU0 : eS);  // u0 is the stage input at stage 0
-  for (int idx = tid; idx < ne * TC * TL; idx += nt) {
-    const int s = idx % TL, rest = idx / TL;
-    const int c = rest % TC, e = rest / TC;
+  for (int idx = tid; idx < ne * kTC * kTL; idx += blockDim.x) {
+    const int s = idx % kTL, rest = idx / kTL;
+    const int c = rest % kTC, e = rest / kTC;
     const int i = i0 + s;
     if (col0 + c >= ncol || i >= nl) continue;
     const int64_t off = cbs[c] + i;
@@ -339,9 +729,9 @@ __device__ __forceinline__ void vic_finish_subtile(const Geo& g, const B& b, con
     cp_async_elem(CE(e, c, s), src);
   }
   if (!du_only) {
-    for (int idx = tid; idx < 4 * NS * TC * TL; idx += nt) {
-      const int s = idx % TL, rest = idx / TL;
-      const int c = rest % TC, q = rest / TC;
+    for (int idx = tid; idx < 4 * NS * kTC * kTL; idx += blockDim.x) {
+      const int s = idx % kTL, rest = idx / kTL;
+      const int c = rest % kTC, q = rest / kTC;
       const int n = q / 4, kind = q % 4;
       const int i = i0 + s;
       if (col0 + c >= ncol || i >= nl || (kind == 1 && first)) continue;
@@ -354,20 +744,18 @@ __device__ __forceinline__ void vic_finish_subtile(const Geo& g, const B& b, con
   cp_async_commit();
   cp_async_wait<0>();
   __syncthreads();
-  for (int idx = tid; idx < TC * TL; idx += nt) {
-    const int s = idx % TL, c = idx / TL;
+  for (int idx = tid; idx < kTC * kTL; idx += blockDim.x) {
+    const int s = idx % kTL, c = idx / kTL;
     const int i = i0 + s;
     if (col0 + c >= ncol || i >= nl) continue;
     const int64_t off = cbs[c] + i;
     const int xi = g.il + i;
-    const double sum_a2 = zs[c] + zs[2 * TC + c];
-    const double b_dry = zs[TC + c] + zs[3 * TC + c];
     const double rhok = vic_full(b, (double)*CE(eRHO, c, s), IDN, xi);
     const double etk = *CE(eDU, c, s);
-    const double ai = rhok * g.vol;
-    const double fix = DL(0, c, s) - etk;
+    double ai = rhok * g.vol;
+    double fix = DL(0, c, s) - etk;
     double du[5];
-    du[IDN] = etk + fix * 1. + rhok * ai * b_dry / sum_a2;
+    du[IDN] = etk + fix * 1. + rhok * ai * zs[kTC + c] / zs[c];
     if constexpr (N == 3) {
       du[IVX] = DL(1, c, s);
       du[IVY] = *CE(eDU + 1, c, s);
@@ -387,8 +775,8 @@ __device__ __forceinline__ void vic_finish_subtile(const Geo& g, const B& b, con
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
       const double uo = *CE(eU + v, c, s), u0o = first ? 0. : (double)*CE(eU0 + v, c, s);
-      const double un = vic_rk_from(b.u, b.u0, v * sv + off, first, uo, u0o, b.wgt0, b.wgt1,
-                                    b.wgt2, du[v]);
+      double un = vic_rk_from(b.u, b.u0, v * sv + off, first, uo, u0o, b.wgt0, b.wgt1, b.wgt2,
+                              du[v]);
       if (v == IDN) unew_rho = vic_full_rho(b, un, xi);
     }
 #pragma unroll
@@ -397,270 +785,234 @@ __device__ __forceinline__ void vic_finish_subtile(const Geo& g, const B& b, con
       const double so = *CE(eS + 4 * n, c, s);
       const double s0o = first ? 0. : (double)*CE(eS + 4 * n + 1, c, s);
       const double ro = *CE(eS + 4 * n + 2, c, s), dso = *CE(eS + 4 * n + 3, c, s);
-      const double ds = dso + fix * ro;
-      const double sn = vic_rk_from(b.s, b.s0, o, first, so, s0o, b.wgt0, b.wgt1, b.wgt2, ds);
+      double ds = dso + fix * ro;
+      double sn = vic_rk_from(b.s, b.s0, o, first, so, s0o, b.wgt0, b.wgt1, b.wgt2, ds);
       b.r[o] = sn / unew_rho;
     }
   }
-  __syncthreads();  // the staging area is refilled by the next sub-tile
 }
 
-// ---------------------------------------------------------------------------
-// One tile: columns [tile * TC, tile * TC + TC) of the block, whole CTA
-// (VicCfg<N>::NT threads).  sm: dynamic shared memory of vic_smem_bytes().
-// ---------------------------------------------------------------------------
-template <int N, int NS, class B>
-__device__ __forceinline__ void vic_tile(const Geo& g, const Phys& p, const B& b, int64_t tile,
-                                         double* sm) {
-  using C = VicCfg<N>;
-  constexpr int TC = C::TC, K = C::K, PW = C::PW, NN = C::NN, RE = C::RE, ES = C::ES;
-  constexpr int BD = C::BD, BE = C::BE;
-  constexpr size_t region = (vic_smem_bytes<N, NS, StoredT<B>>() - C::fixed_bytes) / sizeof(double);
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+// Register variant (scalars, or FP64 state: the staged inputs would not fit
+// in 48 KB of shared memory and would cut the resident CTAs): each thread
+// issues the loads of its cells before any store.
+template <int N, int NS, class B, int NT, int kTL>
+__device__ __forceinline__ void vic_finish_tile_regs(const Geo& g, const Phys& p, const B& b,
+                                                int64_t col0, int i0) {
+  constexpr int ES = VicDims<N>::ES;
   const int nl = g.nx1;
+  const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
   const int64_t sv = g.sv;
-  const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
-  const int64_t col0 = tile * TC;
-  double* S = b.vic + tile * (int64_t)nl * ES * TC;  // this tile's records [nl][ES][TC]
-  double* ring = sm;                                 // [2 buf][2 end][K][RE][TC]
-  double* midb = sm + region;                        // [ES][TC]
-  double* xmid = midb + (size_t)ES * TC;             // [N][TC]
-  double* zs = xmid + (size_t)N * TC;                // [4][TC]: sum_a2, b_dry per chain
-  int64_t* cbs = reinterpret_cast<int64_t*>(zs + 4 * TC);  // [TC]
-  if (tid < TC) cbs[tid] = col0 + tid < ncol ? column_base(g, col0 + tid) : 0;
-  __syncthreads();
-  const int m = nl / 2;                      // middle layer; the bottom end owns 0..m
-  const int nch = (m + 1 + K - 1) / K;       // chunks (the top end has nl-1-m <= m+1 layers)
-  const double dt = *b.dt;
-  const bool colok = col0 + lane < ncol;
-  auto RG = [&](int buf, int end, int k) -> double* {
-    return ring + ((size_t)((buf * 2 + end) * K + k) * RE) * TC + lane;
-  };
-  auto produce = [&](int ch) {
-    const int pw = warp - 2, end = pw / PW, ph = pw % PW;
-    if (!colok) return;
-    const int64_t cb = cbs[lane];
-#pragma unroll
-    for (int k = ph; k < K; k += PW) {
-      const int j = ch * K + k;
-      const int i = end == 0 ? j : nl - 1 - j;
-      if (end == 0 ? (j > m) : (i <= m)) continue;
-      vic_layer_blocks<N, B>(g, p, b, cb, i, nl, dt, RG(ch & 1, end, k));
-    }
-  };
-  // (1) + (2): chunk ch is consumed while chunk ch + 1 is formed
-  double rb[N][N], rd[N];  // last reduced block and partial solution of this chain
-  if (warp >= 2) produce(0);
-  __syncthreads();
-  for (int ch = 0; ch < nch; ++ch) {
-    if (warp < 2) {
-      if (colok) {
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-          const int j = ch * K + k;
-          const int i = warp == 0 ? j : nl - 1 - j;
-          if (warp == 0 ? (i >= m) : (i <= m)) continue;
-          const double* src = RG(ch & 1, warp, k);
-          double a[N][N], bb[N][N], cc[N][N], r[N];
-#pragma unroll
-          for (int x = 0; x < N; ++x) {
-#pragma unroll
-            for (int q = 0; q < N; ++q) {
-              a[x][q] = src[(x * N + q) * TC];
-              bb[x][q] = src[(NN + x * N + q) * TC];
-              cc[x][q] = src[(2 * NN + x * N + q) * TC];
-            }
-            r[x] = src[(3 * NN + x) * TC];
-          }
-          if (warp == 0) {
-            // bottom-up (ForwardSweep): a'_i = (a_i - b_i a'_{i-1})^-1 c_i
-            if (i > 0) vic_eliminate<N>(a, r, bb, rb, rd);
-            block_solve<N>(a, cc, r);
-#pragma unroll
-            for (int x = 0; x < N; ++x)
-#pragma unroll
-              for (int q = 0; q < N; ++q) rb[x][q] = cc[x][q];
-          } else {
-            // top-down: b'_i = (a_i - c_i b'_{i+1})^-1 b_i
-            if (i < nl - 1) vic_eliminate<N>(a, r, cc, rb, rd);
-            block_solve<N>(a, bb, r);
-#pragma unroll
-            for (int x = 0; x < N; ++x)
-#pragma unroll
-              for (int q = 0; q < N; ++q) rb[x][q] = bb[x][q];
-          }
-          double* rec = S + (int64_t)i * ES * TC + lane;
-#pragma unroll
-          for (int x = 0; x < N; ++x) {
-            rd[x] = r[x];
-            rec[(NN + x) * TC] = r[x];
-#pragma unroll
-            for (int q = 0; q < N; ++q) rec[(x * N + q) * TC] = rb[x][q];
-          }
-        }
-      }
-    } else if (ch + 1 < nch) {
-      produce(ch + 1);
-    }
-    __syncthreads();
+  const double* S = b.vic;
+  const double* Z = S + (int64_t)nl * ES * ncol;
+  __shared__ double dl[N][kTC][kTL + 1];
+  __shared__ double zs[2][kTC];
+  __shared__ int64_t cbs[kTC];  // (k, j, il) offsets of the tile's columns
+  const int tid = threadIdx.x;
+  for (int idx = tid; idx < N * kTC * kTL; idx += blockDim.x) {
+    int c = idx % kTC, rest = idx / kTC;
+    int s = rest % kTL, r = rest / kTL;
+    int64_t col = col0 + c;
+    int i = i0 + s;
+    dl[r][c][s] = (col < ncol && i < nl) ? S[((int64_t)i * ES + N * N + r) * ncol + col] : 0.;
   }
-  // the middle layer: its row couples both reduced systems
-  if (warp == 1 && colok && m < nl - 1) {
-#pragma unroll
-    for (int x = 0; x < N; ++x) {
-      midb[(NN + x) * TC + lane] = rd[x];
-#pragma unroll
-      for (int q = 0; q < N; ++q) midb[(x * N + q) * TC + lane] = rb[x][q];
-    }
+  if (tid < 2 * kTC) {
+    int c = tid % kTC, k = tid / kTC;
+    zs[k][c] = col0 + c < ncol ? Z[k * ncol + col0 + c] : 1.;
+    if (k == 0) cbs[c] = col0 + c < ncol ? column_base(g, col0 + c) : 0;
   }
   __syncthreads();
-  if (warp == 0 && colok) {
-    const double* src = RG((m / K) & 1, 0, m % K);  // chunk nch-1, never overwritten
-    double a[N][N], bb[N][N], cc[N][N], r[N], z[N][N];
+  // (2) each thread's kTC kTL / NT cells: every load first (no store in
+  // between, so they are all in flight together), then the arithmetic and
+  // the stores.  Cells are distinct, so the order is the sequential one's.
+  constexpr int IT = kTC * kTL / NT, NSA = NS > 0 ? NS : 1;
+  using T = std::remove_pointer_t<decltype(b.u)>;  // stored precision (FP32 / FP64)
+  T rho[IT], et[IT], dvy[IT], dvz[IT], uo[IT][5], u0o[IT][5];
+  T so[IT][NSA], s0o[IT][NSA], ro[IT][NSA], dso[IT][NSA];
+  int64_t offs[IT];
+  bool ok[IT];
+  const bool du_only = b.vic_du_only, first = b.stage == 0;
 #pragma unroll
-    for (int x = 0; x < N; ++x) {
-#pragma unroll
-      for (int q = 0; q < N; ++q) {
-        a[x][q] = src[(x * N + q) * TC];
-        bb[x][q] = src[(NN + x * N + q) * TC];
-        cc[x][q] = src[(2 * NN + x * N + q) * TC];
-        z[x][q] = 0.;
-      }
-      r[x] = src[(3 * NN + x) * TC];
+  for (int k = 0; k < IT; ++k) {
+    const int idx = tid + k * NT;
+    const int s = idx % kTL, c = idx / kTL;
+    const int64_t col = col0 + c;
+    const int i = i0 + s;
+    ok[k] = col < ncol && i < nl;
+    if (!ok[k]) continue;
+    const int64_t off = cbs[c] + i;
+    offs[k] = off;
+    rho[k] = b.w[IDN * sv + off];
+    et[k] = b.D[IDN * sv + off];
+    if constexpr (N == 3) {
+      dvy[k] = b.D[IVY * sv + off];
+      dvz[k] = b.D[IVZ * sv + off];
     }
-    if (m > 0) vic_eliminate<N>(a, r, bb, rb, rd);
-    if (m < nl - 1) {
-      double tb[N][N], td[N];
+    if (!du_only) {
 #pragma unroll
-      for (int x = 0; x < N; ++x) {
-        td[x] = midb[(NN + x) * TC + lane];
-#pragma unroll
-        for (int q = 0; q < N; ++q) tb[x][q] = midb[(x * N + q) * TC + lane];
+      for (int v = 0; v < 5; ++v) {
+        uo[k][v] = b.u[v * sv + off];
+        if (!first) u0o[k][v] = b.u0[v * sv + off];
       }
-      vic_eliminate<N>(a, r, cc, tb, td);
-    }
-    block_solve<N>(a, z, r);
-    double* rec = S + (int64_t)m * ES * TC + lane;
 #pragma unroll
-    for (int x = 0; x < N; ++x) {
-      rd[x] = r[x];
-      rec[(NN + x) * TC] = r[x];
-      xmid[x * TC + lane] = r[x];
+      for (int n = 0; n < NS; ++n) {
+        const int64_t o = n * sv + off;
+        so[k][n] = b.s[o];
+        if (!first) s0o[k][n] = b.s0[o];
+        ro[k][n] = b.r[o];
+        dso[k][n] = b.D[(5 + n) * sv + off];
+      }
     }
   }
-  __syncthreads();
-  // (3) back substitution outwards from the middle, with the column sums
-  // sum (rho V)^2 and B_dry = sum (du[IDN] - delta_0) V of each chain; each
-  // layer's record, du[IDN] and w[IDN] arrive BD layers ahead through a
-  // per-thread cp.async ring (in the shared region, the chunks being spent)
-  if (warp < 2) {
-    double sa2 = 0., bdry = 0.;
-    if (colok) {
-      const int64_t cb = cbs[lane];
-      const int dir = warp == 0 ? -1 : 1;
-      const int ifirst = warp == 0 ? m : m + 1;
-      const int cnt = warp == 0 ? m + 1 : nl - 1 - m;
-      double* br = sm + (size_t)warp * BD * BE * 32;
-      auto slot_at = [&](int slot, int e) { return br + ((size_t)(slot * BE + e) * 32 + lane); };
-      auto fetch = [&](int t, int slot) {
-        if (t < cnt) {
-          const int i = ifirst + dir * t;
-          const double* rec = S + (int64_t)i * ES * TC + lane;
 #pragma unroll
-          for (int e = 0; e < ES; ++e) cp_async_bytes8(slot_at(slot, e), rec + e * TC);
-          cp_async_elem(slot_at(slot, ES), b.D + IDN * sv + cb + i);
-          cp_async_elem(slot_at(slot, ES + 1), b.w + IDN * sv + cb + i);
-        }
-        cp_async_commit();
-      };
+  for (int k = 0; k < IT; ++k) {
+    if (!ok[k]) continue;
+    const int idx = tid + k * NT;
+    const int s = idx % kTL, c = idx / kTL;
+    const int64_t off = offs[k];
+    const int xi = g.il + i0 + s;
+    const double rhok = vic_full(b, (double)rho[k], IDN, xi), etk = et[k];
+    double ai = rhok * g.vol;
+    double fix = dl[0][c][s] - etk;
+    double du[5];
+    du[IDN] = etk + fix * 1. + rhok * ai * zs[1][c] / zs[0][c];
+    if constexpr (N == 3) {
+      du[IVX] = dl[1][c][s];
+      du[IVY] = dvy[k];
+      du[IVZ] = dvz[k];
+      du[IPR] = dl[2][c][s];
+    } else {
 #pragma unroll
-      for (int t = 0; t < BD; ++t) fetch(t, t);
-      double xp[N];
-#pragma unroll
-      for (int x = 0; x < N; ++x) xp[x] = warp == 0 ? rd[x] : xmid[x * TC + lane];
-      const double V = g.vol;
-      for (int t = 0, slot = 0; t < cnt; ++t) {
-        cp_async_wait<BD - 1>();  // the group of step t has landed
-        const int i = ifirst + dir * t;
-        double cur[ES];
-#pragma unroll
-        for (int e = 0; e < ES; ++e) cur[e] = *slot_at(slot, e);
-        const double du0 = ring_elem(slot_at(slot, ES), b.D);
-        const double rho = vic_full(b, ring_elem(slot_at(slot, ES + 1), b.w), IDN, g.il + i);
-        fetch(t + BD, slot);  // the slot's values are in registers: refill it
-        slot = slot + 1 == BD ? 0 : slot + 1;
-        double x[N];
-        if (warp == 0 && t == 0) {
-#pragma unroll
-          for (int r = 0; r < N; ++r) x[r] = xp[r];  // the middle layer itself
-        } else {
-#pragma unroll
-          for (int r = 0; r < N; ++r) {
-            double s = 0.;
-#pragma unroll
-            for (int q = 0; q < N; ++q) s += cur[r * N + q] * xp[q];
-            x[r] = cur[NN + r] - s;
-          }
-          double* rec = S + (int64_t)i * ES * TC + lane;
-#pragma unroll
-          for (int r = 0; r < N; ++r) rec[(NN + r) * TC] = x[r];
-        }
-        const double ai = rho * V;
-        sa2 += ai * ai;
-        bdry += (du0 - x[0]) * 1. * V;
-#pragma unroll
-        for (int r = 0; r < N; ++r) xp[r] = x[r];
-      }
-      cp_async_wait<0>();
+      for (int v = 1; v < 5; ++v) du[v] = dl[v][c][s];
     }
-    zs[(2 * warp) * TC + lane] = sa2;
-    zs[(2 * warp + 1) * TC + lane] = bdry;
+    if (b.M) b.M[IDN * sv + off] = fix;
+    if (du_only) {
+#pragma unroll
+      for (int v = 0; v < 5; ++v) vic_set_d(b, v * sv + off, du[v]);
+      continue;
+    }
+    double unew_rho = 0.;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      double un = vic_rk_from(b.u, b.u0, v * sv + off, first, uo[k][v], u0o[k][v], b.wgt0,
+                              b.wgt1, b.wgt2, du[v]);
+      if (v == IDN) unew_rho = vic_full_rho(b, un, xi);
+    }
+#pragma unroll
+    for (int n = 0; n < NS; ++n) {
+      const int64_t o = n * sv + off;
+      double ds = (double)dso[k][n] + fix * (double)ro[k][n];
+      double sn = vic_rk_from(b.s, b.s0, o, first, so[k][n], s0o[k][n], b.wgt0, b.wgt1,
+                              b.wgt2, ds);
+      b.r[o] = sn / unew_rho;
+    }
   }
-  __syncthreads();
-  // (4) the tile's cells
-  using F = VicFin<N, NS, StoredT<B>>;
-  for (int i0 = 0; i0 < nl; i0 += F::TL)
-    vic_finish_subtile<N, NS, B>(g, b, S, zs, cbs, col0, ncol, i0, sm);
+}
+
+// Which finish variant a form takes, and its launch shape.
+template <int N, int NS, class T>
+struct FinCfg {
+  static constexpr bool staged = finish_smem_bytes<N, NS, T>() <= 48 * 1024;
+  static constexpr int threads = 256;
+  static constexpr int layers = staged ? FinSmem<N, NS>::TL : 32;  // tile height
+  static constexpr int min_ctas = staged ? 4 : 2;  // register budget of the batched kernel
+  // one-block kernel: two resident CTAs for FP32 state (its register
+  // variant sits just above 128 registers uncapped, which would leave one);
+  // FP64 state keeps the compiler's budget (capping it spills)
+  static constexpr int min_ctas_single = staged ? 4 : (sizeof(T) == 4 ? 2 : 1);
+  static constexpr size_t smem = staged ? finish_smem_bytes<N, NS, T>() : 0;
+};
+// the FP32 form stages exactly when it carries no scalars (the batched plan
+// sizes its tiles with vic_finish_layers32)
+static_assert(FinCfg<3, 0, float>::staged && FinCfg<5, 0, float>::staged &&
+                  !FinCfg<3, 1, float>::staged && !FinCfg<5, 1, float>::staged,
+              "finish variant of the FP32 form");
+template <class B>
+using StoredT = std::remove_pointer_t<decltype(std::declval<B>().u)>;
+
+template <int N, int NS, class B>
+__device__ __forceinline__ void vic_finish_tile(const Geo& g, const Phys& p, const B& b,
+                                                int64_t col0, int i0) {
+  using C = FinCfg<N, NS, StoredT<B>>;
+  if constexpr (C::staged)
+    vic_finish_tile_staged<N, NS, B>(g, p, b, col0, i0);
+  else
+    vic_finish_tile_regs<N, NS, B, C::threads, C::layers>(g, p, b, col0, i0);
 }
 
 template <int N, int NS, class B>
-__global__ void __launch_bounds__(VicCfg<N>::NT, N == 3 ? 2 : 1) k_vic(Geo g, Phys p, B b) {
-  extern __shared__ __align__(16) double vic_smem[];
-  vic_tile<N, NS, B>(g, p, b, (int64_t)blockIdx.x, vic_smem);
-}
-
-template <int N, int NS, class B>
-static cudaError_t launch_vic_ns(const Geo& g, const Phys& p, const B& b, cudaStream_t st) {
-  const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
-  const int64_t tiles = (ncol + VicCfg<N>::TC - 1) / VicCfg<N>::TC;
-  constexpr size_t smem = vic_smem_bytes<N, NS, StoredT<B>>();
-  raise_smem_limit(k_vic<N, NS, B>, smem);
-  k_vic<N, NS, B><<<(unsigned)tiles, VicCfg<N>::NT, smem, st>>>(g, p, b);
-  return cudaGetLastError();
+__global__ void __launch_bounds__(FinCfg<N, NS, StoredT<B>>::threads,
+                                  FinCfg<N, NS, StoredT<B>>::min_ctas_single) k_vic_finish(Geo g, Phys p, B b) {
+  vic_finish_tile<N, NS, B>(g, p, b, (int64_t)blockIdx.x * kTC,
+                            (int)blockIdx.y * FinCfg<N, NS, StoredT<B>>::layers);
 }
 
 template <int N, class B>
 static cudaError_t launch_vic_n(const Geo& g, const Phys& p, const B& b, cudaStream_t st) {
+  const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
+  const int nl = g.nx1;
+  // small column counts: narrower CTAs spread the sequential sweeps over more SMs
+  int bs = ncol >= 148 * 128 ? 128 : (ncol >= 148 * 64 ? 64 : 32);
+  bool split = false;
+  if constexpr (std::is_same_v<B, StageBufs>) split = b.vicT != nullptr;
+  if constexpr (std::is_same_v<B, StageBufs>) {
+    if (split) {
+      const int64_t nb = ncol * (nl + 2);
+      k_vic_blocks<N><<<(unsigned)((nb + 255) / 256), 256, 0, st>>>(g, p, b);
+      allow_ring_smem(k_vic_column_pre<N>, pre_ring_bytes<N>(128));
+      k_vic_column_pre<N><<<(unsigned)((ncol + bs - 1) / bs), bs, pre_ring_bytes<N>(bs), st>>>(
+          g, p, b);
+    }
+  }
+  if (!split) {
+    allow_ring_smem(k_vic_column<N, B>, back_ring_bytes<N>(128));
+    k_vic_column<N, B><<<(unsigned)((ncol + bs - 1) / bs), bs, back_ring_bytes<N>(bs), st>>>(
+        g, p, b);
+  }
+  using T = std::remove_pointer_t<decltype(b.u)>;
+#define SNAPB_VF(NS)                                                   \
+  case NS: {                                                           \
+    using FC = FinCfg<N, NS, T>;                                       \
+    dim3 gf((unsigned)((ncol + kTC - 1) / kTC),                        \
+            (unsigned)((nl + FC::layers - 1) / FC::layers));           \
+    if (FC::smem) allow_ring_smem(k_vic_finish<N, NS, B>, FC::smem);   \
+    k_vic_finish<N, NS, B><<<gf, FC::threads, FC::smem, st>>>(g, p, b); \
+  } break;
   switch (p.nscalar) {
-    case 0: return launch_vic_ns<N, 0, B>(g, p, b, st);
-    case 1: return launch_vic_ns<N, 1, B>(g, p, b, st);
-    case 2: return launch_vic_ns<N, 2, B>(g, p, b, st);
-    case 3: return launch_vic_ns<N, 3, B>(g, p, b, st);
+    SNAPB_VF(0)
+    SNAPB_VF(1)
+    SNAPB_VF(2)
+    SNAPB_VF(3)
     default: return cudaErrorInvalidValue;
   }
+#undef SNAPB_VF
+  return cudaGetLastError();
+}
+
+// The column + finish pair (default) or the fused kernel of vicf.cu when the
+// environment sets SNAPB_VIC_KERNEL=fused (read at every launch).
+static bool vic_fused_selected() {
+  const char* v = std::getenv("SNAPB_VIC_KERNEL");
+  return v && std::strcmp(v, "fused") == 0;
+}
+
+cudaError_t launch_vic_column(const Geo& g, const Phys& p, const StageBufs& b,
+                              cudaStream_t st) {
+  if (vic_n(p) == 5) return launch_vic_n<5>(g, p, b, st);
+  return launch_vic_n<3>(g, p, b, st);
 }
 
 cudaError_t launch_vic(const Geo& g, const Phys& p, const StageBufs& b, cudaStream_t st) {
-  if (vic_n(p) == 5) return launch_vic_n<5>(g, p, b, st);
-  return launch_vic_n<3>(g, p, b, st);
+  if (vic_fused_selected()) return launch_vicf(g, p, b, st);
+  return launch_vic_column(g, p, b, st);
 }
 
 cudaError_t launch_vic32(const Geo& g, const Phys& p, const StageBufs32& b, cudaStream_t st) {
+  if (vic_fused_selected()) return launch_vicf32(g, p, b, st);
   if (vic_n(p) == 5) return launch_vic_n<5>(g, p, b, st);
   return launch_vic_n<3>(g, p, b, st);
 }
 
-// ---- persistent batched variant (ensemble members, FP32 form) ----
+// ---- persistent batched variants (ensemble members, FP32 form) ----
 __device__ __forceinline__ void set_stage_vic32(StageBufs32& b, int stage) {
   double w0 = 1., w1 = 0., w2 = 1.;
   if (stage == 1) w0 = 3. / 4., w1 = 1. / 4., w2 = 1. / 4.;
@@ -671,56 +1023,105 @@ __device__ __forceinline__ void set_stage_vic32(StageBufs32& b, int stage) {
   b.wgt2 = w2;
 }
 
-// Work items: the 32-column tiles of every member.  Each member's result is
-// bit-identical to snapb_stage_f32 on that member alone (same tile function).
-template <int N, int NS>
-__global__ void __launch_bounds__(VicCfg<N>::NT, N == 3 ? 2 : 1)
-    k_vic_batch(const Member32* __restrict__ mem, Phys p, WorkQueue q, int stage) {
-  // the member's descriptor is read from shared memory as the tile needs its
-  // fields rather than held in registers
+// V selects the register budget: 0 = compiler's choice, 1 = at least 3 CTAs of
+// 128 threads per SM (~168 registers), 2 = 4 CTAs (128 registers, some spill)
+template <int N, int V>
+__global__ void __launch_bounds__(128, V == 0 ? 1 : (V == 1 ? 3 : 4))
+    k_vic_column_batch(const Member32* __restrict__ mem, Phys p, WorkQueue q, int stage) {
+  // The member's descriptor is read from shared memory as the sweep needs its
+  // fields instead of being copied into registers (~50 of them) for the tile
+  // (for the sweeps of stage32.cu the compiler hoists those reads and spills).
   __shared__ Member32 s_mem;
-  extern __shared__ __align__(16) double vic_smem[];
+  int m;
+  int64_t tile;
+  while (queue_next(q, m, tile)) {  // (starts with a barrier: the last tile is done)
+    load_member(s_mem, mem, m);
+    const int64_t col = tile * s_mem.vic_cols + threadIdx.x;
+    if ((int)threadIdx.x < s_mem.vic_cols) vic_column<N, StageBufs32>(s_mem.g, p, s_mem.b, col);
+  }
+  (void)stage;
+}
+
+template <int N, int NS>
+__global__ void __launch_bounds__(FinCfg<N, NS, float>::threads,
+                                  FinCfg<N, NS, float>::min_ctas) k_vic_finish_batch(const Member32* __restrict__ mem,
+                                                          Phys p, WorkQueue q, int stage) {
+  __shared__ Member32 s_mem;  // the member's descriptor, read as needed (see the column kernel)
   int m;
   int64_t tile;
   while (queue_next(q, m, tile)) {  // (starts with a barrier: the last tile is done)
     load_member(s_mem, mem, m);
     if (threadIdx.x == 0) set_stage_vic32(s_mem.b, stage);
     __syncthreads();
-    vic_tile<N, NS, StageBufs32>(s_mem.g, p, s_mem.b, tile, vic_smem);
+    constexpr int TLY = FinCfg<N, NS, float>::layers;
+    const int nlb = (s_mem.g.nx1 + TLY - 1) / TLY;
+    const int64_t cb = tile / nlb;
+    const int lb = (int)(tile - cb * nlb);
+    vic_finish_tile<N, NS, StageBufs32>(s_mem.g, p, s_mem.b, cb * kTC, lb * TLY);
   }
 }
 
-template <int N, int NS>
-static cudaError_t launch_vic_batch_ns(const Member32* mem, const Phys& p, const WorkQueue& q,
-                                       int stage, const PersistGrid& pg, cudaStream_t st) {
-  constexpr size_t smem = vic_smem_bytes<N, NS, float>();
-  raise_smem_limit(k_vic_batch<N, NS>, smem);
-  const int grid = persistent_grid(k_vic_batch<N, NS>, VicCfg<N>::NT, smem, pg);
-  k_vic_batch<N, NS><<<grid, VicCfg<N>::NT, smem, st>>>(mem, p, q, stage);
+template <int N, int V>
+static void launch_vcb(const Member32* mem, const Phys& p, const WorkQueue& q, int stage,
+                       const PersistGrid& pg, int block, cudaStream_t st) {
+  const size_t smem = back_ring_bytes<N>(block);
+  allow_ring_smem(k_vic_column_batch<N, V>, back_ring_bytes<N>(128));
+  k_vic_column_batch<N, V><<<persistent_grid(k_vic_column_batch<N, V>, block, smem, pg), block,
+                             smem, st>>>(mem, p, q, stage);
+}
+
+cudaError_t launch_vic_column_batch(const Member32* mem, const Phys& p, const WorkQueue& q,
+                                    int stage, const PersistGrid& pg, int block, int variant,
+                                    cudaStream_t st) {
+  const bool five = vic_n(p) == 5;
+  switch (variant) {
+    case 1: five ? launch_vcb<5, 1>(mem, p, q, stage, pg, block, st)
+                 : launch_vcb<3, 1>(mem, p, q, stage, pg, block, st); break;
+    case 2: five ? launch_vcb<5, 2>(mem, p, q, stage, pg, block, st)
+                 : launch_vcb<3, 2>(mem, p, q, stage, pg, block, st); break;
+    default: five ? launch_vcb<5, 0>(mem, p, q, stage, pg, block, st)
+                  : launch_vcb<3, 0>(mem, p, q, stage, pg, block, st);
+  }
   return cudaGetLastError();
 }
 
-cudaError_t launch_vic_batch(const Member32* mem, const Phys& p, const WorkQueue& q, int stage,
-                             const PersistGrid& pg, cudaStream_t st) {
-#define SNAPB_VB(NV)                                                          \
-  switch (p.nscalar) {                                                        \
-    case 0: return launch_vic_batch_ns<NV, 0>(mem, p, q, stage, pg, st);      \
-    case 1: return launch_vic_batch_ns<NV, 1>(mem, p, q, stage, pg, st);      \
-    case 2: return launch_vic_batch_ns<NV, 2>(mem, p, q, stage, pg, st);      \
-    case 3: return launch_vic_batch_ns<NV, 3>(mem, p, q, stage, pg, st);      \
-    default: return cudaErrorInvalidValue;                                    \
-  }
-  if (vic_n(p) == 5) {
-    SNAPB_VB(5)
-  }
-  SNAPB_VB(3)
-#undef SNAPB_VB
+int vic_finish_layers32(int nscalar) {
+  return nscalar == 0 ? FinCfg<3, 0, float>::layers : FinCfg<3, 1, float>::layers;
 }
 
-int vic_tile_columns() { return VicCfg<3>::TC; }
+cudaError_t launch_vic_finish_batch(const Member32* mem, const Phys& p, const WorkQueue& q,
+                                    int stage, const PersistGrid& pg, cudaStream_t st) {
+  static_assert(kTC == kVicFinishCols, "finish tile shape");
+#define SNAPB_VFB(N, NS)                                                                  \
+  {                                                                                       \
+    using FC = FinCfg<N, NS, float>;                                                      \
+    if (FC::smem) allow_ring_smem(k_vic_finish_batch<N, NS>, FC::smem);                   \
+    k_vic_finish_batch<N, NS><<<persistent_grid(k_vic_finish_batch<N, NS>, FC::threads,   \
+                                                FC::smem, pg),                            \
+                                FC::threads, FC::smem, st>>>(mem, p, q, stage);           \
+  }
+  if (vic_n(p) == 5) {
+    switch (p.nscalar) {
+      case 0: SNAPB_VFB(5, 0); break;
+      case 1: SNAPB_VFB(5, 1); break;
+      case 2: SNAPB_VFB(5, 2); break;
+      case 3: SNAPB_VFB(5, 3); break;
+      default: return cudaErrorInvalidValue;
+    }
+  } else {
+    switch (p.nscalar) {
+      case 0: SNAPB_VFB(3, 0); break;
+      case 1: SNAPB_VFB(3, 1); break;
+      case 2: SNAPB_VFB(3, 2); break;
+      case 3: SNAPB_VFB(3, 3); break;
+      default: return cudaErrorInvalidValue;
+    }
+  }
+#undef SNAPB_VFB
+  return cudaGetLastError();
+}
 
 }  // namespace snapb
-
 
 // ---------------------------------------------------------------------------
 // Implicit correction without any allocation.
@@ -778,7 +1179,7 @@ extern "C" int snapb_implicit_correction_noalloc(const snapb_hydro_config* cfg, 
   Geo g = make_geo(*cfg);
   Phys p = make_phys(*cfg);
   p.nscalar = 0;
-  size_t need = vic_scratch_bytes(g, p);
+  size_t need = vic_column_scratch_bytes(g, p);
   if (need > kNoAllocScratchBytes)
     return internal_fail(SNAPB_ERR_ARG,
                          "implicit_correction_noalloc: the column solve needs " +
@@ -801,7 +1202,7 @@ extern "C" int snapb_implicit_correction_noalloc(const snapb_hydro_config* cfg, 
   b.M = mass_corr;
   b.vic = scratch;
   b.vic_du_only = 1;
-  e = launch_vic(g, p, b, static_cast<cudaStream_t>(stream));
+  e = launch_vic_column(g, p, b, static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess)
     return internal_fail(SNAPB_ERR_CUDA, std::string("implicit_correction_noalloc: ") +
                                              cudaGetErrorString(e));

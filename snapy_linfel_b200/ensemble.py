@@ -174,7 +174,8 @@ class Ensemble:
         import torch
 
         cand = candidates or {"x1_columns": [0, 4, 8], "march_segment": [16, 32, 64],
-                              "ctas_per_sm": [0, 4, 8]}
+                              "ctas_per_sm": [0, 4, 8], "vic_block": [32, 64, 128],
+                              "vic_regs": [0, 1, 2, 3]}
         snap = self.save()
         results = []
         best = None

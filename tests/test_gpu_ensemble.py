@@ -95,3 +95,15 @@ def test_autotuner_keeps_results(dev):
     ens.step()
     for a, b in zip([b.hydro_u for b in ens.blocks], ref):
         assert torch.equal(a, b)
+
+
+def test_fused_implicit_variant_batched_equals_one_block(dev, monkeypatch):
+    """the fused implicit-solve kernel (tuning vic_regs = 3, and
+    SNAPB_VIC_KERNEL=fused for the one-block path) gives every member exactly
+    the one-block result"""
+    monkeypatch.setenv("SNAPB_VIC_KERNEL", "fused")
+    members = small_members(n=4, seed=11)
+    ref = singles(members, 2, dev)
+    _, got = batched(members, 2, dev, tuning={"vic_regs": 3})
+    for k, (a, b) in enumerate(zip(got, ref)):
+        assert torch.equal(a, b), f"member {k}: max diff {float((a - b).abs().max())}"

@@ -224,6 +224,23 @@ def test_forward_sod(L, oracle):
     assert err < 1e-12
 
 
+@pytest.mark.parametrize("variant", ["column", "fused"])
+def test_steps_3d_scalars_implicit_both_variants(L, oracle, variant, monkeypatch):
+    """three steps of a 3-D Roe domain with two tracers and VIC 3x3 through
+    either implicit-solve variant, against the oracle"""
+    if variant == "fused":
+        monkeypatch.setenv("SNAPB_VIC_KERNEL", "fused")
+    opts, w, r = problems.large_3d(nx3=10, nx2=12, nx1=16, nscalar=2)
+    dts = [0.5, 0.5, 0.5]
+    mb, _ = _run_gpu(opts, w, r, 3, dts=dts)
+    u_ref, s_ref, _ = _run_oracle(oracle, opts, w, r, 3, dts=dts)
+    it = (slice(None),) + opts.hydro.interior()
+    assert state_err(mb.hydro_u.cpu().numpy()[it], u_ref[it], u_ref[it]) < 1e-12 * 3
+    s = mb.scalar_s.cpu().numpy()[it]
+    assert_finite(s)
+    assert np.max(np.abs(s - s_ref[it])) / np.max(np.abs(s_ref[it])) < 1e-12 * 3
+
+
 @pytest.mark.parametrize("riemann", ["lmars", "hllc", "roe"])
 @pytest.mark.parametrize("scheme", [0, 1, 9])
 def test_forward_straka(L, oracle, riemann, scheme):
@@ -361,8 +378,13 @@ def golden_npz():
 
 
 # ------------------------------------------------ implicit correction ----
+@pytest.mark.parametrize("variant", ["column", "fused"])
 @pytest.mark.parametrize("scheme", [1, 9])
-def test_implicit_correction_matches_oracle(L, oracle, scheme):
+def test_implicit_correction_matches_oracle(L, oracle, scheme, variant, monkeypatch):
+    """both implicit-solve variants: the column + finish kernels and the
+    fused kernel (SNAPB_VIC_KERNEL=fused)"""
+    if variant == "fused":
+        monkeypatch.setenv("SNAPB_VIC_KERNEL", "fused")
     opts, w, _ = problems.straka(nx2=40, nx1=24, implicit_scheme=scheme)
     c = opts.hydro
     oracle.bc_apply(c, w, PRIMITIVE)

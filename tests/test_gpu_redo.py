@@ -36,6 +36,19 @@ def _block(nscalar=0):
     return mb
 
 
+def _dt_pair(mb):
+    """(dt at the block's current_redo, dt at current_redo = 0) from the same
+    hydro_w: the retried step's limit is the CFL limit of the state hydro_w
+    holds (the last stage's input, as in the reference), scaled by 2^-redo"""
+    d1 = float(mb.max_time_step().item())
+    r = mb.current_redo
+    mb.current_redo = 0
+    d0 = float(mb.max_time_step().item())
+    mb.current_redo = r
+    mb.max_time_step()
+    return d1, d0
+
+
 def _cell(mb):
     c = mb.cfg
     return (c.nghost + 1 if c.nx3 > 1 else 0, c.nghost + 2 if c.nx2 > 1 else 0, c.nghost + 3)
@@ -45,7 +58,7 @@ def test_negative_density_rejects_and_restores_bit_for_bit():
     mb = _block(nscalar=2)
     mb.step()
     assert mb.check_redo() == 0
-    dt_full = float(mb.max_time_step().item())
+    mb.max_time_step()
     u_start = mb.hydro_u.clone()
     s_start = mb.scalar_s.clone()
     for s in range(3):
@@ -58,9 +71,9 @@ def test_negative_density_rejects_and_restores_bit_for_bit():
     assert torch.equal(mb.scalar_s, s_start)
     assert mb.current_redo == 1
     assert mb.cycle == cycle - 1
-    # the retried step's CFL dt is halved (same state, same limit)
-    dt_half = float(mb.max_time_step().item())
-    assert dt_half == 0.5 * dt_full
+    # the retried step's CFL dt carries the factor 2^-1
+    d1, d0 = _dt_pair(mb)
+    assert d1 == 0.5 * d0
     # a healthy retry clears the redo count
     for s in range(3):
         mb.forward(s)
@@ -93,16 +106,14 @@ def test_gives_up_past_max_redo():
     mb = _block()
     mb.step()
     max_redo = mb.options.integration.max_redo
-    dts = []
     for n in range(max_redo):
-        dts.append(float(mb.max_time_step().item()))
+        d1, d0 = _dt_pair(mb)
+        assert d1 == 2.0 ** -n * d0
         for s in range(3):
             mb.forward(s)
         mb.hydro_u[(0,) + _cell(mb)] = 0.0  # density <= 0 every time
         assert mb.check_redo() == 1
         assert mb.current_redo == n + 1
-    for a, b in zip(dts, dts[1:]):
-        assert b == 0.5 * a
     for s in range(3):
         mb.forward(s)
     mb.hydro_u[(0,) + _cell(mb)] = -2.0
