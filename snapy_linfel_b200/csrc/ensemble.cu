@@ -180,7 +180,7 @@ int plan(snapb_ensemble* e) {
     tiles[PH_X2] = e->a2 ? ((lines2 + 127) / 128) * mb.nseg2 : 0;
     tiles[PH_X3] = e->a3 ? ((lines3 + 127) / 128) * mb.nseg3 : 0;
     tiles[PH_VCOL] = e->p.implicit_scheme ? (ncolv + mb.vic_cols - 1) / mb.vic_cols : 0;
-    const int fl = vic_finish_layers32(e->p.nscalar);
+    const int fl = vic_finish_layers32(e->p);
     tiles[PH_VFIN] = e->p.implicit_scheme
                          ? ((ncolv + kVicFinishCols - 1) / kVicFinishCols) * ((g.nx1 + fl - 1) / fl)
                          : 0;

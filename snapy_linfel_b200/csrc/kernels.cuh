@@ -212,7 +212,7 @@ cudaError_t launch_vic_column(const Geo& g, const Phys& p, const StageBufs& b, c
 cudaError_t launch_vicf(const Geo& g, const Phys& p, const StageBufs& b, cudaStream_t st);
 cudaError_t launch_vicf32(const Geo& g, const Phys& p, const StageBufs32& b, cudaStream_t st);
 size_t vic_blocks_bytes(const Geo& g, const Phys& p);
-int vic_finish_layers32(int nscalar);  // layers per implicit-finish tile, FP32 form
+int vic_finish_layers32(const Phys& p);  // layers per implicit-finish tile, FP32 form
 
 cudaError_t launch_cons2prim(const Geo& g, const Phys& p, const double* u, double* w,
                              cudaStream_t st);

@@ -85,7 +85,8 @@ size_t vic_blocks_bytes(const Geo& g, const Phys& p) {
   return (size_t)((int64_t)(g.nx1 + 2) * 2 * N * N * ncol) * sizeof(double);
 }
 
-constexpr int kTC = 32;  // columns per tile
+constexpr int kTC = 32;           // columns per tile
+constexpr int kFinThreads = 256;  // threads of a finish CTA
 
 // Back substitution: the reduced block, partial solution and du[IDN] of a
 // layer are fetched kBackDepth<N> layers ahead into a per-thread ring in
@@ -99,9 +100,11 @@ struct BackRing {
   static constexpr int depth = N == 3 ? 4 : 2;
   static constexpr int elems = N * N + N + 1;
 };
-template <int N>
+// RT: ring element type, the scratch precision of the solve (FP32 slots
+// leave the L1 share of the SM's shared-memory carveout twice as large)
+template <int N, class RT = double>
 constexpr size_t back_ring_bytes(int threads) {
-  return (size_t)threads * BackRing<N>::depth * BackRing<N>::elems * sizeof(double);
+  return (size_t)threads * BackRing<N>::depth * BackRing<N>::elems * sizeof(RT);
 }
 
 
@@ -172,9 +175,24 @@ __device__ __forceinline__ double vic_full_rho(const StageBufs32& b, double u_rh
   return u_rho + b.rb[xi];
 }
 
-// Block construction per form: the FP64 plain form in FP64; the FP32
-// perturbation form forms |A| and J in FP32 from the full states (only the
-// elimination and the balance terms stay FP64 there) and widens them.
+// Precision of the elimination and of its scratch per form and block size:
+// FP64 for the FP64 plain form; for the FP32 perturbation form (whose blocks
+// |A| and J are formed in FP32 from the full states) FP32 for N = 3 and FP64
+// for N = 5.  The block systems are diagonally dominant (the 1/dt diagonal
+// over upwind-split off-diagonal blocks, |A| +- J >= 0 in the characteristic
+// basis), so an FP32 elimination does not amplify its rounding; the N = 3
+// cofactor solve has a fixed operation order, while the pivoted N = 5 LU in
+// FP32 meets near-ties in the pivot choice, where one-ulp differences of the
+// compiled kernels (one-block and batched) would select different rows.  The
+// MS-VIC column sums are accumulated in FP64 in every case.
+template <int N, class T>  // T: stored precision of the state
+using VicScratchT = std::conditional_t<N == 3 && std::is_same_v<T, float>, float, double>;
+template <class B, int N>
+struct VicPrec {
+  using T = VicScratchT<N, std::remove_pointer_t<decltype(std::declval<B>().u)>>;
+};
+
+// Block construction per form, in the elimination precision
 template <int N>
 __device__ __forceinline__ void absA_of(const StageBufs&, double gm1, const double* wl,
                                         const double* wr, double (&A)[N][N]) {
@@ -212,6 +230,20 @@ __device__ __forceinline__ void jac_of(const StageBufs32&, double gm1, const dou
 #pragma unroll
     for (int q = 0; q < N; ++q) J[r][q] = (double)F[r][q];
 }
+template <int N>
+__device__ __forceinline__ void absA_of(const StageBufs32&, double gm1, const float* wl,
+                                        const float* wr, float (&A)[N][N]) {
+  absA_block<N, float>((float)gm1, wl, wr, A);
+}
+template <int N>
+__device__ __forceinline__ void jac_of(const StageBufs32&, double gm1, const float* w,
+                                       float (&J)[N][N]) {
+  jac_block<N, float>((float)gm1, w, J);
+}
+// right-hand side du / dt of one row: the FP64 form divides as the reference
+// does; the FP32 form multiplies by 1/dt
+__device__ __forceinline__ double vic_rhs(double d, double dt, double) { return d / dt; }
+__device__ __forceinline__ float vic_rhs(double d, double, float idt) { return (float)d * idt; }
 
 // One layer of the block-Thomas forward elimination: a_i, b_i, c_i from |A|
 // at the layer's lower / upper faces (Am, Ap) and J of the cells below /
@@ -333,30 +365,32 @@ __device__ __forceinline__ void vic_back(const B& b, double* S, double* Z, int64
 template <int N, class B>
 __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B& b, int64_t col) {
   constexpr int ES = VicDims<N>::ES;
+  using ET = typename VicPrec<B, N>::T;  // elimination and scratch precision
   const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
   if (col >= ncol) return;
   const int nl = g.nx1;
   const int64_t sv = g.sv;
   const int64_t cb = column_base(g, col);
-  double* S = b.vic + col;
-  double* Z = S + (int64_t)nl * ES * ncol;
-  auto Sat = [&](int i, int e) -> double& { return S[((int64_t)i * ES + e) * ncol]; };
-  auto load_w = [&](int i, double* w) {
+  ET* S = reinterpret_cast<ET*>(b.vic) + col;  // [nl][ES][ncol] in ET
+  double* Z = b.vic + (int64_t)nl * ES * ncol + col;
+  auto Sat = [&](int i, int e) -> ET& { return S[((int64_t)i * ES + e) * ncol]; };
+  auto load_w = [&](int i, ET* w) {
 #pragma unroll
-    for (int v = 0; v < 5; ++v) w[v] = vic_w(b, sv, v, cb + i, g.il + i);
+    for (int v = 0; v < 5; ++v) w[v] = (ET)vic_w(b, sv, v, cb + i, g.il + i);
   };
   const double gm1c = p.gammad - 1.;
   const double gm1f = 0.5 * (p.gammad + p.gammad) - 1.;
-  const double dt = *b.dt;
-  const double Aa = g.A1, hiv = 0.5 / g.vol, idt = 1. / dt, grav = p.grav1, V = g.vol;
+  const double dt = *b.dt, V = g.vol;
+  const ET Aa = (ET)g.A1, hiv = (ET)(0.5 / g.vol), idt = (ET)(1. / dt), grav = (ET)p.grav1;
   // Forward sweep inputs (w of cell L and the rows of du at layer L-1,
   // 1 <= L <= nl) arrive kFwdDepth layers ahead through the same per-thread
   // shared-memory ring as the back substitution, layout [slot][element][thread].
   constexpr int DF = kFwdDepth, FE = 5 + N;
   static_assert(DF * FE <= BackRing<N>::depth * BackRing<N>::elems, "ring too small");
   extern __shared__ double vic_ring[];
+  ET* const ringb = reinterpret_cast<ET*>(vic_ring);  // slots in the scratch precision
   const int nt = blockDim.x, lane = threadIdx.x;
-  auto fring = [&](int slot, int e) { return vic_ring + ((size_t)(slot * FE + e) * nt + lane); };
+  auto fring = [&](int slot, int e) { return ringb + ((size_t)(slot * FE + e) * nt + lane); };
   auto ffetch = [&](int L, int slot) {
     if (L <= nl) {
 #pragma unroll
@@ -369,8 +403,8 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
   };
 #pragma unroll
   for (int k = 0; k < DF; ++k) ffetch(1 + k, k);
-  double wc[5], wn[5];
-  double Am[N][N], Jp[N][N], Jc[N][N], ap[N][N], dp[N];
+  ET wc[5], wn[5];
+  ET Am[N][N], Jp[N][N], Jc[N][N], ap[N][N], dp[N];
   load_w(-1, wn);
   jac_of<N>(b, gm1c, wn, Jp);
   load_w(0, wc);
@@ -378,23 +412,23 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
   jac_of<N>(b, gm1c, wc, Jc);
   double sum_a2 = 0.;
   for (int i = 0, fslot = 0; i < nl; ++i) {
-    double Ap[N][N], Jn[N][N], rhs[N];
+    ET Ap[N][N], Jn[N][N], rhs[N];
     cp_async_wait<DF - 1>();  // the group of cell i+1 has landed
 #pragma unroll
     for (int v = 0; v < 5; ++v)  // cell i+1 (the ghost cell nl at the top)
-      wn[v] = vic_full(b, ring_elem(fring(fslot, v), b.w), v, g.il + i + 1);
+      wn[v] = (ET)vic_full(b, ring_elem(fring(fslot, v), b.w), v, g.il + i + 1);
 #pragma unroll
-    for (int r = 0; r < N; ++r) rhs[r] = ring_elem(fring(fslot, 5 + r), b.D) / dt;
+    for (int r = 0; r < N; ++r) rhs[r] = vic_rhs(ring_elem(fring(fslot, 5 + r), b.D), dt, idt);
     absA_of<N>(b, gm1f, wc, wn, Ap);
     jac_of<N>(b, gm1c, wn, Jn);
-    double ai = wc[IDN] * V;
+    double ai = (double)wc[IDN] * V;
     sum_a2 += ai * ai;
-    double a[N][N], bb[N][N], c[N][N];
+    ET a[N][N], bb[N][N], c[N][N];
 #pragma unroll
     for (int r = 0; r < N; ++r)
 #pragma unroll
       for (int q = 0; q < N; ++q) {
-        double phi = 0.;
+        ET phi = 0.;
         if (r == 1 && q == 0) phi = grav;
         if (N == 3 && r == 2 && q == 1) phi = grav;
         if (N == 5 && r == IPR && q == IVX) phi = grav;
@@ -408,21 +442,21 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
 #pragma unroll
       for (int r = 0; r < N; ++r)
 #pragma unroll
-        for (int q = 0; q < N; ++q) a[r][q] += bb[r][q] * (q == 1 ? -1. : 1.);
+        for (int q = 0; q < N; ++q) a[r][q] += bb[r][q] * (q == 1 ? ET(-1) : ET(1));
     }
     if (i == nl - 1) {
 #pragma unroll
       for (int r = 0; r < N; ++r)
 #pragma unroll
-        for (int q = 0; q < N; ++q) a[r][q] += c[r][q] * (q == 1 ? -1. : 1.);
+        for (int q = 0; q < N; ++q) a[r][q] += c[r][q] * (q == 1 ? ET(-1) : ET(1));
     }
     if (i > 0) {
 #pragma unroll
       for (int r = 0; r < N; ++r) {
-        double bd = 0.;
+        ET bd = 0.;
 #pragma unroll
         for (int q = 0; q < N; ++q) {
-          double t = 0.;
+          ET t = 0.;
 #pragma unroll
           for (int kk = 0; kk < N; ++kk) t += bb[r][kk] * ap[kk][q];
           a[r][q] -= t;
@@ -460,36 +494,36 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
   // way, the inputs of each layer arriving through the shared-memory ring.
   constexpr int DB = BackRing<N>::depth, RE = BackRing<N>::elems;
   cp_async_wait<0>();  // the forward ring is drained before its memory is reused
-  auto ring = [&](int slot, int e) { return vic_ring + ((size_t)(slot * RE + e) * nt + lane); };
+  auto ring = [&](int slot, int e) { return ringb + ((size_t)(slot * RE + e) * nt + lane); };
   auto fetch = [&](int i, int slot) {
     if (i >= 0) {
 #pragma unroll
-      for (int e = 0; e < ES; ++e) cp_async_bytes8(ring(slot, e), &Sat(i, e));
+      for (int e = 0; e < ES; ++e) cp_async_elem(ring(slot, e), &Sat(i, e));
       cp_async_elem(ring(slot, ES), b.D + IDN * sv + cb + i);
     }
     cp_async_commit();
   };
-  double dn[N];
+  ET dn[N];
 #pragma unroll
   for (int r = 0; r < N; ++r) dn[r] = dp[r];
-  double b_dry = (vic_d(b, IDN * sv + cb + nl - 1) - dn[0]) * 1. * V;
+  double b_dry = (vic_d(b, IDN * sv + cb + nl - 1) - (double)dn[0]) * 1. * V;
 #pragma unroll
   for (int k = 0; k < DB; ++k) fetch(nl - 2 - k, k);
   for (int i = nl - 2, slot = 0; i >= 0; --i) {
     cp_async_wait<DB - 1>();  // the group of layer i has landed
-    double cur[ES];
+    ET cur[ES];
 #pragma unroll
-    for (int e = 0; e < ES; ++e) cur[e] = *ring(slot, e);
+    for (int e = 0; e < ES; ++e) cur[e] = (ET)ring_elem(ring(slot, e), S);
     const double dcur = ring_elem(ring(slot, ES), b.D);
-    double d[N];
+    ET d[N];
 #pragma unroll
     for (int r = 0; r < N; ++r) {
-      double t = 0.;
+      ET t = 0.;
 #pragma unroll
       for (int q = 0; q < N; ++q) t += cur[r * N + q] * dn[q];
       d[r] = cur[N * N + r] - t;
     }
-    b_dry += (dcur - d[0]) * 1. * V;
+    b_dry += (dcur - (double)d[0]) * 1. * V;
     fetch(i - DB, slot);  // the slot's values are consumed: refill it
     slot = slot + 1 == DB ? 0 : slot + 1;
 #pragma unroll
@@ -650,26 +684,37 @@ template <int N, class B>
 __global__ void __launch_bounds__(128) k_vic_column(Geo g, Phys p, B b) {
   vic_column<N, B>(g, p, b, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
 }
+// the FP32 form's N = 3 sweep (FP32 elimination): its 128-register build
+// serialises the next layer's block formation behind the elimination, so it
+// takes the register budget of one resident CTA
+__global__ void __launch_bounds__(128, 1) k_vic_column32_n3(Geo g, Phys p, StageBufs32 b) {
+  vic_column<3, StageBufs32>(g, p, b, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
+}
 
 // (3) redistribution + RK combination (or du), tiles of 32 columns x 32
 // layers: delta is transposed through shared memory so that the state
 // arrays are read and written along x1.
 // one tile: columns col0 .. col0+kTC-1, layers i0 .. i0+kTL-1 (whole CTA)
 // Shared memory of one finish tile: the back-substituted solution rows
-// [N][kTC][kTL+1] (doubles), the column sums and offsets, then the tile's cell
-// inputs [element][kTC][kTL] in the stored precision T: w'[IDN], the du rows
-// the solve does not replace, and (RK update) u, u0, and per scalar s, s0, r
-// and its du row.
+// [N][kTC][kTL+1] in the scratch precision of the solve, the column sums and
+// offsets, then the tile's cell inputs [element][kTC][kTL] in the stored
+// precision T.  Cell inputs: w'[IDN], the du
+// rows the solve does not replace, and (RK update) u, u0, and per scalar s,
+// s0, r and its du row.
 template <int N, int NS>
 struct FinSmem {
   static constexpr int TL = 16;  // layers per staged tile
   static constexpr int du_rows = N == 3 ? 3 : 1;           // IDN (+ IVY, IVZ)
   static constexpr int elems = 1 + du_rows + 10 + 4 * NS;  // upper bound
-  static constexpr size_t head = ((size_t)N * kTC * (TL + 1) + 3 * kTC) * sizeof(double);
+  template <class T>
+  static constexpr size_t head() {  // (N kTC (TL+1) 4 is a multiple of 8)
+    return (size_t)N * kTC * (TL + 1) * sizeof(VicScratchT<N, T>) + 3 * kTC * sizeof(double);
+  }
 };
 template <int N, int NS, class T>
 constexpr size_t finish_smem_bytes() {
-  return FinSmem<N, NS>::head + (size_t)FinSmem<N, NS>::elems * kTC * FinSmem<N, NS>::TL * sizeof(T);
+  return FinSmem<N, NS>::template head<T>() +
+         (size_t)FinSmem<N, NS>::elems * kTC * FinSmem<N, NS>::TL * sizeof(T);
 }
 
 // One tile: columns col0 .. col0+kTC-1, layers i0 .. i0+kTL-1 (whole CTA).
@@ -682,17 +727,18 @@ __device__ __forceinline__ void vic_finish_tile_staged(const Geo& g, const Phys&
                                                 int64_t col0, int i0) {
   constexpr int ES = VicDims<N>::ES, DR = FinSmem<N, NS>::du_rows, kTL = FinSmem<N, NS>::TL;
   using T = std::remove_pointer_t<decltype(b.u)>;  // stored precision (FP32 / FP64)
+  using ET = typename VicPrec<B, N>::T;              // scratch precision of the solve
   const int nl = g.nx1;
   const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
   const int64_t sv = g.sv;
-  const double* S = b.vic;
-  const double* Z = S + (int64_t)nl * ES * ncol;
+  const ET* S = reinterpret_cast<const ET*>(b.vic);
+  const double* Z = b.vic + (int64_t)nl * ES * ncol;
   extern __shared__ double fin_smem[];
-  double* dl = fin_smem;                                     // [N][kTC][kTL+1]
-  double* zs = dl + (size_t)N * kTC * (kTL + 1);             // [2][kTC]
+  ET* dl = reinterpret_cast<ET*>(fin_smem);                  // [N][kTC][kTL+1]
+  double* zs = reinterpret_cast<double*>(dl + (size_t)N * kTC * (kTL + 1));  // [2][kTC]
   int64_t* cbs = reinterpret_cast<int64_t*>(zs + 2 * kTC);   // [kTC]
   T* cell = reinterpret_cast<T*>(cbs + kTC);                 // [element][kTC][kTL]
-  auto DL = [&](int r, int c, int s) -> double& {
+  auto DL = [&](int r, int c, int s) -> ET& {
     return dl[((size_t)r * kTC + c) * (kTL + 1) + s];
   };
   auto CE = [&](int e, int c, int s) -> T* { return cell + ((size_t)e * kTC + c) * kTL + s; };
@@ -706,39 +752,58 @@ __device__ __forceinline__ void vic_finish_tile_staged(const Geo& g, const Phys&
     if (k == 0) cbs[c] = col0 + c < ncol ? column_base(g, col0 + c) : 0;
   }
   __syncthreads();
-  for (int idx = tid; idx < N * kTC * kTL; idx += blockDim.x) {
-    int c = idx % kTC, rest = idx / kTC;
-    int s = rest % kTL, r = rest / kTL;
-    int64_t col = col0 + c;
-    int i = i0 + s;
-    if (col < ncol && i < nl)
-      cp_async_bytes8(&DL(r, c, s), S + ((int64_t)i * ES + N * N + r) * ncol + col);
+  // Each thread copies the same CPT cells of every element: their offsets are
+  // formed once, and the element loops pick one source array per pass.
+  constexpr int CPT = kTC * kTL / kFinThreads;
+  static_assert(CPT * kFinThreads == kTC * kTL, "finish tile and CTA shape");
+  {  // solution rows, columns fastest (S is [layer][element][column])
+    int64_t soff[CPT];
+    bool sok[CPT];
+#pragma unroll
+    for (int j = 0; j < CPT; ++j) {
+      const int idx = tid + j * kFinThreads, c = idx % kTC, s = idx / kTC;
+      sok[j] = col0 + c < ncol && i0 + s < nl;
+      soff[j] = ((int64_t)(i0 + s) * ES + N * N) * ncol + col0 + c;
+    }
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+      for (int j = 0; j < CPT; ++j) {
+        const int idx = tid + j * kFinThreads;
+        if (sok[j]) cp_async_elem(&DL(r, idx % kTC, idx / kTC), S + soff[j] + (int64_t)r * ncol);
+      }
   }
-  const int ne = du_only ? eU : (first ? eU0 : eS);  // u0 is the stage input at stage 0
-  for (int idx = tid; idx < ne * kTC * kTL; idx += blockDim.x) {
-    const int s = idx % kTL, rest = idx / kTL;
-    const int c = rest % kTC, e = rest / kTC;
-    const int i = i0 + s;
-    if (col0 + c >= ncol || i >= nl) continue;
-    const int64_t off = cbs[c] + i;
-    const T* src;
-    if (e == eRHO) src = b.w + IDN * sv + off;
-    else if (e < eU) src = b.D + (e == eDU ? IDN : (e == eDU + 1 ? IVY : IVZ)) * sv + off;
-    else if (e < eU0) src = b.u + (e - eU) * sv + off;
-    else src = b.u0 + (e - eU0) * sv + off;
-    cp_async_elem(CE(e, c, s), src);
+  // cell inputs, layers fastest (the state arrays run along x1)
+  int64_t goff[CPT];
+  bool gok[CPT];
+#pragma unroll
+  for (int j = 0; j < CPT; ++j) {
+    const int idx = tid + j * kFinThreads, s = idx % kTL, c = idx / kTL;
+    gok[j] = col0 + c < ncol && i0 + s < nl;
+    goff[j] = gok[j] ? cbs[c] + i0 + s : 0;
+  }
+  auto stage_elem = [&](int e, const T* base) {
+    T* dst = CE(e, 0, 0);
+#pragma unroll
+    for (int j = 0; j < CPT; ++j)
+      if (gok[j]) cp_async_elem(dst + tid + j * kFinThreads, base + goff[j]);
+  };
+  stage_elem(eRHO, b.w + IDN * sv);
+  stage_elem(eDU, b.D + IDN * sv);
+  if constexpr (N == 3) {
+    stage_elem(eDU + 1, b.D + IVY * sv);
+    stage_elem(eDU + 2, b.D + IVZ * sv);
   }
   if (!du_only) {
-    for (int idx = tid; idx < 4 * NS * kTC * kTL; idx += blockDim.x) {
-      const int s = idx % kTL, rest = idx / kTL;
-      const int c = rest % kTC, q = rest / kTC;
-      const int n = q / 4, kind = q % 4;
-      const int i = i0 + s;
-      if (col0 + c >= ncol || i >= nl || (kind == 1 && first)) continue;
-      const int64_t o = n * sv + cbs[c] + i;
-      const T* src = kind == 0 ? b.s + o
-                               : (kind == 1 ? b.s0 + o : (kind == 2 ? b.r + o : b.D + 5 * sv + o));
-      cp_async_elem(CE(eS + q, c, s), src);
+    for (int v = 0; v < 5; ++v) {
+      stage_elem(eU + v, b.u + v * sv);
+      if (!first) stage_elem(eU0 + v, b.u0 + v * sv);  // u0 is the stage input at stage 0
+    }
+    for (int n = 0; n < NS; ++n) {
+      stage_elem(eS + 4 * n, b.s + n * sv);
+      if (!first) stage_elem(eS + 4 * n + 1, b.s0 + n * sv);
+      stage_elem(eS + 4 * n + 2, b.r + n * sv);
+      stage_elem(eS + 4 * n + 3, b.D + (5 + n) * sv);
     }
   }
   cp_async_commit();
@@ -799,12 +864,13 @@ template <int N, int NS, class B, int NT, int kTL>
 __device__ __forceinline__ void vic_finish_tile_regs(const Geo& g, const Phys& p, const B& b,
                                                 int64_t col0, int i0) {
   constexpr int ES = VicDims<N>::ES;
+  using ET = typename VicPrec<B, N>::T;  // scratch precision of the solve
   const int nl = g.nx1;
   const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
   const int64_t sv = g.sv;
-  const double* S = b.vic;
-  const double* Z = S + (int64_t)nl * ES * ncol;
-  __shared__ double dl[N][kTC][kTL + 1];
+  const ET* S = reinterpret_cast<const ET*>(b.vic);
+  const double* Z = b.vic + (int64_t)nl * ES * ncol;
+  __shared__ ET dl[N][kTC][kTL + 1];
   __shared__ double zs[2][kTC];
   __shared__ int64_t cbs[kTC];  // (k, j, il) offsets of the tile's columns
   const int tid = threadIdx.x;
@@ -813,7 +879,7 @@ __device__ __forceinline__ void vic_finish_tile_regs(const Geo& g, const Phys& p
     int s = rest % kTL, r = rest / kTL;
     int64_t col = col0 + c;
     int i = i0 + s;
-    dl[r][c][s] = (col < ncol && i < nl) ? S[((int64_t)i * ES + N * N + r) * ncol + col] : 0.;
+    dl[r][c][s] = (col < ncol && i < nl) ? S[((int64_t)i * ES + N * N + r) * ncol + col] : ET(0);
   }
   if (tid < 2 * kTC) {
     int c = tid % kTC, k = tid / kTC;
@@ -912,7 +978,7 @@ __device__ __forceinline__ void vic_finish_tile_regs(const Geo& g, const Phys& p
 template <int N, int NS, class T>
 struct FinCfg {
   static constexpr bool staged = finish_smem_bytes<N, NS, T>() <= 48 * 1024;
-  static constexpr int threads = 256;
+  static constexpr int threads = kFinThreads;
   static constexpr int layers = staged ? FinSmem<N, NS>::TL : 32;  // tile height
   static constexpr int min_ctas = staged ? 4 : 2;  // register budget of the batched kernel
   // one-block kernel: two resident CTAs for FP32 state (its register
@@ -921,11 +987,6 @@ struct FinCfg {
   static constexpr int min_ctas_single = staged ? 4 : (sizeof(T) == 4 ? 2 : 1);
   static constexpr size_t smem = staged ? finish_smem_bytes<N, NS, T>() : 0;
 };
-// the FP32 form stages exactly when it carries no scalars (the batched plan
-// sizes its tiles with vic_finish_layers32)
-static_assert(FinCfg<3, 0, float>::staged && FinCfg<5, 0, float>::staged &&
-                  !FinCfg<3, 1, float>::staged && !FinCfg<5, 1, float>::staged,
-              "finish variant of the FP32 form");
 template <class B>
 using StoredT = std::remove_pointer_t<decltype(std::declval<B>().u)>;
 
@@ -964,9 +1025,14 @@ static cudaError_t launch_vic_n(const Geo& g, const Phys& p, const B& b, cudaStr
     }
   }
   if (!split) {
-    allow_ring_smem(k_vic_column<N, B>, back_ring_bytes<N>(128));
-    k_vic_column<N, B><<<(unsigned)((ncol + bs - 1) / bs), bs, back_ring_bytes<N>(bs), st>>>(
-        g, p, b);
+    const unsigned grid = (unsigned)((ncol + bs - 1) / bs);
+    if constexpr (N == 3 && std::is_same_v<B, StageBufs32>) {
+      allow_ring_smem(k_vic_column32_n3, back_ring_bytes<N, float>(128));
+      k_vic_column32_n3<<<grid, bs, back_ring_bytes<N, float>(bs), st>>>(g, p, b);
+    } else {
+      allow_ring_smem(k_vic_column<N, B>, back_ring_bytes<N>(128));
+      k_vic_column<N, B><<<grid, bs, back_ring_bytes<N>(bs), st>>>(g, p, b);
+    }
   }
   using T = std::remove_pointer_t<decltype(b.u)>;
 #define SNAPB_VF(NS)                                                   \
@@ -1064,8 +1130,9 @@ __global__ void __launch_bounds__(FinCfg<N, NS, float>::threads,
 template <int N, int V>
 static void launch_vcb(const Member32* mem, const Phys& p, const WorkQueue& q, int stage,
                        const PersistGrid& pg, int block, cudaStream_t st) {
-  const size_t smem = back_ring_bytes<N>(block);
-  allow_ring_smem(k_vic_column_batch<N, V>, back_ring_bytes<N>(128));
+  using RT = VicScratchT<N, float>;
+  const size_t smem = back_ring_bytes<N, RT>(block);
+  allow_ring_smem(k_vic_column_batch<N, V>, back_ring_bytes<N, RT>(128));
   k_vic_column_batch<N, V><<<persistent_grid(k_vic_column_batch<N, V>, block, smem, pg), block,
                              smem, st>>>(mem, p, q, stage);
 }
@@ -1085,8 +1152,18 @@ cudaError_t launch_vic_column_batch(const Member32* mem, const Phys& p, const Wo
   return cudaGetLastError();
 }
 
-int vic_finish_layers32(int nscalar) {
-  return nscalar == 0 ? FinCfg<3, 0, float>::layers : FinCfg<3, 1, float>::layers;
+// finish tile height of the FP32 form (the batched plan sizes its tiles with it)
+template <int N>
+static int finish_layers32(int nscalar) {
+  switch (nscalar) {
+    case 0: return FinCfg<N, 0, float>::layers;
+    case 1: return FinCfg<N, 1, float>::layers;
+    case 2: return FinCfg<N, 2, float>::layers;
+    default: return FinCfg<N, 3, float>::layers;
+  }
+}
+int vic_finish_layers32(const Phys& p) {
+  return vic_n(p) == 5 ? finish_layers32<5>(p.nscalar) : finish_layers32<3>(p.nscalar);
 }
 
 cudaError_t launch_vic_finish_batch(const Member32* mem, const Phys& p, const WorkQueue& q,

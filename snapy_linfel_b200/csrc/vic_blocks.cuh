@@ -81,23 +81,22 @@ __device__ __forceinline__ void absA_block(T gm1, const T* wl, const T* wr, T (&
 
 // X = M^-1 [C | rhs] for an N x N block: cofactor inverse for N = 3,
 // LU with implicit-scaling partial pivoting (Crout) for N = 5
-template <int N>
-__device__ __forceinline__ void block_solve(double (&M)[N][N], double (&C)[N][N],
-                                            double (&rhs)[N]) {
+template <int N, class T>
+__device__ __forceinline__ void block_solve(T (&M)[N][N], T (&C)[N][N], T (&rhs)[N]) {
   if constexpr (N == 3) {
     auto cof = [&](int i, int j) {
       int i1 = (i + 1) % 3, i2 = (i + 2) % 3, j1 = (j + 1) % 3, j2 = (j + 2) % 3;
       return M[i1][j1] * M[i2][j2] - M[i1][j2] * M[i2][j1];
     };
-    double c00 = cof(0, 0), c10 = cof(1, 0), c20 = cof(2, 0);
-    double det = c00 * M[0][0] + c10 * M[1][0] + c20 * M[2][0];
-    double id = 1. / det;
-    double inv[3][3];
+    T c00 = cof(0, 0), c10 = cof(1, 0), c20 = cof(2, 0);
+    T det = c00 * M[0][0] + c10 * M[1][0] + c20 * M[2][0];
+    T id = T(1) / det;
+    T inv[3][3];
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
       for (int j = 0; j < 3; ++j) inv[i][j] = cof(j, i) * id;
-    double x[3], X[3][3];
+    T x[3], X[3][3];
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
       x[i] = inv[i][0] * rhs[0] + inv[i][1] * rhs[1] + inv[i][2] * rhs[2];
@@ -112,33 +111,33 @@ __device__ __forceinline__ void block_solve(double (&M)[N][N], double (&C)[N][N]
       for (int j = 0; j < 3; ++j) C[i][j] = X[i][j];
     }
   } else {
-    double vv[N];
+    T vv[N];
 #pragma unroll
     for (int i = 0; i < N; ++i) {
-      double big = 0.;
+      T big = T(0);
 #pragma unroll
       for (int j = 0; j < N; ++j) big = fmax(big, fabs(M[i][j]));
-      vv[i] = 1.0 / big;
+      vv[i] = T(1) / big;
     }
     int indx[N];
 #pragma unroll
     for (int j = 0; j < N; ++j) {
 #pragma unroll
       for (int i = 0; i < j; ++i) {
-        double s = M[i][j];
+        T s = M[i][j];
 #pragma unroll
         for (int k = 0; k < i; ++k) s -= M[i][k] * M[k][j];
         M[i][j] = s;
       }
-      double big = 0.;
+      T big = T(0);
       int imax = j;
 #pragma unroll
       for (int i = j; i < N; ++i) {
-        double s = M[i][j];
+        T s = M[i][j];
 #pragma unroll
         for (int k = 0; k < j; ++k) s -= M[i][k] * M[k][j];
         M[i][j] = s;
-        double d = vv[i] * fabs(s);
+        T d = vv[i] * fabs(s);
         if (d >= big) {
           big = d;
           imax = i;
@@ -150,18 +149,18 @@ __device__ __forceinline__ void block_solve(double (&M)[N][N], double (&C)[N][N]
         if (i == imax) {
 #pragma unroll
           for (int k = 0; k < N; ++k) {
-            double t = M[i][k];
+            T t = M[i][k];
             M[i][k] = M[j][k];
             M[j][k] = t;
           }
-          double t = vv[i];
+          T t = vv[i];
           vv[i] = vv[j];
           vv[j] = t;
         }
       }
       indx[j] = imax;
       if (j != N - 1) {
-        double d = 1.0 / M[j][j];
+        T d = T(1) / M[j][j];
 #pragma unroll
         for (int i = j + 1; i < N; ++i) M[i][j] *= d;
       }
@@ -175,11 +174,11 @@ __device__ __forceinline__ void block_solve(double (&M)[N][N], double (&C)[N][N]
         if (r2 == ip) {
 #pragma unroll
           for (int c = 0; c < N; ++c) {
-            double t = C[r2][c];
+            T t = C[r2][c];
             C[r2][c] = C[i][c];
             C[i][c] = t;
           }
-          double t = rhs[r2];
+          T t = rhs[r2];
           rhs[r2] = rhs[i];
           rhs[i] = t;
         }
@@ -199,7 +198,7 @@ __device__ __forceinline__ void block_solve(double (&M)[N][N], double (&C)[N][N]
         for (int c = 0; c < N; ++c) C[i][c] -= M[i][j] * C[j][c];
         rhs[i] -= M[i][j] * rhs[j];
       }
-      double d = 1. / M[i][i];
+      T d = T(1) / M[i][i];
 #pragma unroll
       for (int c = 0; c < N; ++c) C[i][c] *= d;
       rhs[i] *= d;
