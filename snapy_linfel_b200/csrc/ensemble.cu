@@ -100,7 +100,8 @@ __global__ void k_fill_u64(unsigned long long* p, int n, unsigned long long v) {
 // host plan
 // ---------------------------------------------------------------------------
 enum Phase {
-  PH_X1 = 0, PH_X2, PH_X3, PH_VCOL, PH_VFIN, PH_VFUSED, PH_BCU, PH_BCS, PH_CFL, PH_COUNT
+  PH_X1 = 0, PH_X1REV, PH_X2, PH_X3, PH_VCOL, PH_VFIN, PH_VFUSED, PH_BCU, PH_BCS, PH_CFL,
+  PH_COUNT
 };
 
 // vic_regs value of the tuning that selects the fused implicit-solve kernel
@@ -161,7 +162,7 @@ int plan(snapb_ensemble* e) {
     // x1: columns per tile
     size_t per = x1_smem32_per_column(g, nvt);
     int C = t.x1_columns > 0 ? t.x1_columns : (int)std::min<size_t>(16, (96 * 1024) / per);
-    C = std::max(1, std::min<int>(C, (int)((200 * 1024) / per)));
+    C = x1_columns_pow2(std::max(1, std::min<int>(C, (int)((200 * 1024) / per))));
     mb.x1_cols = C;
     e->x1_smem = std::max(e->x1_smem, per * C);
     int64_t ncol1 = (int64_t)g.nc2 * g.nc3;
@@ -177,6 +178,7 @@ int plan(snapb_ensemble* e) {
     mb.vic_cols = t.vic_block > 0 ? t.vic_block : 64;
     int64_t tiles[PH_COUNT] = {0};
     tiles[PH_X1] = e->a1 ? (ncol1 + C - 1) / C : 0;
+    tiles[PH_X1REV] = e->a1 && e->p.grav1 != 0. ? (ncol1 * 2 * g.ng + 255) / 256 : 0;
     tiles[PH_X2] = e->a2 ? ((lines2 + 127) / 128) * mb.nseg2 : 0;
     tiles[PH_X3] = e->a3 ? ((lines3 + 127) / 128) * mb.nseg3 : 0;
     tiles[PH_VCOL] = e->p.implicit_scheme ? (ncolv + mb.vic_cols - 1) / mb.vic_cols : 0;
@@ -387,8 +389,11 @@ int snapb_ensemble_stage_f32(snapb_ensemble* e, int stage, void* stream) {
   int last = e->a3 ? 3 : (e->a2 ? 2 : 1);
   if (e->a1) {
     ScopedTimer t(SNAPB_K_X1, st);
-    c = launch_x1_32_batch(mem, p, queue(e, PH_X1), stage, last == 1, pgrid(e, PH_X1),
-                           e->x1_smem, st);
+    if (p.grav1 != 0.)
+      c = launch_x1_ghost_revision32_batch(mem, p, queue(e, PH_X1REV), pgrid(e, PH_X1REV), st);
+    if (c == cudaSuccess)
+      c = launch_x1_32_batch(mem, p, queue(e, PH_X1), stage, last == 1, pgrid(e, PH_X1),
+                             e->x1_smem, st);
     if (c != cudaSuccess) return cuda_e(c, "ensemble x1");
   }
   if (e->a2) {

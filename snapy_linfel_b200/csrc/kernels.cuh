@@ -182,6 +182,10 @@ int vicf_tile_columns();
 cudaError_t launch_bc32_batch(const Member32* mem, const Phys& p, const WorkQueue& q, int kind,
                               double igm1, const PersistGrid& pg, cudaStream_t st);
 size_t x1_smem32_per_column(const Geo& g, int nvt);
+int x1_columns_pow2(int c);  // x1 tile width rounded down to a power of two
+cudaError_t launch_x1_ghost_revision32_batch(const Member32* mem, const Phys& p,
+                                             const WorkQueue& q, const PersistGrid& pg,
+                                             cudaStream_t st);
 StageBufs32 bufs32_of(const snapb_hydro_config& c, void* ws);
 size_t workspace_size_f32_of(const snapb_hydro_config& c);
 constexpr int kVicFinishCols = 32;    // columns per implicit-finish tile

@@ -153,100 +153,131 @@ __device__ __forceinline__ void cons2prim_pert(const float* u, float* w, float r
 // ---------------------------------------------------------------------------
 // x1 column kernel
 // ---------------------------------------------------------------------------
+// Shared memory per column: W' rows [NV][nc1], the full density row [nc1]
+// (rho_bar + rho', the reconstructed density) and the face flux rows [NV][nc1].
 size_t x1_smem32_per_column(const Geo& g, int nvt) {
-  return (size_t)(2 * nvt) * g.nc1 * sizeof(float);
+  return (size_t)(2 * nvt + 1) * g.nc1 * sizeof(float);
 }
 
-// One tile: columns col0 .. col0+C-1 of the block, smf = 2 * NV * nc1 * C floats.
-// Every thread of the CTA calls it (it synchronises the CTA).
+// Isentropic x1 ghost revision on full values, in FP64, written into W' of the
+// ghost cells (density and pressure rows).  The recurrence
+// p_{n+1} = (p_n^a + c)^(1/a) has h_n = p_n^a = p_e^a + n c, so every ghost
+// level is independent: one slot per (column, end, level), all columns of the
+// block (ghost columns included), slot = (col * 2 + top) * ng + n.  The x1
+// sweep reads these W' values for its ghost cells and leaves them in place.
+__device__ __forceinline__ void x1_ghost_revision32(const Geo& g, const Phys& p,
+                                                    const StageBufs32& b, int64_t slot) {
+  const int ng = g.ng;
+  const int64_t col = slot / (2 * ng);
+  const int rest = (int)(slot - col * 2 * ng);
+  const int top = rest / ng, n = rest - top * ng;
+  const int64_t sv = g.sv, cb = col * g.nc1;  // (k, j, 0) offset: s2 = nc1
+  const int e = top ? g.iu : g.il, dir = top ? 1 : -1;
+  float ue[5], we[5];
+#pragma unroll
+  for (int v = 0; v < 5; ++v) ue[v] = b.u[v * sv + cb + e];
+  cons2prim_pert(ue, we, b.rbf[e], (float)(p.gammad - 1.));
+  const double gam = p.gammad;
+  const double a = (gam - 1.) / gam, ig = 1. / gam, ia = 1. / a;
+  const double grav = -p.grav1, dz = g.dx1;
+  const double ps = b.pb[e] + we[IPR], rs = b.rb[e] + we[IDN];
+  const double K = ps / pow(rs, gam), kg = pow(K, ig);
+  const double step = (top ? -a : a) * grav * dz / kg;
+  const double h = pow(ps, a) + (n + 1) * step;
+  const double pn = pow(h, ia);
+  const double rn = pow(pn / K, ig);
+  const int cell = e + dir * (n + 1);  // ghosts only; the edge cell is never written
+  b.w[IPR * sv + cb + cell] = (float)(pn - b.pb[cell]);
+  b.w[IDN * sv + cb + cell] = (float)(rn - b.rb[cell]);
+}
+
+__global__ void __launch_bounds__(256) k_x1_ghost_revision32(Geo g, Phys p, StageBufs32 b) {
+  const int64_t slot = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot < (int64_t)g.nc2 * g.nc3 * 2 * g.ng) x1_ghost_revision32(g, p, b, slot);
+}
+
+// One tile: columns col0 .. col0+C-1 of the block (C a power of two dividing
+// the CTA size), smf = x1_smem32_per_column * C bytes.  Every thread of the CTA
+// calls it (it synchronises the CTA).  Threads are laid out tpc = nt / C per
+// column, so a thread's column and its cells follow from shifts and masks:
+//   (1) U' -> W' of the column's cells into shared memory, with W' and the
+//       scalar mixing ratios stored; ghost cells take density and pressure
+//       from the ghost revision (when gravity acts along x1);
+//   (2) the face states and fluxes, faces il .. iu of each column by its
+//       threads and face iu+1 of all columns by the first C threads;
+//   (3) the flux differences, then du or the RK combination (finalize32).
 template <int NS>
 __device__ __forceinline__ void x1_32_tile(const Geo& g, const Phys& p, const StageBufs32& b,
                                            int C, int last, int64_t col0, float* smf) {
   constexpr int NV = 5 + NS;
-  const int nc1 = g.nc1;
-  float* sw = smf;
-  float* sf = sw + (size_t)C * NV * nc1;
+  const int nc1 = g.nc1, ng = g.ng, il = g.il, iu = g.iu;
+  float* sw = smf;                              // [C][NV][nc1]
+  float* sr = sw + (size_t)C * NV * nc1;        // [C][nc1]
+  float* sf = sr + (size_t)C * nc1;             // [C][NV][nc1]
   const int64_t ncol = (int64_t)g.nc2 * g.nc3;
   const int tid = threadIdx.x, nt = blockDim.x;
+  const int lgC = __ffs(C) - 1, tpc = nt >> lgC;
+  const int c = tid / tpc, t = tid - c * tpc;  // this thread's column and rank in it
   const int64_t sv = g.sv;
   const float gm1 = (float)(p.gammad - 1.);
   const float gamma = (float)p.gammad;
+  const bool revise = p.grav1 != 0.;
 
-  for (int idx = tid; idx < C * nc1; idx += nt) {
-    int c = idx / nc1, i = idx - c * nc1;
-    int64_t col = col0 + c;
-    if (col >= ncol) continue;
-    int64_t off = col * nc1 + i;
+  // (1) interior cells of this thread's column, then the ghost cells of all
+  // columns (2 ng per column, spread over the CTA)
+  auto convert = [&](int cc, int i, bool ghost) {
+    const int64_t off = (col0 + cc) * nc1 + i;
     float uc[5], wc[5];
 #pragma unroll
     for (int v = 0; v < 5; ++v) uc[v] = b.u[v * sv + off];
     cons2prim_pert(uc, wc, b.rbf[i], gm1);
+    float* base = sw + (size_t)cc * NV * nc1;
+    if (ghost && revise) {  // density and pressure from the ghost revision
+      wc[IDN] = b.w[IDN * sv + off];
+      wc[IPR] = b.w[IPR * sv + off];
 #pragma unroll
-    for (int v = 0; v < 5; ++v) sw[(c * NV + v) * nc1 + i] = wc[v];
+      for (int v = IVX; v <= IVZ; ++v) b.w[v * sv + off] = wc[v];
+    } else {
+#pragma unroll
+      for (int v = 0; v < 5; ++v) b.w[v * sv + off] = wc[v];
+    }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) base[v * nc1 + i] = wc[v];
+    sr[(size_t)cc * nc1 + i] = b.rbf[i] + wc[IDN];
 #pragma unroll
     for (int n = 0; n < NS; ++n) {
       float rr = b.s[n * sv + off] / (b.rbf[i] + uc[IDN]);
-      sw[(c * NV + 5 + n) * nc1 + i] = rr;
+      base[(5 + n) * nc1 + i] = rr;
       b.R[n * sv + off] = rr;
     }
+  };
+  const bool col_ok = col0 + c < ncol;
+  if (col_ok)
+    for (int i = il + t; i <= iu; i += tpc) convert(c, i, false);
+  for (int idx = tid; idx < 2 * ng * C; idx += nt) {
+    const int cc = idx & (C - 1), k = idx >> lgC;
+    if (col0 + cc < ncol) convert(cc, k < ng ? k : iu + 1 + (k - ng), true);
   }
   __syncthreads();
 
-  // isentropic x1 ghost revision on full values, in FP64.  The recurrence
-  // p_{n+1} = (p_n^a + c)^(1/a) has h_n = p_n^a = p_e^a + n c, so every ghost
-  // level is independent: one thread per (column, end, level)
-  if (p.grav1 != 0. && tid < 2 * g.ng * C) {
-    const int c = tid / (2 * g.ng), rest = tid - c * 2 * g.ng;
-    const int top = rest / g.ng, n = rest - top * g.ng;
-    if (col0 + c < ncol) {
-      float* pp = sw + (c * NV + IPR) * nc1;
-      float* rr = sw + (c * NV + IDN) * nc1;
-      const double gam = p.gammad;
-      const double a = (gam - 1.) / gam, ig = 1. / gam, ia = 1. / a;
-      const double grav = -p.grav1, dz = g.dx1;
-      const int e = top ? g.iu : g.il, dir = top ? 1 : -1;
-      const double ps = b.pb[e] + pp[e], rs = b.rb[e] + rr[e];
-      const double K = ps / pow(rs, gam), kg = pow(K, ig);
-      const double step = (top ? -a : a) * grav * dz / kg;
-      const double h = pow(ps, a) + (n + 1) * step;
-      const double pn = pow(h, ia);
-      const double rn = pow(pn / K, ig);
-      const int cell = e + dir * (n + 1);  // ghosts only; the edge cell is never written
-      pp[cell] = (float)(pn - b.pb[cell]);
-      rr[cell] = (float)(rn - b.rb[cell]);
-    }
-  }
-  __syncthreads();
-
-  for (int idx = tid; idx < C * nc1; idx += nt) {
-    int c = idx / nc1, i = idx - c * nc1;
-    int64_t col = col0 + c;
-    if (col >= ncol) continue;
-    int64_t off = col * nc1 + i;
-#pragma unroll
-    for (int v = 0; v < 5; ++v) b.w[v * sv + off] = sw[(c * NV + v) * nc1 + i];
-  }
-
-  const int nf = g.nx1 + 1;
+  // (2) faces: the stencil f-3 .. f+2 stays inside the column (ng >= 3)
   const int ptype = (p.r1_shock) ? p.r1_type : interp2_of(p.r1_type);
-  for (int idx = tid; idx < C * nf; idx += nt) {
-    int c = idx / nf, f = g.il + (idx - c * nf);
-    int64_t col = col0 + c;
-    if (col >= ncol) continue;
-    int j = umod(col, g.nc2), k = udiv(col, g.nc2);
-    if (j < g.jl || j > g.ju || k < g.kl || k > g.ku) continue;
-    const float* base = sw + (size_t)c * NV * nc1;
+  auto interior = [&](int cc) {
+    const int64_t col = col0 + cc;
+    if (col >= ncol) return false;
+    const int j = umod(col, g.nc2), k = udiv(col, g.nc2);
+    return j >= g.jl && j <= g.ju && k >= g.kl && k <= g.ku;
+  };
+  auto face = [&](int cc, int f) {
+    const float* base = sw + (size_t)cc * NV * nc1 + f - 3;
+    const float* rho = sr + (size_t)cc * nc1 + f - 3;
     float L[NV], R[NV], F[NV];
     float pl, pr;
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
       float q[6];
 #pragma unroll
-      for (int t = 0; t < 6; ++t) {
-        int cell = min(max(f - 3 + t, 0), nc1 - 1);
-        q[t] = base[v * nc1 + cell];
-        if (v == IDN) q[t] += b.rbf[cell];  // density reconstructed as a full field
-      }
+      for (int s6 = 0; s6 < 6; ++s6) q[s6] = v == IDN ? rho[s6] : base[v * nc1 + s6];
       if (v == IPR) {
         face_states<float>(ptype, p.r1_scale != 0, q, pl, pr);
         pl += b.offL[f];
@@ -260,12 +291,12 @@ __device__ __forceinline__ void x1_32_tile(const Geo& g, const Phys& p, const St
         R[v] = R[v] < 0.f ? 0.f : R[v];
       }
     }
-    if (p.grav1 != 0.) {
-      if (f == g.il) {
+    if (revise) {
+      if (f == il) {
         pl = pr;
         L[IDN] = R[IDN];
       }
-      if (f == g.iu + 1) {
+      if (f == iu + 1) {
         pr = pl;
         R[IDN] = L[IDN];
       }
@@ -282,28 +313,29 @@ __device__ __forceinline__ void x1_32_tile(const Geo& g, const Phys& p, const St
 #pragma unroll
     for (int n = 0; n < NS; ++n) F[5 + n] = F[IDN] > 0.f ? F[IDN] * L[5 + n] : F[IDN] * R[5 + n];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) sf[(c * NV + v) * nc1 + f] = F[v];
-  }
+    for (int v = 0; v < NV; ++v) sf[((size_t)cc * NV + v) * nc1 + f] = F[v];
+  };
+  const bool mine = interior(c);
+  if (mine)
+    for (int f = il + t; f <= iu; f += tpc) face(c, f);
+  for (int cc = tid; cc < C; cc += nt)
+    if (interior(cc)) face(cc, iu + 1);
   __syncthreads();
 
+  // (3) flux differences of this thread's column
+  if (!mine) return;
   const float A1 = (float)g.A1;
-  for (int idx = tid; idx < C * g.nx1; idx += nt) {
-    int c = idx / g.nx1, i = g.il + (idx - c * g.nx1);
-    int64_t col = col0 + c;
-    if (col >= ncol) continue;
-    int j = umod(col, g.nc2), k = udiv(col, g.nc2);
-    if (j < g.jl || j > g.ju || k < g.kl || k > g.ku) continue;
-    int64_t off = col * nc1 + i;
+  const float* fc = sf + (size_t)c * NV * nc1;
+  const float* wcol = sw + (size_t)c * NV * nc1;
+  for (int i = il + t; i <= iu; i += tpc) {
+    const int64_t off = (col0 + c) * nc1 + i;
     float d[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      const float* fv = sf + (c * NV + v) * nc1;
-      d[v] = A1 * fv[i + 1] - A1 * fv[i];
-    }
+    for (int v = 0; v < NV; ++v) d[v] = A1 * fc[v * nc1 + i + 1] - A1 * fc[v * nc1 + i];
     if (last) {
       float wc[5];
 #pragma unroll
-      for (int v = 0; v < 5; ++v) wc[v] = sw[(c * NV + v) * nc1 + i];
+      for (int v = 0; v < 5; ++v) wc[v] = wcol[v * nc1 + i];
       finalize32<NS>(g, p, b, off, i, d, wc);
     } else {
 #pragma unroll
@@ -593,14 +625,27 @@ template <int NS>
 __global__ void __launch_bounds__(256, 4) k_x1_32_batch(const Member32* __restrict__ mem, Phys p,
                                                      WorkQueue q, int stage, int last) {
   extern __shared__ float smf[];
+  __shared__ Member32 s_mem;  // the member's descriptor, read as the tile needs its fields
+  int m;
+  int64_t tile;
+  while (queue_next(q, m, tile)) {  // (starts with a barrier: the last tile is done)
+    load_member(s_mem, mem, m);
+    if (threadIdx.x == 0) set_stage32(s_mem.b, stage);
+    __syncthreads();
+    const int C = s_mem.x1_cols;
+    x1_32_tile<NS>(s_mem.g, p, s_mem.b, C, last, tile * C, smf);
+  }
+}
+
+// the x1 ghost revision of every member, 256 slots per tile
+__global__ void __launch_bounds__(256) k_x1_ghost_revision32_batch(const Member32* __restrict__ mem,
+                                                                   Phys p, WorkQueue q) {
   int m;
   int64_t tile;
   while (queue_next(q, m, tile)) {
-    const Geo g = mem[m].g;
-    StageBufs32 b = mem[m].b;
-    set_stage32(b, stage);
-    const int C = mem[m].x1_cols;
-    x1_32_tile<NS>(g, p, b, C, last, tile * C, smf);
+    const Geo& g = mem[m].g;
+    const int64_t slot = tile * blockDim.x + threadIdx.x;
+    if (slot < (int64_t)g.nc2 * g.nc3 * 2 * g.ng) x1_ghost_revision32(g, p, mem[m].b, slot);
   }
 }
 
@@ -663,6 +708,14 @@ cudaError_t launch_x1_32_batch(const Member32* mem, const Phys& p, const WorkQue
   return cudaGetLastError();
 }
 
+cudaError_t launch_x1_ghost_revision32_batch(const Member32* mem, const Phys& p,
+                                             const WorkQueue& q, const PersistGrid& pg,
+                                             cudaStream_t st) {
+  k_x1_ghost_revision32_batch<<<persistent_grid(k_x1_ghost_revision32_batch, 256, 0, pg), 256, 0,
+                                st>>>(mem, p, q);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_march32_batch(int axis, const Member32* mem, const Phys& p,
                                  const WorkQueue& q, int stage, bool first, bool last,
                                  const PersistGrid& pg, cudaStream_t st) {
@@ -703,10 +756,24 @@ cudaError_t launch_ref32(const Geo& g, const Phys& p, const double* rb, const do
   return cudaGetLastError();
 }
 
+// columns per x1 tile: a power of two (the tile's thread layout), at most 16
+// and about 96 KB of shared memory
+int x1_columns_pow2(int c) {
+  c = std::max(1, std::min(c, 32));
+  while (c & (c - 1)) c &= c - 1;
+  return c;
+}
 int x1_columns_per_cta32(const Geo& g, int nvt) {
   size_t per = x1_smem32_per_column(g, nvt);
-  int c = (int)std::max<size_t>(1, (96 * 1024) / per);
-  return std::min(c, 16);
+  return x1_columns_pow2((int)std::min<size_t>(16, std::max<size_t>(1, (96 * 1024) / per)));
+}
+
+cudaError_t launch_x1_ghost_revision32(const Geo& g, const Phys& p, const StageBufs32& b,
+                                       cudaStream_t st) {
+  if (p.grav1 == 0.) return cudaSuccess;
+  const int64_t n = (int64_t)g.nc2 * g.nc3 * 2 * g.ng;
+  k_x1_ghost_revision32<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g, p, b);
+  return cudaGetLastError();
 }
 
 template <int NS>
@@ -717,6 +784,8 @@ static cudaError_t launch_x1_32t(const Geo& g, const Phys& p, const StageBufs32&
   size_t smem = (size_t)C * x1_smem32_per_column(g, nvt);
   if (smem > 200 * 1024) return cudaErrorInvalidConfiguration;
   raise_smem_limit(k_x1_32<NS>, 200 * 1024);
+  cudaError_t e = launch_x1_ghost_revision32(g, p, b, st);
+  if (e != cudaSuccess) return e;
   int64_t ncol = (int64_t)g.nc2 * g.nc3;
   k_x1_32<NS><<<(unsigned)((ncol + C - 1) / C), 256, smem, st>>>(g, p, b, C, last ? 1 : 0);
   return cudaGetLastError();
