@@ -33,7 +33,6 @@ __device__ __forceinline__ double ring_elem(const double* slot, const double*) {
 __device__ __forceinline__ double ring_elem(const double* slot, const float*) {
   return (double)*reinterpret_cast<const float*>(slot);
 }
-__device__ __forceinline__ double ring_elem(const float* slot, const float*) { return *slot; }
 
 // Slot-element address of this thread in a ring of E elements per slot.
 struct Ring {

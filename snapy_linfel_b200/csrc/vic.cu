@@ -100,11 +100,9 @@ struct BackRing {
   static constexpr int depth = N == 3 ? 4 : 2;
   static constexpr int elems = N * N + N + 1;
 };
-// RT: ring element type, the scratch precision of the solve (FP32 slots
-// leave the L1 share of the SM's shared-memory carveout twice as large)
-template <int N, class RT = double>
+template <int N>
 constexpr size_t back_ring_bytes(int threads) {
-  return (size_t)threads * BackRing<N>::depth * BackRing<N>::elems * sizeof(RT);
+  return (size_t)threads * BackRing<N>::depth * BackRing<N>::elems * sizeof(double);
 }
 
 
@@ -175,24 +173,9 @@ __device__ __forceinline__ double vic_full_rho(const StageBufs32& b, double u_rh
   return u_rho + b.rb[xi];
 }
 
-// Precision of the elimination and of its scratch per form and block size:
-// FP64 for the FP64 plain form; for the FP32 perturbation form (whose blocks
-// |A| and J are formed in FP32 from the full states) FP32 for N = 3 and FP64
-// for N = 5.  The block systems are diagonally dominant (the 1/dt diagonal
-// over upwind-split off-diagonal blocks, |A| +- J >= 0 in the characteristic
-// basis), so an FP32 elimination does not amplify its rounding; the N = 3
-// cofactor solve has a fixed operation order, while the pivoted N = 5 LU in
-// FP32 meets near-ties in the pivot choice, where one-ulp differences of the
-// compiled kernels (one-block and batched) would select different rows.  The
-// MS-VIC column sums are accumulated in FP64 in every case.
-template <int N, class T>  // T: stored precision of the state
-using VicScratchT = std::conditional_t<N == 3 && std::is_same_v<T, float>, float, double>;
-template <class B, int N>
-struct VicPrec {
-  using T = VicScratchT<N, std::remove_pointer_t<decltype(std::declval<B>().u)>>;
-};
-
-// Block construction per form, in the elimination precision
+// Block construction per form: the FP64 plain form in FP64; the FP32
+// perturbation form forms |A| and J in FP32 from the full states (only the
+// elimination and the balance terms stay FP64 there) and widens them.
 template <int N>
 __device__ __forceinline__ void absA_of(const StageBufs&, double gm1, const double* wl,
                                         const double* wr, double (&A)[N][N]) {
@@ -202,6 +185,37 @@ template <int N>
 __device__ __forceinline__ void jac_of(const StageBufs&, double gm1, const double* w,
                                        double (&J)[N][N]) {
   jac_block<N>(gm1, w, J);
+}
+// Precision of the blocks (|A|, J and the assembled a, b, c) per form: FP64
+// for the FP64 plain form, FP32 for the FP32 perturbation form, whose states
+// are FP32.  The elimination, the back substitution and the scratch stay FP64
+// in both forms: the assembled blocks are widened before they enter it.
+template <class B>
+struct BlockPrec {
+  using T = double;
+};
+template <>
+struct BlockPrec<StageBufs32> {
+  using T = float;
+};
+template <int N>
+__device__ __forceinline__ void absA_of(const StageBufs32&, double gm1, const double* wl,
+                                        const double* wr, float (&A)[N][N]) {
+  float fl[5], fr[5];
+#pragma unroll
+  for (int v = 0; v < 5; ++v) {
+    fl[v] = (float)wl[v];
+    fr[v] = (float)wr[v];
+  }
+  absA_block<N, float>((float)gm1, fl, fr, A);
+}
+template <int N>
+__device__ __forceinline__ void jac_of(const StageBufs32&, double gm1, const double* w,
+                                       float (&J)[N][N]) {
+  float fw[5];
+#pragma unroll
+  for (int v = 0; v < 5; ++v) fw[v] = (float)w[v];
+  jac_block<N, float>((float)gm1, fw, J);
 }
 template <int N>
 __device__ __forceinline__ void absA_of(const StageBufs32&, double gm1, const double* wl,
@@ -230,20 +244,6 @@ __device__ __forceinline__ void jac_of(const StageBufs32&, double gm1, const dou
 #pragma unroll
     for (int q = 0; q < N; ++q) J[r][q] = (double)F[r][q];
 }
-template <int N>
-__device__ __forceinline__ void absA_of(const StageBufs32&, double gm1, const float* wl,
-                                        const float* wr, float (&A)[N][N]) {
-  absA_block<N, float>((float)gm1, wl, wr, A);
-}
-template <int N>
-__device__ __forceinline__ void jac_of(const StageBufs32&, double gm1, const float* w,
-                                       float (&J)[N][N]) {
-  jac_block<N, float>((float)gm1, w, J);
-}
-// right-hand side du / dt of one row: the FP64 form divides as the reference
-// does; the FP32 form multiplies by 1/dt
-__device__ __forceinline__ double vic_rhs(double d, double dt, double) { return d / dt; }
-__device__ __forceinline__ float vic_rhs(double d, double, float idt) { return (float)d * idt; }
 
 // One layer of the block-Thomas forward elimination: a_i, b_i, c_i from |A|
 // at the layer's lower / upper faces (Am, Ap) and J of the cells below /
@@ -365,32 +365,32 @@ __device__ __forceinline__ void vic_back(const B& b, double* S, double* Z, int64
 template <int N, class B>
 __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B& b, int64_t col) {
   constexpr int ES = VicDims<N>::ES;
-  using ET = typename VicPrec<B, N>::T;  // elimination and scratch precision
+  using BT = typename BlockPrec<B>::T;  // precision of the blocks and their assembly
   const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
   if (col >= ncol) return;
   const int nl = g.nx1;
   const int64_t sv = g.sv;
   const int64_t cb = column_base(g, col);
-  ET* S = reinterpret_cast<ET*>(b.vic) + col;  // [nl][ES][ncol] in ET
-  double* Z = b.vic + (int64_t)nl * ES * ncol + col;
-  auto Sat = [&](int i, int e) -> ET& { return S[((int64_t)i * ES + e) * ncol]; };
-  auto load_w = [&](int i, ET* w) {
+  double* S = b.vic + col;
+  double* Z = S + (int64_t)nl * ES * ncol;
+  auto Sat = [&](int i, int e) -> double& { return S[((int64_t)i * ES + e) * ncol]; };
+  auto load_w = [&](int i, double* w) {
 #pragma unroll
-    for (int v = 0; v < 5; ++v) w[v] = (ET)vic_w(b, sv, v, cb + i, g.il + i);
+    for (int v = 0; v < 5; ++v) w[v] = vic_w(b, sv, v, cb + i, g.il + i);
   };
   const double gm1c = p.gammad - 1.;
   const double gm1f = 0.5 * (p.gammad + p.gammad) - 1.;
-  const double dt = *b.dt, V = g.vol;
-  const ET Aa = (ET)g.A1, hiv = (ET)(0.5 / g.vol), idt = (ET)(1. / dt), grav = (ET)p.grav1;
+  const double dt = *b.dt;
+  const double V = g.vol;
+  const BT Aa = (BT)g.A1, hiv = (BT)(0.5 / g.vol), idt = (BT)(1. / dt), grav = (BT)p.grav1;
   // Forward sweep inputs (w of cell L and the rows of du at layer L-1,
   // 1 <= L <= nl) arrive kFwdDepth layers ahead through the same per-thread
   // shared-memory ring as the back substitution, layout [slot][element][thread].
   constexpr int DF = kFwdDepth, FE = 5 + N;
   static_assert(DF * FE <= BackRing<N>::depth * BackRing<N>::elems, "ring too small");
   extern __shared__ double vic_ring[];
-  ET* const ringb = reinterpret_cast<ET*>(vic_ring);  // slots in the scratch precision
   const int nt = blockDim.x, lane = threadIdx.x;
-  auto fring = [&](int slot, int e) { return ringb + ((size_t)(slot * FE + e) * nt + lane); };
+  auto fring = [&](int slot, int e) { return vic_ring + ((size_t)(slot * FE + e) * nt + lane); };
   auto ffetch = [&](int L, int slot) {
     if (L <= nl) {
 #pragma unroll
@@ -403,8 +403,9 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
   };
 #pragma unroll
   for (int k = 0; k < DF; ++k) ffetch(1 + k, k);
-  ET wc[5], wn[5];
-  ET Am[N][N], Jp[N][N], Jc[N][N], ap[N][N], dp[N];
+  double wc[5], wn[5];
+  BT Am[N][N], Jp[N][N], Jc[N][N];
+  double ap[N][N], dp[N];
   load_w(-1, wn);
   jac_of<N>(b, gm1c, wn, Jp);
   load_w(0, wc);
@@ -412,51 +413,62 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
   jac_of<N>(b, gm1c, wc, Jc);
   double sum_a2 = 0.;
   for (int i = 0, fslot = 0; i < nl; ++i) {
-    ET Ap[N][N], Jn[N][N], rhs[N];
+    BT Ap[N][N], Jn[N][N];
+    double rhs[N];
     cp_async_wait<DF - 1>();  // the group of cell i+1 has landed
 #pragma unroll
     for (int v = 0; v < 5; ++v)  // cell i+1 (the ghost cell nl at the top)
-      wn[v] = (ET)vic_full(b, ring_elem(fring(fslot, v), b.w), v, g.il + i + 1);
+      wn[v] = vic_full(b, ring_elem(fring(fslot, v), b.w), v, g.il + i + 1);
 #pragma unroll
-    for (int r = 0; r < N; ++r) rhs[r] = vic_rhs(ring_elem(fring(fslot, 5 + r), b.D), dt, idt);
+    for (int r = 0; r < N; ++r) rhs[r] = ring_elem(fring(fslot, 5 + r), b.D) / dt;
     absA_of<N>(b, gm1f, wc, wn, Ap);
     jac_of<N>(b, gm1c, wn, Jn);
-    double ai = (double)wc[IDN] * V;
+    double ai = wc[IDN] * V;
     sum_a2 += ai * ai;
-    ET a[N][N], bb[N][N], c[N][N];
+    // assembly in the block precision, then widened for the elimination
+    BT af[N][N], bf[N][N], cf[N][N];
 #pragma unroll
     for (int r = 0; r < N; ++r)
 #pragma unroll
       for (int q = 0; q < N; ++q) {
-        ET phi = 0.;
+        BT phi = BT(0);
         if (r == 1 && q == 0) phi = grav;
         if (N == 3 && r == 2 && q == 1) phi = grav;
         if (N == 5 && r == IPR && q == IVX) phi = grav;
-        a[r][q] = (Am[r][q] * Aa + Ap[r][q] * Aa) * hiv - phi;
-        bb[r][q] = -(Am[r][q] + Jp[r][q]) * Aa * hiv;
-        c[r][q] = -(Ap[r][q] - Jn[r][q]) * Aa * hiv;
+        af[r][q] = (Am[r][q] * Aa + Ap[r][q] * Aa) * hiv - phi;
+        bf[r][q] = -(Am[r][q] + Jp[r][q]) * Aa * hiv;
+        cf[r][q] = -(Ap[r][q] - Jn[r][q]) * Aa * hiv;
       }
 #pragma unroll
-    for (int r = 0; r < N; ++r) a[r][r] += idt;
+    for (int r = 0; r < N; ++r) af[r][r] += idt;
     if (i == 0) {
 #pragma unroll
       for (int r = 0; r < N; ++r)
 #pragma unroll
-        for (int q = 0; q < N; ++q) a[r][q] += bb[r][q] * (q == 1 ? ET(-1) : ET(1));
+        for (int q = 0; q < N; ++q) af[r][q] += bf[r][q] * (q == 1 ? BT(-1) : BT(1));
     }
     if (i == nl - 1) {
 #pragma unroll
       for (int r = 0; r < N; ++r)
 #pragma unroll
-        for (int q = 0; q < N; ++q) a[r][q] += c[r][q] * (q == 1 ? ET(-1) : ET(1));
+        for (int q = 0; q < N; ++q) af[r][q] += cf[r][q] * (q == 1 ? BT(-1) : BT(1));
     }
+    double a[N][N], bb[N][N], c[N][N];
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        a[r][q] = (double)af[r][q];
+        bb[r][q] = (double)bf[r][q];
+        c[r][q] = (double)cf[r][q];
+      }
     if (i > 0) {
 #pragma unroll
       for (int r = 0; r < N; ++r) {
-        ET bd = 0.;
+        double bd = 0.;
 #pragma unroll
         for (int q = 0; q < N; ++q) {
-          ET t = 0.;
+          double t = 0.;
 #pragma unroll
           for (int kk = 0; kk < N; ++kk) t += bb[r][kk] * ap[kk][q];
           a[r][q] -= t;
@@ -494,36 +506,36 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
   // way, the inputs of each layer arriving through the shared-memory ring.
   constexpr int DB = BackRing<N>::depth, RE = BackRing<N>::elems;
   cp_async_wait<0>();  // the forward ring is drained before its memory is reused
-  auto ring = [&](int slot, int e) { return ringb + ((size_t)(slot * RE + e) * nt + lane); };
+  auto ring = [&](int slot, int e) { return vic_ring + ((size_t)(slot * RE + e) * nt + lane); };
   auto fetch = [&](int i, int slot) {
     if (i >= 0) {
 #pragma unroll
-      for (int e = 0; e < ES; ++e) cp_async_elem(ring(slot, e), &Sat(i, e));
+      for (int e = 0; e < ES; ++e) cp_async_bytes8(ring(slot, e), &Sat(i, e));
       cp_async_elem(ring(slot, ES), b.D + IDN * sv + cb + i);
     }
     cp_async_commit();
   };
-  ET dn[N];
+  double dn[N];
 #pragma unroll
   for (int r = 0; r < N; ++r) dn[r] = dp[r];
-  double b_dry = (vic_d(b, IDN * sv + cb + nl - 1) - (double)dn[0]) * 1. * V;
+  double b_dry = (vic_d(b, IDN * sv + cb + nl - 1) - dn[0]) * 1. * V;
 #pragma unroll
   for (int k = 0; k < DB; ++k) fetch(nl - 2 - k, k);
   for (int i = nl - 2, slot = 0; i >= 0; --i) {
     cp_async_wait<DB - 1>();  // the group of layer i has landed
-    ET cur[ES];
+    double cur[ES];
 #pragma unroll
-    for (int e = 0; e < ES; ++e) cur[e] = (ET)ring_elem(ring(slot, e), S);
+    for (int e = 0; e < ES; ++e) cur[e] = *ring(slot, e);
     const double dcur = ring_elem(ring(slot, ES), b.D);
-    ET d[N];
+    double d[N];
 #pragma unroll
     for (int r = 0; r < N; ++r) {
-      ET t = 0.;
+      double t = 0.;
 #pragma unroll
       for (int q = 0; q < N; ++q) t += cur[r * N + q] * dn[q];
       d[r] = cur[N * N + r] - t;
     }
-    b_dry += (dcur - (double)d[0]) * 1. * V;
+    b_dry += (dcur - d[0]) * 1. * V;
     fetch(i - DB, slot);  // the slot's values are consumed: refill it
     slot = slot + 1 == DB ? 0 : slot + 1;
 #pragma unroll
@@ -684,37 +696,26 @@ template <int N, class B>
 __global__ void __launch_bounds__(128) k_vic_column(Geo g, Phys p, B b) {
   vic_column<N, B>(g, p, b, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
 }
-// the FP32 form's N = 3 sweep (FP32 elimination): its 128-register build
-// serialises the next layer's block formation behind the elimination, so it
-// takes the register budget of one resident CTA
-__global__ void __launch_bounds__(128, 1) k_vic_column32_n3(Geo g, Phys p, StageBufs32 b) {
-  vic_column<3, StageBufs32>(g, p, b, (int64_t)blockIdx.x * blockDim.x + threadIdx.x);
-}
 
 // (3) redistribution + RK combination (or du), tiles of 32 columns x 32
 // layers: delta is transposed through shared memory so that the state
 // arrays are read and written along x1.
 // one tile: columns col0 .. col0+kTC-1, layers i0 .. i0+kTL-1 (whole CTA)
 // Shared memory of one finish tile: the back-substituted solution rows
-// [N][kTC][kTL+1] in the scratch precision of the solve, the column sums and
-// offsets, then the tile's cell inputs [element][kTC][kTL] in the stored
-// precision T.  Cell inputs: w'[IDN], the du
-// rows the solve does not replace, and (RK update) u, u0, and per scalar s,
-// s0, r and its du row.
+// [N][kTC][kTL+1] (doubles), the column sums and offsets, then the tile's cell
+// inputs [element][kTC][kTL] in the stored precision T: w'[IDN], the du rows
+// the solve does not replace, and (RK update) u, u0, and per scalar s, s0, r
+// and its du row.
 template <int N, int NS>
 struct FinSmem {
   static constexpr int TL = 16;  // layers per staged tile
   static constexpr int du_rows = N == 3 ? 3 : 1;           // IDN (+ IVY, IVZ)
   static constexpr int elems = 1 + du_rows + 10 + 4 * NS;  // upper bound
-  template <class T>
-  static constexpr size_t head() {  // (N kTC (TL+1) 4 is a multiple of 8)
-    return (size_t)N * kTC * (TL + 1) * sizeof(VicScratchT<N, T>) + 3 * kTC * sizeof(double);
-  }
+  static constexpr size_t head = ((size_t)N * kTC * (TL + 1) + 3 * kTC) * sizeof(double);
 };
 template <int N, int NS, class T>
 constexpr size_t finish_smem_bytes() {
-  return FinSmem<N, NS>::template head<T>() +
-         (size_t)FinSmem<N, NS>::elems * kTC * FinSmem<N, NS>::TL * sizeof(T);
+  return FinSmem<N, NS>::head + (size_t)FinSmem<N, NS>::elems * kTC * FinSmem<N, NS>::TL * sizeof(T);
 }
 
 // One tile: columns col0 .. col0+kTC-1, layers i0 .. i0+kTL-1 (whole CTA).
@@ -727,18 +728,17 @@ __device__ __forceinline__ void vic_finish_tile_staged(const Geo& g, const Phys&
                                                 int64_t col0, int i0) {
   constexpr int ES = VicDims<N>::ES, DR = FinSmem<N, NS>::du_rows, kTL = FinSmem<N, NS>::TL;
   using T = std::remove_pointer_t<decltype(b.u)>;  // stored precision (FP32 / FP64)
-  using ET = typename VicPrec<B, N>::T;              // scratch precision of the solve
   const int nl = g.nx1;
   const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
   const int64_t sv = g.sv;
-  const ET* S = reinterpret_cast<const ET*>(b.vic);
-  const double* Z = b.vic + (int64_t)nl * ES * ncol;
+  const double* S = b.vic;
+  const double* Z = S + (int64_t)nl * ES * ncol;
   extern __shared__ double fin_smem[];
-  ET* dl = reinterpret_cast<ET*>(fin_smem);                  // [N][kTC][kTL+1]
-  double* zs = reinterpret_cast<double*>(dl + (size_t)N * kTC * (kTL + 1));  // [2][kTC]
+  double* dl = fin_smem;                                     // [N][kTC][kTL+1]
+  double* zs = dl + (size_t)N * kTC * (kTL + 1);             // [2][kTC]
   int64_t* cbs = reinterpret_cast<int64_t*>(zs + 2 * kTC);   // [kTC]
   T* cell = reinterpret_cast<T*>(cbs + kTC);                 // [element][kTC][kTL]
-  auto DL = [&](int r, int c, int s) -> ET& {
+  auto DL = [&](int r, int c, int s) -> double& {
     return dl[((size_t)r * kTC + c) * (kTL + 1) + s];
   };
   auto CE = [&](int e, int c, int s) -> T* { return cell + ((size_t)e * kTC + c) * kTL + s; };
@@ -770,7 +770,7 @@ __device__ __forceinline__ void vic_finish_tile_staged(const Geo& g, const Phys&
 #pragma unroll
       for (int j = 0; j < CPT; ++j) {
         const int idx = tid + j * kFinThreads;
-        if (sok[j]) cp_async_elem(&DL(r, idx % kTC, idx / kTC), S + soff[j] + (int64_t)r * ncol);
+        if (sok[j]) cp_async_bytes8(&DL(r, idx % kTC, idx / kTC), S + soff[j] + (int64_t)r * ncol);
       }
   }
   // cell inputs, layers fastest (the state arrays run along x1)
@@ -864,13 +864,12 @@ template <int N, int NS, class B, int NT, int kTL>
 __device__ __forceinline__ void vic_finish_tile_regs(const Geo& g, const Phys& p, const B& b,
                                                 int64_t col0, int i0) {
   constexpr int ES = VicDims<N>::ES;
-  using ET = typename VicPrec<B, N>::T;  // scratch precision of the solve
   const int nl = g.nx1;
   const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
   const int64_t sv = g.sv;
-  const ET* S = reinterpret_cast<const ET*>(b.vic);
-  const double* Z = b.vic + (int64_t)nl * ES * ncol;
-  __shared__ ET dl[N][kTC][kTL + 1];
+  const double* S = b.vic;
+  const double* Z = S + (int64_t)nl * ES * ncol;
+  __shared__ double dl[N][kTC][kTL + 1];
   __shared__ double zs[2][kTC];
   __shared__ int64_t cbs[kTC];  // (k, j, il) offsets of the tile's columns
   const int tid = threadIdx.x;
@@ -879,7 +878,7 @@ __device__ __forceinline__ void vic_finish_tile_regs(const Geo& g, const Phys& p
     int s = rest % kTL, r = rest / kTL;
     int64_t col = col0 + c;
     int i = i0 + s;
-    dl[r][c][s] = (col < ncol && i < nl) ? S[((int64_t)i * ES + N * N + r) * ncol + col] : ET(0);
+    dl[r][c][s] = (col < ncol && i < nl) ? S[((int64_t)i * ES + N * N + r) * ncol + col] : 0.;
   }
   if (tid < 2 * kTC) {
     int c = tid % kTC, k = tid / kTC;
@@ -1025,14 +1024,9 @@ static cudaError_t launch_vic_n(const Geo& g, const Phys& p, const B& b, cudaStr
     }
   }
   if (!split) {
-    const unsigned grid = (unsigned)((ncol + bs - 1) / bs);
-    if constexpr (N == 3 && std::is_same_v<B, StageBufs32>) {
-      allow_ring_smem(k_vic_column32_n3, back_ring_bytes<N, float>(128));
-      k_vic_column32_n3<<<grid, bs, back_ring_bytes<N, float>(bs), st>>>(g, p, b);
-    } else {
-      allow_ring_smem(k_vic_column<N, B>, back_ring_bytes<N>(128));
-      k_vic_column<N, B><<<grid, bs, back_ring_bytes<N>(bs), st>>>(g, p, b);
-    }
+    allow_ring_smem(k_vic_column<N, B>, back_ring_bytes<N>(128));
+    k_vic_column<N, B><<<(unsigned)((ncol + bs - 1) / bs), bs, back_ring_bytes<N>(bs), st>>>(
+        g, p, b);
   }
   using T = std::remove_pointer_t<decltype(b.u)>;
 #define SNAPB_VF(NS)                                                   \
@@ -1130,9 +1124,8 @@ __global__ void __launch_bounds__(FinCfg<N, NS, float>::threads,
 template <int N, int V>
 static void launch_vcb(const Member32* mem, const Phys& p, const WorkQueue& q, int stage,
                        const PersistGrid& pg, int block, cudaStream_t st) {
-  using RT = VicScratchT<N, float>;
-  const size_t smem = back_ring_bytes<N, RT>(block);
-  allow_ring_smem(k_vic_column_batch<N, V>, back_ring_bytes<N, RT>(128));
+  const size_t smem = back_ring_bytes<N>(block);
+  allow_ring_smem(k_vic_column_batch<N, V>, back_ring_bytes<N>(128));
   k_vic_column_batch<N, V><<<persistent_grid(k_vic_column_batch<N, V>, block, smem, pg), block,
                              smem, st>>>(mem, p, q, stage);
 }
