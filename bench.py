@@ -486,6 +486,20 @@ def run_adjoint_timing(args, opts, state, cells, stream, barrier):
     e1.record(stream)
     barrier()
     roll_bwd_ms = e0.elapsed_time(e1) / nsteps
+    del x, uT
+    # the same rollout keeping every step's stage inputs (no re-run backwards)
+    x = u0.clone().requires_grad_(True)
+    barrier()
+    e0.record(stream)
+    uT, _ = rollout(opts, x, s0, dts, checkpoint_every=0, runner=runner)
+    e1.record(stream)
+    barrier()
+    keep_fwd_ms = e0.elapsed_time(e1) / nsteps
+    e0.record(stream)
+    uT.backward(torch.ones_like(uT) * 1e-3)
+    e1.record(stream)
+    barrier()
+    keep_bwd_ms = e0.elapsed_time(e1) / nsteps
     del x, uT, runner, adj
     torch.cuda.empty_cache()
     return {"steps": nsteps, "forward_ms_per_step": fwd_ms, "reverse_ms_per_step": rev_ms,
@@ -494,6 +508,10 @@ def run_adjoint_timing(args, opts, state, cells, stream, barrier):
                              "backward_ms_per_step": roll_bwd_ms,
                              "backward_over_forward": roll_bwd_ms / roll_fwd_ms,
                              "checkpoint_every": nsteps},
+            "stage_inputs_kept": {"forward_ms_per_step": keep_fwd_ms,
+                                  "backward_ms_per_step": keep_bwd_ms,
+                                  "backward_over_forward": keep_bwd_ms / fwd_ms,
+                                  "memory": "3 states per step kept by the forward pass"},
             "reverse_kernel_ms_per_stage": kern, "dtype": "f64",
             "value": cells * 3 / (rev_ms / 1e3) / 1e6, "unit": "Mcell-updates/s (reverse)"}
 
@@ -501,11 +519,14 @@ def run_adjoint_timing(args, opts, state, cells, stream, barrier):
 def ensemble_launches_per_step(cfg, tuning=None) -> int:
     """kernels of one batched step: CFL fill + reduce + final, then per stage
     the x1 ghost revision (gravity along x1), the x1, x2, x3 sweeps, the
-    implicit solve (column + finish, or the fused kernel) and the boundary
-    fill(s)"""
-    fused = bool(tuning) and tuning.get("vic_regs") == 3
+    implicit solve (one cyclic-reduction or fused launch, or column + finish)
+    and the boundary fill(s)"""
+    kernel = (tuning or {}).get("vic_kernel", 0)
+    cyclic = (kernel == 1 and cfg.implicit_scheme and not (cfg.implicit_scheme >> 3) & 1
+              and cfg.nx1 <= 256)
+    vic = 1 if kernel == 2 or cyclic else 2
     per_stage = (1 + int(cfg.grav1 != 0) + int(cfg.nx2 > 1) + int(cfg.nx3 > 1) +
-                 ((1 if fused else 2) if cfg.implicit_scheme else 0) + 1 + int(cfg.nscalar > 0))
+                 (vic if cfg.implicit_scheme else 0) + 1 + int(cfg.nscalar > 0))
     return 3 + 3 * per_stage
 
 
@@ -1131,7 +1152,7 @@ def main():
                     help="skip the 384 x 384 x 192 FP32/FP64 comparison of the ensemble line")
     ap.add_argument("--tuning", default="",
                     help="fixed ensemble tile shapes instead of the autotuner, "
-                         "e.g. x1_columns=8,march_segment=16,vic_block=32,vic_regs=0")
+                         "e.g. x1_columns=8,march_segment=16,vic_kernel=0,vic_block=32,vic_regs=0")
     ap.add_argument("--adj-steps", type=int, default=2)
     ap.add_argument("--adj-nsteps", type=int, default=200)
     ap.add_argument("--adj-every", type=int, default=20)

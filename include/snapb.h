@@ -295,14 +295,17 @@ typedef struct snapb_member_f32 {
   size_t workspace_bytes;
 } snapb_member_f32;
 
-/* tile shapes; 0 = default.  x1_columns: columns per x1 tile; march_segment:
- * faces per x2/x3 segment; ctas_per_sm: persistent CTAs per SM cap; vic_block:
- * columns per implicit-column tile (32, 64 or 128); vic_regs: variant of the
- * implicit solve (0 column kernel with the compiler's register budget, 1
- * ~168, 2 128; 3 the fused kernel: blocks, twisted elimination from both
- * column ends, back substitution and finish in one launch). */
+/* tile shapes and kernel variants; 0 = default.  x1_columns: columns per x1
+ * tile (a power of two); march_segment: faces per x2/x3 segment; ctas_per_sm:
+ * persistent CTAs per SM cap; vic_kernel: the implicit solve (0 the column
+ * kernel + finish kernel; 1 block cyclic reduction, one CTA per column, where
+ * it applies: 3x3 blocks and columns of at most 256 layers, else 0; 2 the
+ * fused kernel: blocks, twisted elimination from both column ends, back
+ * substitution and finish in one launch); vic_block: columns per tile of the
+ * column kernel (32, 64 or 128); vic_regs: its register budget (0 the
+ * compiler's, 1 ~168, 2 128). */
 typedef struct snapb_ensemble_tuning {
-  int32_t x1_columns, march_segment, ctas_per_sm, vic_block, vic_regs;
+  int32_t x1_columns, march_segment, ctas_per_sm, vic_block, vic_regs, vic_kernel;
 } snapb_ensemble_tuning;
 
 typedef struct snapb_ensemble snapb_ensemble; /* opaque host-side plan */
@@ -416,6 +419,14 @@ enum {
 };
 int snapb_timing_enable(int on);
 int snapb_timing_query(int kernel, double* total_ms, int* launches);
+
+/* Bulk (TMA-engine) copies: the sweeps that stage their tiles with
+ * cp.async.bulk wait on them with a bounded poll; a CTA whose copy did not
+ * complete in time gives up its tile and raises a device flag.  Returns the
+ * flag (0: every copy completed since the last call; 1: at least one timed
+ * out, so the results of those launches are not to be used) and clears it;
+ * synchronizes the device; -1 on a CUDA error. */
+int snapb_bulk_copy_timeouts(void);
 
 #ifdef __cplusplus
 }

@@ -80,6 +80,7 @@ def lib():
         "snapb_conserved_totals_f32": (i, [cp, vp, i, vp, vp, sz, vp, sz, vp]),
         "snapb_timing_enable": (i, [i]),
         "snapb_timing_query": (i, [i, ctypes.POINTER(d), ctypes.POINTER(i)]),
+        "snapb_bulk_copy_timeouts": (i, []),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -96,7 +97,7 @@ def exported_symbols():
             "snapb_implicit_correction", "snapb_implicit_correction_noalloc", "snapb_stage",
             "snapb_bc_apply", "snapb_max_time_step", "snapb_scale_dt",
             "snapb_check_positive", "snapb_pack_slab", "snapb_unpack_slab",
-            "snapb_timing_enable", "snapb_timing_query",
+            "snapb_timing_enable", "snapb_timing_query", "snapb_bulk_copy_timeouts",
             "snapb_workspace_size_f32", "snapb_reference_f32", "snapb_to_perturbation",
             "snapb_from_perturbation", "snapb_stage_f32", "snapb_bc_apply_f32",
             "snapb_max_time_step_f32", "snapb_adjoint_workspace_size", "snapb_stage_adjoint",

@@ -15,7 +15,9 @@ forward path (``snapb_stage``):
   differentiable op.  The forward pass keeps the state every
   ``checkpoint_every`` steps; the backward pass re-runs each segment from its
   checkpoint, keeping the three stage inputs of every step of the segment, and
-  runs the stage reverses (2, 1, 0) step by step.
+  runs the stage reverses (2, 1, 0) step by step.  ``checkpoint_every=0``
+  keeps the three stage inputs of every step during the forward pass instead
+  (3 states per step of device memory, no re-run).
 
 dt is a constant of the adjoint: ``dts`` holds the step sizes of the forward
 run (for instance the CFL values of a first, non-differentiated run).  Every
@@ -143,12 +145,16 @@ def _autograd():
             ctx.runner, ctx.k = runner, k
             nsteps = dts.numel()
             cks = []
+            kept = None
             runner.load(u, s)
-            for n in range(nsteps):
-                if n % k == 0:
-                    cks.append(runner.snapshot())
-                runner.step(dts[n:n + 1])
-            ctx.cks = cks
+            if k <= 0:  # every step's stage inputs, kept now: no re-run backwards
+                kept = [runner.step(dts[n:n + 1], keep=True) for n in range(nsteps)]
+            else:
+                for n in range(nsteps):
+                    if n % k == 0:
+                        cks.append(runner.snapshot())
+                    runner.step(dts[n:n + 1])
+            ctx.cks, ctx.kept = cks, kept
             ctx.save_for_backward(dts)
             uT, sT = runner.snapshot()
             return uT, (sT if sT is not None else torch.zeros(0, device=u.device))
@@ -162,13 +168,17 @@ def _autograd():
             g = gu.contiguous().clone()
             has_s = runner.cfg.nscalar > 0
             gsc = gs.contiguous().clone() if has_s else None
-            for seg in reversed(range(len(ctx.cks))):
-                n0 = seg * k
-                n1 = min(n0 + k, nsteps)
-                runner.load(*ctx.cks[seg])
-                inputs = []
-                for n in range(n0, n1):
-                    inputs.append(runner.step(dts[n:n + 1], keep=True))
+            if ctx.kept is not None:
+                segments = [(0, nsteps, ctx.kept)]
+            else:
+                segments = []
+                for seg in range(len(ctx.cks)):
+                    n0 = seg * k
+                    segments.append((n0, min(n0 + k, nsteps), None))
+            for n0, n1, inputs in reversed(segments):
+                if inputs is None:  # re-run the segment from its checkpoint
+                    runner.load(*ctx.cks[n0 // k])
+                    inputs = [runner.step(dts[n:n + 1], keep=True) for n in range(n0, n1)]
                 for n in reversed(range(n0, n1)):
                     dt = dts[n:n + 1]
                     gu0 = torch.zeros_like(g)
@@ -253,7 +263,9 @@ def rollout(options, u, s=None, dts=None, checkpoint_every: int = 20, runner=Non
     differentiable op; returns (u_T, s_T) (s_T empty without scalars).
 
     The backward pass re-runs each checkpoint segment once and needs the
-    adjoint workspace plus 3 * checkpoint_every saved states."""
+    adjoint workspace plus 3 * checkpoint_every saved states;
+    checkpoint_every=0 keeps 3 states per step during the forward pass and
+    re-runs nothing."""
     import torch
 
     opts = _opts(options)

@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libsnapb.so")
 BUILD = os.path.join(HERE, "_build")
-SOURCES = ["capi.cu", "stage.cu", "vic.cu", "aux.cu", "stage32.cu", "capi32.cu", "adjoint.cu", "ensemble.cu", "totals.cu", "halo.cu", "vicf.cu"]
+SOURCES = ["capi.cu", "stage.cu", "vic.cu", "aux.cu", "stage32.cu", "capi32.cu", "adjoint.cu", "ensemble.cu", "totals.cu", "halo.cu", "vicf.cu", "vic_cr.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-Xptxas", "-warn-spills"]

@@ -100,12 +100,12 @@ __global__ void k_fill_u64(unsigned long long* p, int n, unsigned long long v) {
 // host plan
 // ---------------------------------------------------------------------------
 enum Phase {
-  PH_X1 = 0, PH_X1REV, PH_X2, PH_X3, PH_VCOL, PH_VFIN, PH_VFUSED, PH_BCU, PH_BCS, PH_CFL,
+  PH_X1 = 0, PH_X1REV, PH_X2, PH_X3, PH_VCOL, PH_VFIN, PH_VFUSED, PH_VCR, PH_BCU, PH_BCS, PH_CFL,
   PH_COUNT
 };
 
-// vic_regs value of the tuning that selects the fused implicit-solve kernel
-constexpr int kVicFusedVariant = 3;
+// vic_kernel values of the tuning: the implicit-solve variants
+constexpr int kVicColumn = 0, kVicCyclic = 1, kVicFused = 2;
 
 struct snapb_ensemble {
   std::vector<snapb_member_f32> in;
@@ -118,6 +118,10 @@ struct snapb_ensemble {
   int use1 = 0, use2 = 0, use3 = 0;
   int sms = 148;
   size_t x1_smem = 0;
+  int x1_cols = 8;  // x1 tile width (columns) of every member
+  int x1_nc1 = 1;   // longest member column (x1 cells with ghosts): the x1 tile layout
+  int vic_kernel = kVicColumn;  // the implicit-solve variant in use
+  int max_layers = 0;           // longest member column (cyclic reduction's shared memory)
   std::vector<int64_t> prefix[PH_COUNT];
   // device layout (offsets into the bound workspace)
   size_t o_mem = 0, o_prefix = 0, o_counter = 0, o_dts = 0, o_slots = 0, total = 0;
@@ -161,10 +165,9 @@ int plan(snapb_ensemble* e) {
     const int nvt = 5 + e->p.nscalar;
     // x1: columns per tile
     size_t per = x1_smem32_per_column(g, nvt);
-    int C = t.x1_columns > 0 ? t.x1_columns : (int)std::min<size_t>(16, (96 * 1024) / per);
+    int C = t.x1_columns > 0 ? t.x1_columns : (int)std::min<size_t>(8, (96 * 1024) / per);
     C = x1_columns_pow2(std::max(1, std::min<int>(C, (int)((200 * 1024) / per))));
     mb.x1_cols = C;
-    e->x1_smem = std::max(e->x1_smem, per * C);
     int64_t ncol1 = (int64_t)g.nc2 * g.nc3;
     // march: 128 lines per tile, segments of seglen faces
     int ni = g.iu - g.il + 1;
@@ -188,6 +191,7 @@ int plan(snapb_ensemble* e) {
                          : 0;
     const int fc = vicf_tile_columns();
     tiles[PH_VFUSED] = e->p.implicit_scheme ? (ncolv + fc - 1) / fc : 0;
+    tiles[PH_VCR] = e->p.implicit_scheme ? ncolv : 0;  // one column per tile
     // ghost-shell cells, 256 per tile (same count as bc_shell_slots)
     const int64_t nj = g.ju - g.jl + 1, nk = g.ku - g.kl + 1;
     const int64_t shell = (g.nc1 > 1 ? nj * nk * 2 * g.ng : 0) +
@@ -199,7 +203,33 @@ int plan(snapb_ensemble* e) {
     tiles[PH_CFL] = (ncell + 1023) / 1024;
     for (int ph = 0; ph < PH_COUNT; ++ph) e->prefix[ph][m + 1] = e->prefix[ph][m] + tiles[ph];
   }
+  // one x1 tile width for the ensemble (the CTA size of the x1 launch): the
+  // smallest member choice, then the tile counts and shared memory from it
+  e->x1_cols = 16;
+  e->x1_nc1 = 1;
+  for (const Member32& mb : e->mem) {
+    e->x1_cols = std::min(e->x1_cols, mb.x1_cols);
+    e->x1_nc1 = std::max(e->x1_nc1, mb.g.nc1);
+  }
+  for (int m = 0; m < e->M; ++m) {
+    Member32& mb = e->mem[m];
+    mb.x1_cols = e->x1_cols;
+    const int64_t ncol1 = (int64_t)mb.g.nc2 * mb.g.nc3;
+    const int64_t n1 = e->a1 ? (ncol1 + e->x1_cols - 1) / e->x1_cols : 0;
+    e->prefix[PH_X1][m + 1] = e->prefix[PH_X1][m] + n1;
+  }
+  e->x1_smem = x1_smem32_bytes(e->x1_nc1, 5 + e->p.nscalar, e->x1_cols);
   if (e->x1_smem > 200 * 1024) return efail(SNAPB_ERR_ARG, "ensemble: x1 tile too large");
+  // implicit solve: cyclic reduction only when every member is in its range
+  e->max_layers = 0;
+  bool cr_ok = true;
+  for (const Member32& mb : e->mem) {
+    e->max_layers = std::max(e->max_layers, mb.g.nx1);
+    cr_ok = cr_ok && vic_cr_applies(mb.g, e->p);
+  }
+  if (t.vic_kernel < 0 || t.vic_kernel > kVicFused)
+    return efail(SNAPB_ERR_ARG, "ensemble: vic_kernel in [0, 2]");
+  e->vic_kernel = t.vic_kernel == kVicCyclic ? (cr_ok ? kVicCyclic : kVicColumn) : t.vic_kernel;
   size_t o = 0;
   e->o_mem = o;
   o = al(o + sizeof(Member32) * e->M);
@@ -393,7 +423,7 @@ int snapb_ensemble_stage_f32(snapb_ensemble* e, int stage, void* stream) {
       c = launch_x1_ghost_revision32_batch(mem, p, queue(e, PH_X1REV), pgrid(e, PH_X1REV), st);
     if (c == cudaSuccess)
       c = launch_x1_32_batch(mem, p, queue(e, PH_X1), stage, last == 1, pgrid(e, PH_X1),
-                             e->x1_smem, st);
+                             e->x1_smem, e->x1_cols, e->x1_nc1, st);
     if (c != cudaSuccess) return cuda_e(c, "ensemble x1");
   }
   if (e->a2) {
@@ -410,7 +440,10 @@ int snapb_ensemble_stage_f32(snapb_ensemble* e, int stage, void* stream) {
   }
   if (p.implicit_scheme) {
     ScopedTimer t(SNAPB_K_VIC, st);
-    if (e->tune.vic_regs == kVicFusedVariant) {
+    if (e->vic_kernel == kVicCyclic) {
+      c = launch_vic_cr32_batch(mem, p, queue(e, PH_VCR), stage, pgrid(e, PH_VCR),
+                                e->max_layers, st);
+    } else if (e->vic_kernel == kVicFused) {
       c = launch_vicf_batch(mem, p, queue(e, PH_VFUSED), stage, pgrid(e, PH_VFUSED), st);
     } else {
       int blk = e->mem.empty() ? 64 : e->mem[0].vic_cols;

@@ -408,6 +408,9 @@ class Ensemble {
     if (tuning.size() > 0) tune_.x1_columns = tuning[0];
     if (tuning.size() > 1) tune_.march_segment = tuning[1];
     if (tuning.size() > 2) tune_.ctas_per_sm = tuning[2];
+    if (tuning.size() > 3) tune_.vic_block = tuning[3];
+    if (tuning.size() > 4) tune_.vic_regs = tuning[4];
+    if (tuning.size() > 5) tune_.vic_kernel = tuning[5];
     std::vector<snapb_member_f32> mem(blocks_.size());
     auto fp = [](torch::Tensor& t) { return t.defined() ? (float*)t.data_ptr() : nullptr; };
     for (size_t k = 0; k < blocks_.size(); ++k) {

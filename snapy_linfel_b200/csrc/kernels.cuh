@@ -93,12 +93,10 @@ struct WorkQueue {
 
 // Next (member, tile) for the whole CTA; false when the queue is drained.
 // Every thread of the CTA must call it.
-__device__ __forceinline__ bool queue_next(const WorkQueue& q, int& m, int64_t& tile) {
-  __shared__ unsigned long long s_item;
-  __syncthreads();
-  if (threadIdx.x == 0) s_item = atomicAdd(q.counter, 1ULL);
-  __syncthreads();
-  const int64_t item = (int64_t)s_item;
+// (member, tile) of a work item (false past the last item): binary search of
+// the per-member prefix table
+__device__ __forceinline__ bool queue_find(const WorkQueue& q, int64_t item, int& m,
+                                           int64_t& tile) {
   if (item >= q.prefix[q.M]) return false;
   int lo = 0, hi = q.M - 1;
   while (lo < hi) {
@@ -109,6 +107,14 @@ __device__ __forceinline__ bool queue_next(const WorkQueue& q, int& m, int64_t& 
   m = lo;
   tile = item - q.prefix[lo];
   return true;
+}
+
+__device__ __forceinline__ bool queue_next(const WorkQueue& q, int& m, int64_t& tile) {
+  __shared__ unsigned long long s_item;
+  __syncthreads();
+  if (threadIdx.x == 0) s_item = atomicAdd(q.counter, 1ULL);
+  __syncthreads();
+  return queue_find(q, (int64_t)s_item, m, tile);
 }
 
 // Raise a kernel's dynamic shared-memory limit above the default 48 KB, once
@@ -133,6 +139,14 @@ inline void raise_smem_limit(K kernel, size_t bytes) {
 // it right after queue_next (whose leading barrier ends the previous tile).
 // Kernels then read the fields as they need them instead of holding the
 // ~50-word struct in registers for the whole tile.
+// the same copy by one warp (no CTA barrier; the warp's lanes see it after
+// __syncwarp, the others after the next CTA barrier)
+__device__ __forceinline__ void load_member_warp(Member32& dst, const Member32* mem, int m) {
+  const int* src = reinterpret_cast<const int*>(mem + m);
+  int* d = reinterpret_cast<int*>(&dst);
+  for (int k = threadIdx.x & 31; k < (int)(sizeof(Member32) / sizeof(int)); k += 32) d[k] = src[k];
+  __syncwarp();
+}
 __device__ __forceinline__ void load_member(Member32& dst, const Member32* mem, int m) {
   static_assert(sizeof(Member32) % sizeof(int) == 0, "member descriptor copy");
   const int* src = reinterpret_cast<const int*>(mem + m);
@@ -164,8 +178,8 @@ inline int persistent_grid(K kernel, int block, size_t smem, const PersistGrid& 
 
 // persistent launchers of the batched FP32 stage
 cudaError_t launch_x1_32_batch(const Member32* mem, const Phys& p, const WorkQueue& q,
-                               int stage, bool last, const PersistGrid& pg, size_t smem,
-                               cudaStream_t st);
+                               int stage, bool last, const PersistGrid& pg, size_t smem, int C,
+                               int nc1max, cudaStream_t st);
 cudaError_t launch_march32_batch(int axis, const Member32* mem, const Phys& p,
                                  const WorkQueue& q, int stage, bool first, bool last,
                                  const PersistGrid& pg, cudaStream_t st);
@@ -174,6 +188,9 @@ cudaError_t launch_vic_column_batch(const Member32* mem, const Phys& p, const Wo
                                     cudaStream_t st);
 cudaError_t launch_vic_finish_batch(const Member32* mem, const Phys& p, const WorkQueue& q,
                                     int stage, const PersistGrid& pg, cudaStream_t st);
+cudaError_t launch_vic_cr32_batch(const Member32* mem, const Phys& p, const WorkQueue& q,
+                                  int stage, const PersistGrid& pg, int max_layers,
+                                  cudaStream_t st);
 // the fused implicit-solve kernel (vicf.cu): one launch per solve, tiles of
 // vicf_tile_columns() columns
 cudaError_t launch_vicf_batch(const Member32* mem, const Phys& p, const WorkQueue& q, int stage,
@@ -183,6 +200,8 @@ cudaError_t launch_bc32_batch(const Member32* mem, const Phys& p, const WorkQueu
                               double igm1, const PersistGrid& pg, cudaStream_t st);
 size_t x1_smem32_per_column(const Geo& g, int nvt);
 int x1_columns_pow2(int c);  // x1 tile width rounded down to a power of two
+// shared memory of an x1 tile of C columns in a launch whose longest column is nc1max
+size_t x1_smem32_bytes(int nc1max, int nvt, int C);
 cudaError_t launch_x1_ghost_revision32_batch(const Member32* mem, const Phys& p,
                                              const WorkQueue& q, const PersistGrid& pg,
                                              cudaStream_t st);
@@ -197,6 +216,17 @@ inline void rk3_weights(int stage, double& a, double& b, double& c) {
   a = W[stage][0];
   b = W[stage][1];
   c = W[stage][2];
+}
+
+// the stage fields of a member's buffers (batched launches set them per stage)
+__device__ __forceinline__ void set_stage32(StageBufs32& b, int stage) {
+  double w0 = 1., w1 = 0., w2 = 1.;
+  if (stage == 1) w0 = 3. / 4., w1 = 1. / 4., w2 = 1. / 4.;
+  if (stage == 2) w0 = 1. / 3., w1 = 2. / 3., w2 = 2. / 3.;
+  b.stage = stage;
+  b.wgt0 = w0;
+  b.wgt1 = w1;
+  b.wgt2 = w2;
 }
 
 // launchers (return a cudaError_t of the launch)
@@ -217,6 +247,11 @@ cudaError_t launch_vicf(const Geo& g, const Phys& p, const StageBufs& b, cudaStr
 cudaError_t launch_vicf32(const Geo& g, const Phys& p, const StageBufs32& b, cudaStream_t st);
 size_t vic_blocks_bytes(const Geo& g, const Phys& p);
 int vic_finish_layers32(const Phys& p);  // layers per implicit-finish tile, FP32 form
+// implicit solve of the FP32 form by block cyclic reduction (vic_cr.cu): one
+// CTA per column, 3x3 blocks, columns of at most 256 layers
+bool vic_cr_applies(const Geo& g, const Phys& p);
+size_t vic_cr_smem_bytes(int nl);
+cudaError_t launch_vic_cr32(const Geo& g, const Phys& p, const StageBufs32& b, cudaStream_t st);
 
 cudaError_t launch_cons2prim(const Geo& g, const Phys& p, const double* u, double* w,
                              cudaStream_t st);

@@ -16,6 +16,7 @@
 #include <algorithm>
 
 #include "kernels.cuh"
+#include "bulk.cuh"
 #include "pert.cuh"
 
 namespace snapb {
@@ -153,11 +154,30 @@ __device__ __forceinline__ void cons2prim_pert(const float* u, float* w, float r
 // ---------------------------------------------------------------------------
 // x1 column kernel
 // ---------------------------------------------------------------------------
-// Shared memory per column: W' rows [NV][nc1], the full density row [nc1]
-// (rho_bar + rho', the reconstructed density) and the face flux rows [NV][nc1].
+// One warp per x1 column, C columns per tile (CTA of 32 C threads).  Shared
+// memory of a tile: W' rows [C][NV][nc1], the full density row [C][nc1]
+// (rho_bar + rho', the reconstructed density), then the staging planes of the
+// tile's U' and scalar slabs, [NV][ps] with ps >= C nc1 + 3, 16-byte aligned.
 size_t x1_smem32_per_column(const Geo& g, int nvt) {
   return (size_t)(2 * nvt + 1) * g.nc1 * sizeof(float);
 }
+// The layout follows the longest column of the launch (nc1max): a batched
+// launch stages the next tile, possibly of another member, while the current
+// one's rows are read, so the staging planes start after the rows of any tile.
+struct X1Smem {
+  int64_t fo, ps;  // float offset of the staging planes, plane stride
+  __host__ __device__ X1Smem(int nc1max, int nvt, int C) {
+    fo = (((int64_t)C * (nvt + 1) * nc1max) + 3) & ~(int64_t)3;
+    ps = ((int64_t)C * nc1max + 3 + 3) & ~(int64_t)3;
+  }
+  __host__ __device__ size_t bytes(int nvt) const {
+    return (size_t)(fo + ps * nvt) * sizeof(float);
+  }
+};
+size_t x1_smem32_bytes(int nc1max, int nvt, int C) { return X1Smem(nc1max, nvt, C).bytes(nvt); }
+
+// set by a CTA of the x1 sweep whose bulk copy did not complete in time
+__device__ int snapb_x1_bulk_timeout = 0;
 
 // Isentropic x1 ghost revision on full values, in FP64, written into W' of the
 // ghost cells (density and pressure rows).  The recurrence
@@ -196,40 +216,72 @@ __global__ void __launch_bounds__(256) k_x1_ghost_revision32(Geo g, Phys p, Stag
   if (slot < (int64_t)g.nc2 * g.nc3 * 2 * g.ng) x1_ghost_revision32(g, p, b, slot);
 }
 
-// One tile: columns col0 .. col0+C-1 of the block (C a power of two dividing
-// the CTA size), smf = x1_smem32_per_column * C bytes.  Every thread of the CTA
-// calls it (it synchronises the CTA).  Threads are laid out tpc = nt / C per
-// column, so a thread's column and its cells follow from shifts and masks:
-//   (1) U' -> W' of the column's cells into shared memory, with W' and the
-//       scalar mixing ratios stored; ghost cells take density and pressure
-//       from the ghost revision (when gravity acts along x1);
-//   (2) the face states and fluxes, faces il .. iu of each column by its
-//       threads and face iu+1 of all columns by the first C threads;
-//   (3) the flux differences, then du or the RK combination (finalize32).
+// (0) Warp 0 stages the U' and scalar slabs of columns col0 .. col0+C-1 (they
+// are consecutive in every variable plane) into the staging planes: the
+// aligned interiors by bulk copies completing on `bar`, the ragged ends by
+// plain loads (visible after the next CTA barrier).
 template <int NS>
-__device__ __forceinline__ void x1_32_tile(const Geo& g, const Phys& p, const StageBufs32& b,
-                                           int C, int last, int64_t col0, float* smf) {
+__device__ __forceinline__ void x1_32_stage(const Geo& g, const StageBufs32& b, int C,
+                                            int64_t col0, float* smf, int nc1max,
+                                            uint64_t* bar) {
+  constexpr int NV = 5 + NS;
+  if (threadIdx.x >= 32) return;
+  const X1Smem L(nc1max, NV, C);
+  const int64_t ncol = (int64_t)g.nc2 * g.nc3;
+  const int64_t nslab = std::min<int64_t>(C, ncol - col0) * g.nc1;
+  auto plane = [&](int v) -> const float* {
+    return (v < 5 ? b.u + v * g.sv : b.s + (v - 5) * g.sv) + col0 * g.nc1;
+  };
+  if (threadIdx.x == 0) {
+    unsigned bytes = 0;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) bytes += (unsigned)(bulk_split(plane(v), nslab).body * 4);
+    fence_proxy_async_smem();  // earlier reads of the staging planes come first
+    mbar_arrive_expect_tx(bar, bytes);
+  }
+  if (threadIdx.x < 8)
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+      bulk_stage_slab(smf + L.fo + v * L.ps, plane(v), nslab, bar, threadIdx.x == 0);
+}
+
+// One tile after its staging completed, every thread of the CTA (one
+// barrier): warp w works column col0 + w.
+//   (1) U' -> W' of the column's cells from the staged slabs into shared
+//       memory, with W' and the scalar mixing ratios stored; ghost cells take
+//       density and pressure from the ghost revision (gravity along x1);
+//   (2) the faces in rounds of 32 (face il + 32 k + lane): states and flux in
+//       registers; the flux difference of cell f takes face f+1 from the next
+//       lane (a shuffle), lane 31 that of the next round's lane 0 one round
+//       later; then du or the RK combination (finalize32).
+// The staging planes are free after (1): on return from x1_32_convert the
+// caller may stage the next tile while x1_32_faces runs.
+template <int NS>
+__device__ __forceinline__ void x1_32_convert(const Geo& g, const Phys& p, const StageBufs32& b,
+                                              int C, int64_t col0, float* smf, int nc1max) {
   constexpr int NV = 5 + NS;
   const int nc1 = g.nc1, ng = g.ng, il = g.il, iu = g.iu;
-  float* sw = smf;                              // [C][NV][nc1]
-  float* sr = sw + (size_t)C * NV * nc1;        // [C][nc1]
-  float* sf = sr + (size_t)C * nc1;             // [C][NV][nc1]
+  const X1Smem L(nc1max, NV, C);
+  float* sw = smf;                        // [C][NV][nc1]
+  float* sr = sw + (size_t)C * NV * nc1;  // [C][nc1]
+  const float* st = smf + L.fo;           // staging planes
   const int64_t ncol = (int64_t)g.nc2 * g.nc3;
-  const int tid = threadIdx.x, nt = blockDim.x;
-  const int lgC = __ffs(C) - 1, tpc = nt >> lgC;
-  const int c = tid / tpc, t = tid - c * tpc;  // this thread's column and rank in it
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, c = tid >> 5;
+  const int lgC = __ffs(C) - 1;
   const int64_t sv = g.sv;
   const float gm1 = (float)(p.gammad - 1.);
-  const float gamma = (float)p.gammad;
   const bool revise = p.grav1 != 0.;
-
-  // (1) interior cells of this thread's column, then the ghost cells of all
-  // columns (2 ng per column, spread over the CTA)
+  int sbase[NV];  // float offset in the staging planes of each variable's element 0
+#pragma unroll
+  for (int v = 0; v < NV; ++v)
+    sbase[v] = (int)(v * L.ps) +
+               bulk_phase((v < 5 ? b.u + v * sv : b.s + (v - 5) * sv) + col0 * nc1);
   auto convert = [&](int cc, int i, bool ghost) {
     const int64_t off = (col0 + cc) * nc1 + i;
+    const int e = cc * nc1 + i;
     float uc[5], wc[5];
 #pragma unroll
-    for (int v = 0; v < 5; ++v) uc[v] = b.u[v * sv + off];
+    for (int v = 0; v < 5; ++v) uc[v] = st[sbase[v] + e];
     cons2prim_pert(uc, wc, b.rbf[i], gm1);
     float* base = sw + (size_t)cc * NV * nc1;
     if (ghost && revise) {  // density and pressure from the ghost revision
@@ -246,32 +298,44 @@ __device__ __forceinline__ void x1_32_tile(const Geo& g, const Phys& p, const St
     sr[(size_t)cc * nc1 + i] = b.rbf[i] + wc[IDN];
 #pragma unroll
     for (int n = 0; n < NS; ++n) {
-      float rr = b.s[n * sv + off] / (b.rbf[i] + uc[IDN]);
+      float rr = st[sbase[5 + n] + e] / (b.rbf[i] + uc[IDN]);
       base[(5 + n) * nc1 + i] = rr;
       b.R[n * sv + off] = rr;
     }
   };
-  const bool col_ok = col0 + c < ncol;
-  if (col_ok)
-    for (int i = il + t; i <= iu; i += tpc) convert(c, i, false);
-  for (int idx = tid; idx < 2 * ng * C; idx += nt) {
+  if (col0 + c < ncol)
+    for (int i = il + lane; i <= iu; i += 32) convert(c, i, false);
+  for (int idx = tid; idx < 2 * ng * C; idx += nt) {  // ghost cells, 2 ng per column
     const int cc = idx & (C - 1), k = idx >> lgC;
     if (col0 + cc < ncol) convert(cc, k < ng ? k : iu + 1 + (k - ng), true);
   }
   __syncthreads();
+}
 
-  // (2) faces: the stencil f-3 .. f+2 stays inside the column (ng >= 3)
-  const int ptype = (p.r1_shock) ? p.r1_type : interp2_of(p.r1_type);
+template <int NS>
+__device__ __forceinline__ void x1_32_faces(const Geo& g, const Phys& p, const StageBufs32& b,
+                                            int C, int last, int64_t col0, const float* smf,
+                                            float* sfe) {
+  constexpr int NV = 5 + NS;
+  const int nc1 = g.nc1, il = g.il, iu = g.iu;
+  const int lane = threadIdx.x & 31, c = threadIdx.x >> 5;
+  const int64_t ncol = (int64_t)g.nc2 * g.nc3;
   auto interior = [&](int cc) {
     const int64_t col = col0 + cc;
     if (col >= ncol) return false;
     const int j = umod(col, g.nc2), k = udiv(col, g.nc2);
     return j >= g.jl && j <= g.ju && k >= g.kl && k <= g.ku;
   };
-  auto face = [&](int cc, int f) {
-    const float* base = sw + (size_t)cc * NV * nc1 + f - 3;
-    const float* rho = sr + (size_t)cc * nc1 + f - 3;
-    float L[NV], R[NV], F[NV];
+  const int64_t sv = g.sv;
+  const float gamma = (float)p.gammad;
+  const bool revise = p.grav1 != 0.;
+  const int ptype = (p.r1_shock) ? p.r1_type : interp2_of(p.r1_type);
+  const float A1 = (float)g.A1;
+  // face f of tile column cc; the stencil f-3 .. f+2 stays inside the column (ng >= 3)
+  auto face = [&](int cc, int f, float* F) {
+    const float* base = smf + (size_t)cc * NV * nc1 + f - 3;
+    const float* rho = smf + (size_t)C * NV * nc1 + (size_t)cc * nc1 + f - 3;
+    float L[NV], R[NV];
     float pl, pr;
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
@@ -312,26 +376,10 @@ __device__ __forceinline__ void x1_32_tile(const Geo& g, const Phys& p, const St
     }
 #pragma unroll
     for (int n = 0; n < NS; ++n) F[5 + n] = F[IDN] > 0.f ? F[IDN] * L[5 + n] : F[IDN] * R[5 + n];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) sf[((size_t)cc * NV + v) * nc1 + f] = F[v];
   };
-  const bool mine = interior(c);
-  if (mine)
-    for (int f = il + t; f <= iu; f += tpc) face(c, f);
-  for (int cc = tid; cc < C; cc += nt)
-    if (interior(cc)) face(cc, iu + 1);
-  __syncthreads();
-
-  // (3) flux differences of this thread's column
-  if (!mine) return;
-  const float A1 = (float)g.A1;
-  const float* fc = sf + (size_t)c * NV * nc1;
-  const float* wcol = sw + (size_t)c * NV * nc1;
-  for (int i = il + t; i <= iu; i += tpc) {
+  const float* wcol = smf + (size_t)c * NV * nc1;
+  auto finish = [&](int i, const float* d) {
     const int64_t off = (col0 + c) * nc1 + i;
-    float d[NV];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) d[v] = A1 * fc[v * nc1 + i + 1] - A1 * fc[v * nc1 + i];
     if (last) {
       float wc[5];
 #pragma unroll
@@ -341,13 +389,79 @@ __device__ __forceinline__ void x1_32_tile(const Geo& g, const Phys& p, const St
 #pragma unroll
       for (int v = 0; v < NV; ++v) b.D[v * sv + off] = d[v];
     }
+  };
+  // faces il .. iu in rounds of 32 (face f0 + lane); the flux difference of
+  // cell f takes face f+1 from the next lane, lane 31 that of the next
+  // round's lane 0 one round later; cell iu waits for face iu+1 (below)
+  const bool mine = interior(c);
+  float Fkeep[NV];  // lane 31: its face of the previous round; the lane of face iu: that face
+#pragma unroll
+  for (int v = 0; v < NV; ++v) Fkeep[v] = 0.f;
+  if (mine) {
+    for (int f0 = il; f0 <= iu; f0 += 32) {
+      const int f = f0 + lane;
+      float F[NV];
+      if (f <= iu) {
+        face(c, f, F);
+      } else {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) F[v] = 0.f;
+      }
+      float Fn[NV];  // lanes 0 .. 30: face f + 1; lane 31: this round's first face
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        const float dn = __shfl_down_sync(0xffffffffu, F[v], 1);
+        const float f0v = __shfl_sync(0xffffffffu, F[v], 0);
+        Fn[v] = lane < 31 ? dn : f0v;
+      }
+      // this lane's cell: f (lanes 0 .. 30), the previous round's last (lane 31)
+      const int i = lane < 31 ? f : f0 - 1;
+      if (i >= il && i < iu) {
+        float d[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) d[v] = A1 * Fn[v] - A1 * (lane < 31 ? F[v] : Fkeep[v]);
+        finish(i, d);
+      }
+      if (lane == 31 || f == iu) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) Fkeep[v] = F[v];
+      }
+    }
+  }
+  // face iu+1 of every interior column of the tile, one lane per column
+  if (c == 0 && lane < C && interior(lane)) {
+    float F[NV];
+    face(lane, iu + 1, F);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) sfe[lane * NV + v] = F[v];
+  }
+  __syncthreads();
+  // cell iu: the lane that computed face iu
+  if (mine && lane == ((iu - il) & 31)) {
+    float d[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) d[v] = A1 * sfe[c * NV + v] - A1 * Fkeep[v];
+    finish(iu, d);
   }
 }
 
+// one tile per CTA: stage, convert, faces
 template <int NS>
-__global__ void __launch_bounds__(256) k_x1_32(Geo g, Phys p, StageBufs32 b, int C, int last) {
-  extern __shared__ float smf[];
-  x1_32_tile<NS>(g, p, b, C, last, (int64_t)blockIdx.x * C, smf);
+__global__ void __launch_bounds__(512, 2) k_x1_32(Geo g, Phys p, StageBufs32 b, int C, int last) {
+  extern __shared__ __align__(16) float smf[];
+  __shared__ uint64_t bar;
+  __shared__ float sfe[16 * (5 + NS)];  // face iu+1 of each column
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  __syncthreads();
+  const int64_t col0 = (int64_t)blockIdx.x * C;
+  x1_32_stage<NS>(g, b, C, col0, smf, g.nc1, &bar);
+  const bool ok = threadIdx.x >= 32 || mbar_wait(&bar, 0, &snapb_x1_bulk_timeout);
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x < 32) mbar_wait(&bar, 0, &snapb_x1_bulk_timeout);  // copies in flight
+    return;
+  }
+  x1_32_convert<NS>(g, p, b, C, col0, smf, g.nc1);
+  x1_32_faces<NS>(g, p, b, C, last, col0, smf, sfe);
 }
 
 // ---------------------------------------------------------------------------
@@ -611,29 +725,65 @@ __global__ void k_cfl32(Geo g, double gammad, int use1, int use2, int use3, cons
 // ---------------------------------------------------------------------------
 // persistent batched kernels: every CTA pulls (member, tile) items
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void set_stage32(StageBufs32& b, int stage) {
-  double w0 = 1., w1 = 0., w2 = 1.;
-  if (stage == 1) w0 = 3. / 4., w1 = 1. / 4., w2 = 1. / 4.;
-  if (stage == 2) w0 = 1. / 3., w1 = 2. / 3., w2 = 2. / 3.;
-  b.stage = stage;
-  b.wgt0 = w0;
-  b.wgt1 = w1;
-  b.wgt2 = w2;
-}
-
+// Persistent batched x1 sweep (CTA of 32 C threads, C the ensemble's tile
+// width): tiles are taken from the queue one ahead, so warp 0 stages the next
+// tile's slabs by bulk copies while the current tile's faces are computed.
 template <int NS>
-__global__ void __launch_bounds__(256, 4) k_x1_32_batch(const Member32* __restrict__ mem, Phys p,
-                                                     WorkQueue q, int stage, int last) {
-  extern __shared__ float smf[];
-  __shared__ Member32 s_mem;  // the member's descriptor, read as the tile needs its fields
+__global__ void __launch_bounds__(512, 2) k_x1_32_batch(const Member32* __restrict__ mem, Phys p,
+                                                        WorkQueue q, int stage, int last,
+                                                        int nc1max) {
+  extern __shared__ __align__(16) float smf[];
+  __shared__ Member32 s_mem[2];  // descriptors of the current and the next tile's member
+  __shared__ uint64_t bar;       // completion of a tile's bulk copies
+  __shared__ unsigned long long s_item;
+  __shared__ float sfe[16 * (5 + NS)];  // face iu+1 of each column
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    mbar_init(&bar, 1);
+    s_item = atomicAdd(q.counter, 1ULL);
+  }
+  __syncthreads();
   int m;
   int64_t tile;
-  while (queue_next(q, m, tile)) {  // (starts with a barrier: the last tile is done)
-    load_member(s_mem, mem, m);
-    if (threadIdx.x == 0) set_stage32(s_mem.b, stage);
-    __syncthreads();
-    const int C = s_mem.x1_cols;
-    x1_32_tile<NS>(s_mem.g, p, s_mem.b, C, last, tile * C, smf);
+  if (!queue_find(q, (int64_t)s_item, m, tile)) return;
+  if (tid < 32) {
+    load_member_warp(s_mem[0], mem, m);
+    if (tid == 0) set_stage32(s_mem[0].b, stage);
+    __syncwarp();
+    x1_32_stage<NS>(s_mem[0].g, s_mem[0].b, s_mem[0].x1_cols, tile * s_mem[0].x1_cols, smf,
+                    nc1max, &bar);
+  }
+  __syncthreads();
+  int buf = 0;
+  unsigned parity = 0;
+  while (true) {
+    const Member32& cur = s_mem[buf];
+    const int C = cur.x1_cols;
+    const int64_t col0 = tile * C;
+    bool ok = true;
+    if (tid < 32) ok = mbar_wait(&bar, parity, &snapb_x1_bulk_timeout);
+    if (tid == 0) s_item = atomicAdd(q.counter, 1ULL);  // the next item
+    if (__syncthreads_or(!ok)) {
+      if (tid < 32) mbar_wait(&bar, parity, &snapb_x1_bulk_timeout);  // copies in flight
+      return;
+    }
+    int nm;
+    int64_t ntile;
+    const bool more = queue_find(q, (int64_t)s_item, nm, ntile);
+    x1_32_convert<NS>(cur.g, p, cur.b, C, col0, smf, nc1max);  // (ends with a CTA barrier)
+    if (more && tid < 32) {  // stage the next tile while this one's faces run
+      Member32& nxt = s_mem[buf ^ 1];
+      load_member_warp(nxt, mem, nm);
+      if (tid == 0) set_stage32(nxt.b, stage);
+      __syncwarp();
+      x1_32_stage<NS>(nxt.g, nxt.b, nxt.x1_cols, ntile * nxt.x1_cols, smf, nc1max, &bar);
+    }
+    x1_32_faces<NS>(cur.g, p, cur.b, C, last, col0, smf, sfe);
+    if (!more) return;
+    __syncthreads();  // this tile's rows are read; the next descriptor is in place
+    buf ^= 1;
+    parity ^= 1;
+    tile = ntile;
   }
 }
 
@@ -688,13 +838,14 @@ __global__ void __launch_bounds__(256) k_bc32_batch(const Member32* __restrict__
 }
 
 cudaError_t launch_x1_32_batch(const Member32* mem, const Phys& p, const WorkQueue& q,
-                               int stage, bool last, const PersistGrid& pg, size_t smem,
-                               cudaStream_t st) {
+                               int stage, bool last, const PersistGrid& pg, size_t smem, int C,
+                               int nc1max, cudaStream_t st) {
+  const int nt = 32 * C;  // one warp per column of a tile
 #define SNAPB_X1B(NS)                                                                         \
   case NS: {                                                                                  \
     raise_smem_limit(k_x1_32_batch<NS>, 200 * 1024);                                        \
-    int grid = persistent_grid(k_x1_32_batch<NS>, 256, smem, pg);                             \
-    k_x1_32_batch<NS><<<grid, 256, smem, st>>>(mem, p, q, stage, last ? 1 : 0);               \
+    int grid = persistent_grid(k_x1_32_batch<NS>, nt, smem, pg);                              \
+    k_x1_32_batch<NS><<<grid, nt, smem, st>>>(mem, p, q, stage, last ? 1 : 0, nc1max);        \
     break;                                                                                    \
   }
   switch (p.nscalar) {
@@ -756,16 +907,16 @@ cudaError_t launch_ref32(const Geo& g, const Phys& p, const double* rb, const do
   return cudaGetLastError();
 }
 
-// columns per x1 tile: a power of two (the tile's thread layout), at most 16
-// and about 96 KB of shared memory
+// columns per x1 tile: a power of two (one warp per column), 8 by default
+// (the fastest measured) within about 96 KB of shared memory
 int x1_columns_pow2(int c) {
-  c = std::max(1, std::min(c, 32));
+  c = std::max(1, std::min(c, 16));  // CTAs of at most 512 threads
   while (c & (c - 1)) c &= c - 1;
   return c;
 }
 int x1_columns_per_cta32(const Geo& g, int nvt) {
   size_t per = x1_smem32_per_column(g, nvt);
-  return x1_columns_pow2((int)std::min<size_t>(16, std::max<size_t>(1, (96 * 1024) / per)));
+  return x1_columns_pow2((int)std::min<size_t>(8, std::max<size_t>(1, (96 * 1024) / per)));
 }
 
 cudaError_t launch_x1_ghost_revision32(const Geo& g, const Phys& p, const StageBufs32& b,
@@ -781,13 +932,13 @@ static cudaError_t launch_x1_32t(const Geo& g, const Phys& p, const StageBufs32&
                                  cudaStream_t st) {
   const int nvt = 5 + NS;
   int C = x1_columns_per_cta32(g, nvt);
-  size_t smem = (size_t)C * x1_smem32_per_column(g, nvt);
+  size_t smem = x1_smem32_bytes(g.nc1, nvt, C);
   if (smem > 200 * 1024) return cudaErrorInvalidConfiguration;
   raise_smem_limit(k_x1_32<NS>, 200 * 1024);
   cudaError_t e = launch_x1_ghost_revision32(g, p, b, st);
   if (e != cudaSuccess) return e;
   int64_t ncol = (int64_t)g.nc2 * g.nc3;
-  k_x1_32<NS><<<(unsigned)((ncol + C - 1) / C), 256, smem, st>>>(g, p, b, C, last ? 1 : 0);
+  k_x1_32<NS><<<(unsigned)((ncol + C - 1) / C), 32 * C, smem, st>>>(g, p, b, C, last ? 1 : 0);
   return cudaGetLastError();
 }
 
@@ -876,3 +1027,15 @@ cudaError_t launch_cfl32(const Geo& g, const Phys& p, const float* w, const doub
 }
 
 }  // namespace snapb
+
+extern "C" int snapb_bulk_copy_timeouts(void) {
+  int v = 0;
+  if (cudaMemcpyFromSymbol(&v, snapb::snapb_x1_bulk_timeout, sizeof(int)) != cudaSuccess)
+    return -1;
+  if (v) {
+    const int z = 0;
+    if (cudaMemcpyToSymbol(snapb::snapb_x1_bulk_timeout, &z, sizeof(int)) != cudaSuccess)
+      return -1;
+  }
+  return v;
+}

@@ -33,6 +33,7 @@
 #include "kernels.cuh"
 #include "ring.cuh"
 #include "vic_blocks.cuh"
+#include "vic_common.cuh"
 
 namespace snapb {
 
@@ -43,12 +44,6 @@ namespace snapb {
 //                        delta_i (back-substituted in place)
 //   Z [2][ncol]          per-column sums: sum (rho V)^2 and B_dry
 // ---------------------------------------------------------------------------
-template <int N>
-struct VicDims {
-  static constexpr int ES = N * N + N;
-};
-
-static inline int vic_n(const Phys& p) { return ((p.implicit_scheme >> 3) & 1) ? 5 : 3; }
 
 size_t vic_column_scratch_bytes(const Geo& g, const Phys& p) {
   if (p.implicit_scheme == 0) return 0;
@@ -105,73 +100,6 @@ constexpr size_t back_ring_bytes(int threads) {
   return (size_t)threads * BackRing<N>::depth * BackRing<N>::elems * sizeof(double);
 }
 
-
-// (k, j, il) offset of interior column `col`
-__device__ __forceinline__ int64_t column_base(const Geo& g, int64_t col) {
-  const int nj = g.ju - g.jl + 1;
-  const int j = g.jl + umod(col, nj), k = g.kl + udiv(col, nj);
-  return (int64_t)k * g.s3 + (int64_t)j * g.s2 + g.il;
-}
-
-// ---- state access, FP64 plain form and FP32 perturbation form ----
-// full primitive of variable v at offset off, x1 index xi
-__device__ __forceinline__ double vic_w(const StageBufs& b, int64_t sv, int v, int64_t off,
-                                        int xi) {
-  return b.w[v * sv + off];
-}
-__device__ __forceinline__ double vic_w(const StageBufs32& b, int64_t sv, int v, int64_t off,
-                                        int xi) {
-  double x = (double)b.w[v * sv + off];
-  if (v == IDN) x += b.rb[xi];
-  if (v == IPR) x += b.pb[xi];
-  return x;
-}
-// full primitive of variable v at x1 index xi from a stored value x
-__device__ __forceinline__ double vic_full(const StageBufs&, double x, int v, int xi) { return x; }
-__device__ __forceinline__ double vic_full(const StageBufs32& b, double x, int v, int xi) {
-  if (v == IDN) x += b.rb[xi];
-  if (v == IPR) x += b.pb[xi];
-  return x;
-}
-__device__ __forceinline__ double vic_d(const StageBufs& b, int64_t idx) { return b.D[idx]; }
-__device__ __forceinline__ double vic_d(const StageBufs32& b, int64_t idx) {
-  return (double)b.D[idx];
-}
-__device__ __forceinline__ void vic_set_d(const StageBufs& b, int64_t idx, double x) {
-  b.D[idx] = x;
-}
-__device__ __forceinline__ void vic_set_d(const StageBufs32& b, int64_t idx, double x) {
-  b.D[idx] = (float)x;
-}
-// RK combination of one stored value (u' for the FP32 form: the reference
-// part of u is constant in time, so the combination is the same), from
-// values already loaded (qo = q[o], q0o = q0[o] when stage > 0); the stored
-// q keeps the stored precision
-__device__ __forceinline__ double vic_rk_from(double* q, double* q0, int64_t o, bool first,
-                                              double qo, double q0o, double w0, double w1,
-                                              double w2, double d) {
-  double q0v = first ? qo : q0o;
-  if (first) q0[o] = qo;
-  double qn = w0 * q0v + w1 * qo + w2 * d;
-  q[o] = qn;
-  return qn;
-}
-__device__ __forceinline__ double vic_rk_from(float* q, float* q0, int64_t o, bool first,
-                                              double qo, double q0o, double w0, double w1,
-                                              double w2, double d) {
-  double q0v = first ? qo : q0o;
-  if (first) q0[o] = (float)qo;
-  float qn = (float)(w0 * q0v + w1 * qo + w2 * d);
-  q[o] = qn;
-  return qn;
-}
-// full density of a stored conserved perturbation
-__device__ __forceinline__ double vic_full_rho(const StageBufs&, double u_rho, int) {
-  return u_rho;
-}
-__device__ __forceinline__ double vic_full_rho(const StageBufs32& b, double u_rho, int xi) {
-  return u_rho + b.rb[xi];
-}
 
 // Block construction per form: the FP64 plain form in FP64; the FP32
 // perturbation form forms |A| and J in FP32 from the full states (only the
@@ -1048,12 +976,16 @@ static cudaError_t launch_vic_n(const Geo& g, const Phys& p, const B& b, cudaStr
   return cudaGetLastError();
 }
 
-// The column + finish pair (default) or the fused kernel of vicf.cu when the
-// environment sets SNAPB_VIC_KERNEL=fused (read at every launch).
-static bool vic_fused_selected() {
+// Variant of the implicit solve, from the environment (read at every launch):
+// the column + finish pair by default; SNAPB_VIC_KERNEL=fused selects the
+// fused kernel of vicf.cu, =cr block cyclic reduction (vic_cr.cu, FP32 form,
+// where it applies).
+static const char* vic_kernel_env() {
   const char* v = std::getenv("SNAPB_VIC_KERNEL");
-  return v && std::strcmp(v, "fused") == 0;
+  return v ? v : "";
 }
+static bool vic_fused_selected() { return std::strcmp(vic_kernel_env(), "fused") == 0; }
+static bool vic_cr_selected() { return std::strcmp(vic_kernel_env(), "cr") == 0; }
 
 cudaError_t launch_vic_column(const Geo& g, const Phys& p, const StageBufs& b,
                               cudaStream_t st) {
@@ -1068,21 +1000,12 @@ cudaError_t launch_vic(const Geo& g, const Phys& p, const StageBufs& b, cudaStre
 
 cudaError_t launch_vic32(const Geo& g, const Phys& p, const StageBufs32& b, cudaStream_t st) {
   if (vic_fused_selected()) return launch_vicf32(g, p, b, st);
+  if (vic_cr_selected() && vic_cr_applies(g, p)) return launch_vic_cr32(g, p, b, st);
   if (vic_n(p) == 5) return launch_vic_n<5>(g, p, b, st);
   return launch_vic_n<3>(g, p, b, st);
 }
 
 // ---- persistent batched variants (ensemble members, FP32 form) ----
-__device__ __forceinline__ void set_stage_vic32(StageBufs32& b, int stage) {
-  double w0 = 1., w1 = 0., w2 = 1.;
-  if (stage == 1) w0 = 3. / 4., w1 = 1. / 4., w2 = 1. / 4.;
-  if (stage == 2) w0 = 1. / 3., w1 = 2. / 3., w2 = 2. / 3.;
-  b.stage = stage;
-  b.wgt0 = w0;
-  b.wgt1 = w1;
-  b.wgt2 = w2;
-}
-
 // V selects the register budget: 0 = compiler's choice, 1 = at least 3 CTAs of
 // 128 threads per SM (~168 registers), 2 = 4 CTAs (128 registers, some spill)
 template <int N, int V>
@@ -1111,7 +1034,7 @@ __global__ void __launch_bounds__(FinCfg<N, NS, float>::threads,
   int64_t tile;
   while (queue_next(q, m, tile)) {  // (starts with a barrier: the last tile is done)
     load_member(s_mem, mem, m);
-    if (threadIdx.x == 0) set_stage_vic32(s_mem.b, stage);
+    if (threadIdx.x == 0) set_stage32(s_mem.b, stage);
     __syncthreads();
     constexpr int TLY = FinCfg<N, NS, float>::layers;
     const int nlb = (s_mem.g.nx1 + TLY - 1) / TLY;

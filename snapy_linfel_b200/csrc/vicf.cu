@@ -45,11 +45,11 @@
 #include "kernels.cuh"
 #include "ring.cuh"
 #include "vic_blocks.cuh"
+#include "vic_common.cuh"
 
 namespace snapb {
 namespace fused {
 
-static inline int vic_n(const Phys& p) { return ((p.implicit_scheme >> 3) & 1) ? 5 : 3; }
 
 // Tile shape and shared-memory plan of the fused kernel for N x N blocks.
 template <int N>
@@ -108,73 +108,6 @@ size_t scratch_bytes(const Geo& g, const Phys& p) {
   const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
   const int64_t tiles = (ncol + 31) / 32;
   return (size_t)(tiles * 32 * (int64_t)g.nx1 * (N * N + N)) * sizeof(double);
-}
-
-// (k, j, il) offset of interior column `col`
-__device__ __forceinline__ int64_t column_base(const Geo& g, int64_t col) {
-  const int nj = g.ju - g.jl + 1;
-  const int j = g.jl + umod(col, nj), k = g.kl + udiv(col, nj);
-  return (int64_t)k * g.s3 + (int64_t)j * g.s2 + g.il;
-}
-
-// ---- state access, FP64 plain form and FP32 perturbation form ----
-// full primitive of variable v at offset off, x1 index xi
-__device__ __forceinline__ double vic_w(const StageBufs& b, int64_t sv, int v, int64_t off,
-                                        int xi) {
-  return b.w[v * sv + off];
-}
-__device__ __forceinline__ double vic_w(const StageBufs32& b, int64_t sv, int v, int64_t off,
-                                        int xi) {
-  double x = (double)b.w[v * sv + off];
-  if (v == IDN) x += b.rb[xi];
-  if (v == IPR) x += b.pb[xi];
-  return x;
-}
-// full primitive of variable v at x1 index xi from a stored value x
-__device__ __forceinline__ double vic_full(const StageBufs&, double x, int v, int xi) { return x; }
-__device__ __forceinline__ double vic_full(const StageBufs32& b, double x, int v, int xi) {
-  if (v == IDN) x += b.rb[xi];
-  if (v == IPR) x += b.pb[xi];
-  return x;
-}
-__device__ __forceinline__ double vic_d(const StageBufs& b, int64_t idx) { return b.D[idx]; }
-__device__ __forceinline__ double vic_d(const StageBufs32& b, int64_t idx) {
-  return (double)b.D[idx];
-}
-__device__ __forceinline__ void vic_set_d(const StageBufs& b, int64_t idx, double x) {
-  b.D[idx] = x;
-}
-__device__ __forceinline__ void vic_set_d(const StageBufs32& b, int64_t idx, double x) {
-  b.D[idx] = (float)x;
-}
-// RK combination of one stored value (u' for the FP32 form: the reference
-// part of u is constant in time, so the combination is the same), from
-// values already loaded (qo = q[o], q0o = q0[o] when stage > 0); the stored
-// q keeps the stored precision
-__device__ __forceinline__ double vic_rk_from(double* q, double* q0, int64_t o, bool first,
-                                              double qo, double q0o, double w0, double w1,
-                                              double w2, double d) {
-  double q0v = first ? qo : q0o;
-  if (first) q0[o] = qo;
-  double qn = w0 * q0v + w1 * qo + w2 * d;
-  q[o] = qn;
-  return qn;
-}
-__device__ __forceinline__ double vic_rk_from(float* q, float* q0, int64_t o, bool first,
-                                              double qo, double q0o, double w0, double w1,
-                                              double w2, double d) {
-  double q0v = first ? qo : q0o;
-  if (first) q0[o] = (float)qo;
-  float qn = (float)(w0 * q0v + w1 * qo + w2 * d);
-  q[o] = qn;
-  return qn;
-}
-// full density of a stored conserved perturbation
-__device__ __forceinline__ double vic_full_rho(const StageBufs&, double u_rho, int) {
-  return u_rho;
-}
-__device__ __forceinline__ double vic_full_rho(const StageBufs32& b, double u_rho, int xi) {
-  return u_rho + b.rb[xi];
 }
 
 // Block construction per form: the FP64 plain form in FP64; the FP32
@@ -669,16 +602,6 @@ cudaError_t launch_vicf32(const Geo& g, const Phys& p, const StageBufs32& b, cud
 namespace fused {
 
 // ---- persistent batched variant (ensemble members, FP32 form) ----
-__device__ __forceinline__ void set_stage_vic32(StageBufs32& b, int stage) {
-  double w0 = 1., w1 = 0., w2 = 1.;
-  if (stage == 1) w0 = 3. / 4., w1 = 1. / 4., w2 = 1. / 4.;
-  if (stage == 2) w0 = 1. / 3., w1 = 2. / 3., w2 = 2. / 3.;
-  b.stage = stage;
-  b.wgt0 = w0;
-  b.wgt1 = w1;
-  b.wgt2 = w2;
-}
-
 // Work items: the 32-column tiles of every member.  Each member's result is
 // bit-identical to snapb_stage_f32 on that member alone (same tile function).
 template <int N, int NS>
@@ -692,7 +615,7 @@ __global__ void __launch_bounds__(VicCfg<N>::NT, N == 3 ? 2 : 1)
   int64_t tile;
   while (queue_next(q, m, tile)) {  // (starts with a barrier: the last tile is done)
     load_member(s_mem, mem, m);
-    if (threadIdx.x == 0) set_stage_vic32(s_mem.b, stage);
+    if (threadIdx.x == 0) set_stage32(s_mem.b, stage);
     __syncthreads();
     vic_tile<N, NS, StageBufs32>(s_mem.g, p, s_mem.b, tile, vic_smem);
   }

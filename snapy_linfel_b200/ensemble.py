@@ -33,7 +33,7 @@ class MemberF32(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("x1_columns", ctypes.c_int32), ("march_segment", ctypes.c_int32),
                 ("ctas_per_sm", ctypes.c_int32), ("vic_block", ctypes.c_int32),
-                ("vic_regs", ctypes.c_int32)]
+                ("vic_regs", ctypes.c_int32), ("vic_kernel", ctypes.c_int32)]
 
     def as_dict(self):
         return {k: int(getattr(self, k)) for k, _ in self._fields_}
@@ -174,14 +174,16 @@ class Ensemble:
         import torch
 
         cand = candidates or {"x1_columns": [0, 4, 8], "march_segment": [16, 32, 64],
-                              "ctas_per_sm": [0, 4, 8], "vic_block": [32, 64, 128],
-                              "vic_regs": [0, 1, 2, 3]}
+                              "ctas_per_sm": [0, 4, 8], "vic_kernel": [0, 1, 2],
+                              "vic_block": [32, 64, 128], "vic_regs": [0, 1, 2]}
         snap = self.save()
         results = []
         best = None
         # coordinate descent: one parameter at a time, starting from the defaults
         current = self.tuning.as_dict()
         for key, values in cand.items():
+            if key in ("vic_block", "vic_regs") and current.get("vic_kernel", 0) != 0:
+                continue  # shapes of the column kernel, not in use
             for v in values:
                 trial = dict(current)
                 trial[key] = v

@@ -150,10 +150,10 @@ def test_ensemble_structs_match_c():
 #include <stddef.h>
 #include "{HEADER}"
 int main() {{
-  printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(snapb_member_f32),
+  printf("%zu %zu %zu %zu %zu %zu %zu\\n", sizeof(snapb_member_f32),
          offsetof(snapb_member_f32, u), offsetof(snapb_member_f32, workspace),
          offsetof(snapb_member_f32, workspace_bytes), sizeof(snapb_ensemble_tuning),
-         offsetof(snapb_ensemble_tuning, vic_regs));
+         offsetof(snapb_ensemble_tuning, vic_regs), offsetof(snapb_ensemble_tuning, vic_kernel));
   return 0;
 }}"""
     d = os.path.join(REPO, "_work")
@@ -164,7 +164,8 @@ int main() {{
     subprocess.run(["gcc", c_path, "-o", exe], check=True)
     vals = list(map(int, subprocess.run([exe], capture_output=True, text=True).stdout.split()))
     py = [ctypes.sizeof(MemberF32), MemberF32.u.offset, MemberF32.workspace.offset,
-          MemberF32.workspace_bytes.offset, ctypes.sizeof(Tuning), Tuning.vic_regs.offset]
+          MemberF32.workspace_bytes.offset, ctypes.sizeof(Tuning), Tuning.vic_regs.offset,
+          Tuning.vic_kernel.offset]
     assert vals == py
 
 

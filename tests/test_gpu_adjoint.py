@@ -364,6 +364,13 @@ def test_rollout_gradient_fd(L):
         with torch.no_grad():
             fd = richardson(lambda t: float(J(dth0 + t * v)), 1e-3)
         check(fd, dot(grad, v), f"rollout trial {trial}")
+    # keeping every step's stage inputs in the forward pass (checkpoint_every=0)
+    # gives the gradient of the checkpointed re-run exactly
+    x0 = dth0.clone().requires_grad_(True)
+    uT, _ = A.rollout(opts, state(x0), None, dts, checkpoint_every=0)
+    j0 = (0.5 * (uT[1] ** 2 + uT[2] ** 2 + uT[3] ** 2) / uT[0])[it].sum()
+    (grad0,) = torch.autograd.grad(j0, x0)
+    assert torch.equal(grad0, grad)
 
 
 def _face_states(cfg, regime, dim, gen):

@@ -51,11 +51,15 @@ def batched(members, steps, dev, tuning=None, graph=False):
 
 @pytest.mark.parametrize("scheme,riemann", [(1, "lmars"), (9, "roe"), (0, "hllc")])
 def test_batched_matches_single_blocks(dev, scheme, riemann):
+    from snapy_linfel_b200 import _lib
+
     members = small_members(implicit_scheme=scheme, riemann=riemann)
     ref = singles(members, 3, dev)
     _, got = batched(members, 3, dev)
     for k, (a, b) in enumerate(zip(got, ref)):
         assert torch.equal(a, b), f"member {k}: max diff {float((a - b).abs().max())}"
+    # the x1 sweeps' bulk copies all completed
+    assert _lib.lib().snapb_bulk_copy_timeouts() == 0
 
 
 def test_tile_shapes_and_graph_replay_are_exact(dev):
@@ -69,6 +73,24 @@ def test_tile_shapes_and_graph_replay_are_exact(dev):
     _, got = batched(members, 2, dev, graph=True)
     for a, b in zip(got, ref):
         assert torch.equal(a, b)
+
+
+def test_x1_prefetch_across_members_of_different_heights(dev):
+    """the batched x1 sweep stages the next tile (of any member) while the
+    current one's faces run: with one CTA per SM every CTA takes many tiles,
+    and members of 8 and 40 layers alternate, so a tile's staging follows
+    rows of a longer or shorter column; every member matches its one-block
+    run exactly"""
+    from snapy_linfel_b200 import _lib
+
+    members = problems.ensemble_members(n=6, seed=21, horiz=(12, 20), vert=(8, 40),
+                                        riemann="lmars", implicit_scheme=1)
+    ref = singles(members, 2, dev)
+    for tuning in ({"x1_columns": 8, "ctas_per_sm": 1}, {"x1_columns": 2, "ctas_per_sm": 1}):
+        _, got = batched(members, 2, dev, tuning=tuning)
+        for k, (a, b) in enumerate(zip(got, ref)):
+            assert torch.equal(a, b), f"{tuning} member {k}: {float((a - b).abs().max())}"
+    assert _lib.lib().snapb_bulk_copy_timeouts() == 0
 
 
 def test_per_member_dt(dev):
@@ -97,13 +119,30 @@ def test_autotuner_keeps_results(dev):
         assert torch.equal(a, b)
 
 
-def test_fused_implicit_variant_batched_equals_one_block(dev, monkeypatch):
-    """the fused implicit-solve kernel (tuning vic_regs = 3, and
-    SNAPB_VIC_KERNEL=fused for the one-block path) gives every member exactly
-    the one-block result"""
-    monkeypatch.setenv("SNAPB_VIC_KERNEL", "fused")
+@pytest.mark.parametrize("kernel,env", [(1, "cr"), (2, "fused")])
+def test_implicit_variants_batched_equal_one_block(dev, monkeypatch, kernel, env):
+    """block cyclic reduction (tuning vic_kernel = 1, SNAPB_VIC_KERNEL=cr for the
+    one-block path) and the fused kernel (vic_kernel = 2, SNAPB_VIC_KERNEL=fused)
+    give every member exactly the one-block result"""
+    monkeypatch.setenv("SNAPB_VIC_KERNEL", env)
     members = small_members(n=4, seed=11)
     ref = singles(members, 2, dev)
-    _, got = batched(members, 2, dev, tuning={"vic_regs": 3})
+    _, got = batched(members, 2, dev, tuning={"vic_kernel": kernel})
     for k, (a, b) in enumerate(zip(got, ref)):
         assert torch.equal(a, b), f"member {k}: max diff {float((a - b).abs().max())}"
+
+
+def test_cyclic_reduction_agrees_with_block_thomas(dev):
+    """block cyclic reduction and the block-Thomas column kernel (the default)
+    eliminate the same system in FP64 in different orders: the FP32 states
+    after two steps agree to a few FP32 ulps"""
+    members = problems.ensemble_members(n=6, seed=13, horiz=(8, 12), vert=(7, 13, 16),
+                                        riemann="lmars", implicit_scheme=1)
+    _, th = batched(members, 2, dev)
+    _, cr = batched(members, 2, dev, tuning={"vic_kernel": 1})
+    for k, (a, b) in enumerate(zip(cr, th)):
+        assert torch.isfinite(a).all()
+        for v in range(a.shape[0]):
+            scale = float(b[v].abs().max())
+            err = float((a[v] - b[v]).abs().max())
+            assert err <= 1e-5 * max(scale, 1e-30), f"member {k} var {v}: {err} vs {scale}"
