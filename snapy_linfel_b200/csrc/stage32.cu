@@ -314,8 +314,7 @@ __device__ __forceinline__ void x1_32_convert(const Geo& g, const Phys& p, const
 
 template <int NS>
 __device__ __forceinline__ void x1_32_faces(const Geo& g, const Phys& p, const StageBufs32& b,
-                                            int C, int last, int64_t col0, const float* smf,
-                                            float* sfe) {
+                                            int C, int last, int64_t col0, const float* smf) {
   constexpr int NV = 5 + NS;
   const int nc1 = g.nc1, il = g.il, iu = g.iu;
   const int lane = threadIdx.x & 31, c = threadIdx.x >> 5;
@@ -390,58 +389,39 @@ __device__ __forceinline__ void x1_32_faces(const Geo& g, const Phys& p, const S
       for (int v = 0; v < NV; ++v) b.D[v * sv + off] = d[v];
     }
   };
-  // faces il .. iu in rounds of 32 (face f0 + lane); the flux difference of
-  // cell f takes face f+1 from the next lane, lane 31 that of the next
-  // round's lane 0 one round later; cell iu waits for face iu+1 (below)
-  const bool mine = interior(c);
-  float Fkeep[NV];  // lane 31: its face of the previous round; the lane of face iu: that face
+  // faces il .. iu+1 in rounds of 32 (face f0 + lane); the flux difference
+  // of cell f takes face f+1 from the next lane, lane 31 that of the next
+  // round's lane 0 one round later
+  if (!interior(c)) return;  // the whole warp
+  float Fkeep[NV];  // lane 31: its face of the previous round
 #pragma unroll
   for (int v = 0; v < NV; ++v) Fkeep[v] = 0.f;
-  if (mine) {
-    for (int f0 = il; f0 <= iu; f0 += 32) {
-      const int f = f0 + lane;
-      float F[NV];
-      if (f <= iu) {
-        face(c, f, F);
-      } else {
-#pragma unroll
-        for (int v = 0; v < NV; ++v) F[v] = 0.f;
-      }
-      float Fn[NV];  // lanes 0 .. 30: face f + 1; lane 31: this round's first face
-#pragma unroll
-      for (int v = 0; v < NV; ++v) {
-        const float dn = __shfl_down_sync(0xffffffffu, F[v], 1);
-        const float f0v = __shfl_sync(0xffffffffu, F[v], 0);
-        Fn[v] = lane < 31 ? dn : f0v;
-      }
-      // this lane's cell: f (lanes 0 .. 30), the previous round's last (lane 31)
-      const int i = lane < 31 ? f : f0 - 1;
-      if (i >= il && i < iu) {
-        float d[NV];
-#pragma unroll
-        for (int v = 0; v < NV; ++v) d[v] = A1 * Fn[v] - A1 * (lane < 31 ? F[v] : Fkeep[v]);
-        finish(i, d);
-      }
-      if (lane == 31 || f == iu) {
-#pragma unroll
-        for (int v = 0; v < NV; ++v) Fkeep[v] = F[v];
-      }
-    }
-  }
-  // face iu+1 of every interior column of the tile, one lane per column
-  if (c == 0 && lane < C && interior(lane)) {
+  for (int f0 = il; f0 <= iu + 1; f0 += 32) {
+    const int f = f0 + lane;
     float F[NV];
-    face(lane, iu + 1, F);
+    if (f <= iu + 1) {
+      face(c, f, F);
+    } else {
 #pragma unroll
-    for (int v = 0; v < NV; ++v) sfe[lane * NV + v] = F[v];
-  }
-  __syncthreads();
-  // cell iu: the lane that computed face iu
-  if (mine && lane == ((iu - il) & 31)) {
-    float d[NV];
+      for (int v = 0; v < NV; ++v) F[v] = 0.f;
+    }
+    float Fn[NV];  // lanes 0 .. 30: face f + 1; lane 31: this round's first face
 #pragma unroll
-    for (int v = 0; v < NV; ++v) d[v] = A1 * sfe[c * NV + v] - A1 * Fkeep[v];
-    finish(iu, d);
+    for (int v = 0; v < NV; ++v) {
+      const float dn = __shfl_down_sync(0xffffffffu, F[v], 1);
+      const float f0v = __shfl_sync(0xffffffffu, F[v], 0);
+      Fn[v] = lane < 31 ? dn : f0v;
+    }
+    // this lane's cell: f (lanes 0 .. 30), the previous round's last (lane 31)
+    const int i = lane < 31 ? f : f0 - 1;
+    if (i >= il && i <= iu) {
+      float d[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) d[v] = A1 * Fn[v] - A1 * (lane < 31 ? F[v] : Fkeep[v]);
+      finish(i, d);
+    }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) Fkeep[v] = F[v];
   }
 }
 
@@ -450,7 +430,6 @@ template <int NS>
 __global__ void __launch_bounds__(512, 2) k_x1_32(Geo g, Phys p, StageBufs32 b, int C, int last) {
   extern __shared__ __align__(16) float smf[];
   __shared__ uint64_t bar;
-  __shared__ float sfe[16 * (5 + NS)];  // face iu+1 of each column
   if (threadIdx.x == 0) mbar_init(&bar, 1);
   __syncthreads();
   const int64_t col0 = (int64_t)blockIdx.x * C;
@@ -461,7 +440,7 @@ __global__ void __launch_bounds__(512, 2) k_x1_32(Geo g, Phys p, StageBufs32 b, 
     return;
   }
   x1_32_convert<NS>(g, p, b, C, col0, smf, g.nc1);
-  x1_32_faces<NS>(g, p, b, C, last, col0, smf, sfe);
+  x1_32_faces<NS>(g, p, b, C, last, col0, smf);
 }
 
 // ---------------------------------------------------------------------------
@@ -736,7 +715,6 @@ __global__ void __launch_bounds__(512, 2) k_x1_32_batch(const Member32* __restri
   __shared__ Member32 s_mem[2];  // descriptors of the current and the next tile's member
   __shared__ uint64_t bar;       // completion of a tile's bulk copies
   __shared__ unsigned long long s_item;
-  __shared__ float sfe[16 * (5 + NS)];  // face iu+1 of each column
   const int tid = threadIdx.x;
   if (tid == 0) {
     mbar_init(&bar, 1);
@@ -778,7 +756,7 @@ __global__ void __launch_bounds__(512, 2) k_x1_32_batch(const Member32* __restri
       __syncwarp();
       x1_32_stage<NS>(nxt.g, nxt.b, nxt.x1_cols, ntile * nxt.x1_cols, smf, nc1max, &bar);
     }
-    x1_32_faces<NS>(cur.g, p, cur.b, C, last, col0, smf, sfe);
+    x1_32_faces<NS>(cur.g, p, cur.b, C, last, col0, smf);
     if (!more) return;
     __syncthreads();  // this tile's rows are read; the next descriptor is in place
     buf ^= 1;
