@@ -307,8 +307,8 @@ def rel_errors(a, b, it):
 # captures of the first 12 ensemble members, scaled to a launch by the cells
 # it processes (their traffic grows in proportion to the cells).  None: not
 # captured for the current build.
-NCU_TRAFFIC_PER_CELL_F32 = {"x1_sweep": 68.2, "x2_sweep": 63.2, "x3_sweep": 63.2,
-                            "implicit_vic": None}
+NCU_TRAFFIC_PER_CELL_F32 = {"x1_sweep": 70.7, "x2_sweep": 66.2, "x3_sweep": 66.2,
+                            "implicit_vic": 348.5}
 
 
 def dominant_roofline(kern, cfg, cells, elem, peak, peak_src):
