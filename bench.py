@@ -307,6 +307,9 @@ def rel_errors(a, b, it):
 # captures of the first 12 ensemble members, scaled to a launch by the cells
 # it processes (their traffic grows in proportion to the cells).  None: not
 # captured for the current build.
+# member groups of the end-to-end form (copies of one group overlap the others' steps)
+E2E_GROUPS = 4
+
 NCU_TRAFFIC_PER_CELL_F32 = {"x1_sweep": 70.7, "x2_sweep": 66.2, "x3_sweep": 66.2,
                             "implicit_vic": 348.5}
 
@@ -622,7 +625,7 @@ def run_ensemble(args):
     import torch.distributed as dist
 
     from snapy_linfel_b200 import _lib, problems
-    from snapy_linfel_b200.ensemble import Ensemble
+    from snapy_linfel_b200.ensemble import Ensemble, StreamedEnsemble
     from snapy_linfel_b200.mesh import MeshBlock
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -695,11 +698,29 @@ def run_ensemble(args):
     torch.cuda.synchronize()
     kern32 = _lib.timing_query()
     _lib.timing_enable(False)
-    # end to end: every member's state from pinned host memory and back, per step
+    # end to end: every member's state from pinned host memory and back, per
+    # step.  (a) StreamedEnsemble: members in groups, each on its own stream,
+    # so one group's copies overlap the other groups' steps; (b) one stream:
+    # all copies in, the step, all copies out.
+    sens = StreamedEnsemble(members, groups=E2E_GROUPS, device=dev, tuning=tune["best"])
+    sens.capture()
+    hus = sens.host_states()
+    nbytes = sum(h.numel() * 4 for h in hus)
+    for _ in range(args.warmup):
+        sens.step(hus)
+    sens.wait()
+    barrier()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        sens.step(hus)
+    sens.wait()
+    ev1.record(stream)
+    barrier()
+    e2e = cells_total * 3 * args.steps / (max_ms(ev0.elapsed_time(ev1)) / 1e3) / 1e6
+    del sens, hus
     hus = [torch.empty(b.hydro_u.shape, dtype=torch.float32).pin_memory() for b in ens.blocks]
     for h, b in zip(hus, ens.blocks):
         h.copy_(b.hydro_u.cpu())
-    nbytes = sum(h.numel() * 4 for h in hus)
     barrier()
     ev0.record(stream)
     for _ in range(args.steps):
@@ -710,8 +731,9 @@ def run_ensemble(args):
             h.copy_(b.hydro_u, non_blocking=True)
     ev1.record(stream)
     barrier()
-    e2e = cells_total * 3 * args.steps / (max_ms(ev0.elapsed_time(ev1)) / 1e3) / 1e6
+    e2e_serial = cells_total * 3 * args.steps / (max_ms(ev0.elapsed_time(ev1)) / 1e3) / 1e6
     del hus
+    torch.cuda.empty_cache()
 
     # ---- plain FP64: member after member through snapb_stage, the whole
     # step (every member's CFL and three stages) replayed from one CUDA graph
@@ -847,6 +869,8 @@ def run_ensemble(args):
             "adjoint": adj,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+                    "form": f"StreamedEnsemble, {E2E_GROUPS} groups on their own streams",
+                    "one_stream_value": e2e_serial,
                     "d2h_bytes_per_step": nbytes},
             "gpu_launches": ensemble_launches_per_step(cfg0, tune["best"]) * args.steps,
             "gpu_launches_counts": "this rank's kernels in the timed region",

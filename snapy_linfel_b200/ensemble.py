@@ -212,3 +212,92 @@ class Ensemble:
         self.restore(snap)
         return {"best": best[0], "best_ms_per_step": best[1],
                 "trials": [{"tuning": t, "ms_per_step": m} for t, m in results]}
+
+
+class StreamedEnsemble:
+    """An ensemble whose states live in pinned host memory: every step copies
+    each member's FP32 state (``hydro_u``, ghosts included) in and its result
+    back out.  The members are split into ``groups`` sub-ensembles balanced by
+    cells, each an ``Ensemble`` with its own CUDA stream and step graph, so
+    the host-to-device copies of one group, the device-to-host copies of
+    another (the two copy directions run on separate engines) and the steps
+    of a third overlap.  A group's copies and steps are ordered on its own
+    stream; groups never wait for each other, so ``step()`` returns after
+    queueing and ``wait()`` joins every group into the current stream.
+
+    members: as ``Ensemble``; host: one pinned FP32 tensor per member, in
+    member order, shaped like its ``hydro_u`` (``host_states()`` makes them
+    from the current states)."""
+
+    def __init__(self, members, groups: int = 4, device=None, tuning: dict | None = None):
+        import torch
+
+        self.device = torch.device(device if device is not None else "cuda")
+        cells = [o.hydro.nx1 * o.hydro.nx2 * o.hydro.nx3 for o, _, _ in members]
+        groups = max(1, min(groups, len(members)))
+        load = [0] * groups
+        self.slots = [[] for _ in range(groups)]  # member indices of each group
+        for m in sorted(range(len(members)), key=lambda k: -cells[k]):
+            g = min(range(groups), key=lambda k: load[k])
+            self.slots[g].append(m)
+            load[g] += cells[m]
+        self.parts = [Ensemble([members[m] for m in idx], device=self.device, tuning=tuning)
+                      for idx in self.slots]
+        self.where = {}  # member -> (group, position)
+        for g, idx in enumerate(self.slots):
+            for k, m in enumerate(idx):
+                self.where[m] = (g, k)
+        self.streams = [torch.cuda.Stream(device=self.device) for _ in self.parts]
+        cur = torch.cuda.current_stream(self.device)
+        for s in self.streams:
+            s.wait_stream(cur)
+
+    @property
+    def blocks(self):
+        """the member blocks in member order"""
+        return [self.parts[g].blocks[k] for g, k in (self.where[m] for m in range(len(self.where)))]
+
+    @property
+    def cells(self):
+        return sum(p.cells for p in self.parts)
+
+    def host_states(self):
+        """pinned host copies of the members' current states, in member order"""
+        import torch
+
+        out = []
+        for b in self.blocks:
+            h = torch.empty(b.hydro_u.shape, dtype=torch.float32).pin_memory()
+            h.copy_(b.hydro_u.cpu())
+            out.append(h)
+        return out
+
+    def capture(self):
+        """capture each group's step in its own CUDA graph"""
+        import torch
+
+        self.wait()
+        for p in self.parts:
+            p.capture()
+        torch.cuda.synchronize(self.device)
+
+    def step(self, host):
+        """one step of every member from and back to its host state (queued
+        on the groups' streams)"""
+        import torch
+
+        for g, (p, s) in enumerate(zip(self.parts, self.streams)):
+            with torch.cuda.stream(s):
+                for k, m in enumerate(self.slots[g]):
+                    p.blocks[k].hydro_u.copy_(host[m], non_blocking=True)
+                p.step()
+                for k, m in enumerate(self.slots[g]):
+                    host[m].copy_(p.blocks[k].hydro_u, non_blocking=True)
+
+    def wait(self):
+        """join every group's queued work into the current stream"""
+        import torch
+
+        cur = torch.cuda.current_stream(self.device)
+        for s in self.streams:
+            cur.wait_stream(s)

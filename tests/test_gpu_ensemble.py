@@ -93,6 +93,25 @@ def test_x1_prefetch_across_members_of_different_heights(dev):
     assert _lib.lib().snapb_bulk_copy_timeouts() == 0
 
 
+def test_streamed_ensemble_from_host_states(dev):
+    """members stepped from pinned host states in groups on their own streams
+    (copies of one group overlapping the steps of the others) end exactly
+    where their one-block runs end"""
+    from snapy_linfel_b200.ensemble import StreamedEnsemble
+
+    members = small_members(n=5, seed=17)
+    ref = singles(members, 3, dev)
+    sens = StreamedEnsemble(members, groups=3, device=dev)
+    sens.capture()
+    host = sens.host_states()
+    for _ in range(3):
+        sens.step(host)
+    sens.wait()
+    torch.cuda.synchronize()
+    for k, (h, b) in enumerate(zip(host, ref)):
+        assert torch.equal(h.to(dev), b), f"member {k}: {float((h.to(dev) - b).abs().max())}"
+
+
 def test_per_member_dt(dev):
     from snapy_linfel_b200.mesh import MeshBlockF32
 
