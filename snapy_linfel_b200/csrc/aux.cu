@@ -89,10 +89,8 @@ __global__ void k_bc(Geo g, AxisBC a1, AxisBC a2, AxisBC a3, double* var, int nv
   if (s >= bc_shell_slots(g)) return;
   const int nc1 = g.nc1, nc2 = g.nc2;
   const int64_t sv = g.sv;
-  const int64_t t = bc_shell_cell(g, s);
-  int i = umod(t, nc1);
-  int j = umod(udiv(t, nc1), nc2);
-  int k = udiv(t, (int64_t)nc1 * nc2);
+  int i, j, k;
+  const int64_t t = bc_shell_cell(g, s, i, j, k);
   bool f1, f2, f3;
   int si = bc_map(a1, i, f1), sj = bc_map(a2, j, f2), sk = bc_map(a3, k, f3);
   if (si == i && sj == j && sk == k) return;  // interior (or identity-mapped) cell

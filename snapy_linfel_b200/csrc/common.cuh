@@ -125,11 +125,12 @@ __host__ __device__ __forceinline__ int64_t bc_shell_slots(const Geo& g) {
   return A + (c1 + c2) * g.nc1;
 }
 
-__host__ __device__ __forceinline__ int64_t bc_shell_cell(const Geo& g, int64_t s) {
+// flat index of ghost slot s, with its (i, j, k)
+__host__ __device__ __forceinline__ int64_t bc_shell_cell(const Geo& g, int64_t s, int& i, int& j,
+                                                          int& k) {
   const int64_t nj = g.ju - g.jl + 1, nk = g.ku - g.kl + 1;
   const int ng2 = 2 * g.ng;
   const int64_t A = g.nc1 > 1 ? nj * nk * ng2 : 0;
-  int i, j, k;
   if (s < A) {
     const int c = umod(s, ng2);
     const int row = udiv(s, ng2);

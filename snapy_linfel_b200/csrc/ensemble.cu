@@ -45,8 +45,8 @@ __global__ void __launch_bounds__(256) k_cfl32_batch(const Member32* __restrict_
     const int ni = g.iu - g.il + 1, nj = g.ju - g.jl + 1, nk = g.ku - g.kl + 1;
     const int64_t n = (int64_t)ni * nj * nk;
     double m1 = 1.7e308, m2 = 1.7e308, m3 = 1.7e308;
-    const int64_t t0 = tile * 1024;
-    for (int64_t t = t0 + threadIdx.x; t < min(t0 + 1024, n); t += blockDim.x) {
+    const int64_t t0 = tile * kCflItem;
+    for (int64_t t = t0 + threadIdx.x; t < min(t0 + kCflItem, n); t += blockDim.x) {
       int i = g.il + umod(t, ni);
       int j = g.jl + umod(udiv(t, ni), nj);
       int k = g.kl + udiv(t, (int64_t)ni * nj);
@@ -181,7 +181,8 @@ int plan(snapb_ensemble* e) {
     mb.vic_cols = t.vic_block > 0 ? t.vic_block : 64;
     int64_t tiles[PH_COUNT] = {0};
     tiles[PH_X1] = e->a1 ? (ncol1 + C - 1) / C : 0;
-    tiles[PH_X1REV] = e->a1 && e->p.grav1 != 0. ? (ncol1 * 2 * g.ng + 255) / 256 : 0;
+    tiles[PH_X1REV] = e->a1 && e->p.grav1 != 0.
+                          ? (ncol1 * 2 * g.ng + kRevisionItem - 1) / kRevisionItem : 0;
     tiles[PH_X2] = e->a2 ? ((lines2 + 127) / 128) * mb.nseg2 : 0;
     tiles[PH_X3] = e->a3 ? ((lines3 + 127) / 128) * mb.nseg3 : 0;
     tiles[PH_VCOL] = e->p.implicit_scheme ? (ncolv + mb.vic_cols - 1) / mb.vic_cols : 0;
@@ -192,15 +193,15 @@ int plan(snapb_ensemble* e) {
     const int fc = vicf_tile_columns();
     tiles[PH_VFUSED] = e->p.implicit_scheme ? (ncolv + fc - 1) / fc : 0;
     tiles[PH_VCR] = e->p.implicit_scheme ? ncolv : 0;  // one column per tile
-    // ghost-shell cells, 256 per tile (same count as bc_shell_slots)
+    // ghost-shell cells, kShellItem per tile (same count as bc_shell_slots)
     const int64_t nj = g.ju - g.jl + 1, nk = g.ku - g.kl + 1;
     const int64_t shell = (g.nc1 > 1 ? nj * nk * 2 * g.ng : 0) +
                           ((g.nc3 > 1 ? (int64_t)2 * g.ng * g.nc2 : 0) +
                            (g.nc2 > 1 ? nk * 2 * g.ng : 0)) * g.nc1;
-    tiles[PH_BCU] = (shell + 255) / 256;
-    tiles[PH_BCS] = e->p.nscalar ? (shell + 255) / 256 : 0;
+    tiles[PH_BCU] = (shell + kShellItem - 1) / kShellItem;
+    tiles[PH_BCS] = e->p.nscalar ? (shell + kShellItem - 1) / kShellItem : 0;
     int64_t ncell = (int64_t)(g.iu - g.il + 1) * (g.ju - g.jl + 1) * (g.ku - g.kl + 1);
-    tiles[PH_CFL] = (ncell + 1023) / 1024;
+    tiles[PH_CFL] = (ncell + kCflItem - 1) / kCflItem;
     for (int ph = 0; ph < PH_COUNT; ++ph) e->prefix[ph][m + 1] = e->prefix[ph][m] + tiles[ph];
   }
   // one x1 tile width for the ensemble (the CTA size of the x1 launch): the

@@ -208,6 +208,11 @@ cudaError_t launch_x1_ghost_revision32_batch(const Member32* mem, const Phys& p,
 StageBufs32 bufs32_of(const snapb_hydro_config& c, void* ws);
 size_t workspace_size_f32_of(const snapb_hydro_config& c);
 constexpr int kVicFinishCols = 32;    // columns per implicit-finish tile
+// work items of the small batched phases (cells or ghost slots per queue item):
+// large enough that the queue fetch and the CTA's reductions are amortised
+constexpr int kCflItem = 8192;       // interior cells per CFL item
+constexpr int kShellItem = 2048;     // ghost-shell slots per boundary-fill item
+constexpr int kRevisionItem = 1024;  // ghost-revision slots per item
 
 // RK3 (Shu-Osher) stage weights: u = wgt0*u0 + wgt1*u + wgt2*du
 inline void rk3_weights(int stage, double& a, double& b, double& c) {

@@ -591,14 +591,11 @@ __device__ __forceinline__ int bc_map32(const AxisBC32& a, int i, bool& flip) {
   return i;
 }
 
-__device__ __forceinline__ void bc32_cell(int nc1, int nc2, int nc3, int64_t sv, AxisBC32 a1,
+// ghost cell t = (i, j, k) of the shell from its image inside the block
+__device__ __forceinline__ void bc32_cell(int nc1, int nc2, int64_t sv, AxisBC32 a1,
                                           AxisBC32 a2, AxisBC32 a3, float* var, int nv,
                                           int kind, const double* rb, const double* pb,
-                                          double igm1, int64_t t) {
-  if (t >= sv) return;
-  int i = umod(t, nc1);
-  int j = umod(udiv(t, nc1), nc2);
-  int k = udiv(t, (int64_t)nc1 * nc2);
+                                          double igm1, int64_t t, int i, int j, int k) {
   bool f1, f2, f3;
   int si = bc_map32(a1, i, f1), sj = bc_map32(a2, j, f2), sk = bc_map32(a3, k, f3);
   if (si == i && sj == j && sk == k) return;
@@ -619,8 +616,9 @@ __global__ void k_bc32(Geo g, AxisBC32 a1, AxisBC32 a2, AxisBC32 a3, float* var,
                        int kind, const double* rb, const double* pb, double igm1) {
   const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= bc_shell_slots(g)) return;
-  bc32_cell(g.nc1, g.nc2, g.nc3, g.sv, a1, a2, a3, var, nv, kind, rb, pb, igm1,
-            bc_shell_cell(g, s));
+  int i, j, k;
+  const int64_t t = bc_shell_cell(g, s, i, j, k);
+  bc32_cell(g.nc1, g.nc2, g.sv, a1, a2, a3, var, nv, kind, rb, pb, igm1, t, i, j, k);
 }
 
 // conversions between the FP64 state and the FP32 perturbation
@@ -765,15 +763,16 @@ __global__ void __launch_bounds__(512, 2) k_x1_32_batch(const Member32* __restri
   }
 }
 
-// the x1 ghost revision of every member, 256 slots per tile
+// the x1 ghost revision of every member, kRevisionItem slots per tile
 __global__ void __launch_bounds__(256) k_x1_ghost_revision32_batch(const Member32* __restrict__ mem,
                                                                    Phys p, WorkQueue q) {
   int m;
   int64_t tile;
   while (queue_next(q, m, tile)) {
     const Geo& g = mem[m].g;
-    const int64_t slot = tile * blockDim.x + threadIdx.x;
-    if (slot < (int64_t)g.nc2 * g.nc3 * 2 * g.ng) x1_ghost_revision32(g, p, mem[m].b, slot);
+    const int64_t n = (int64_t)g.nc2 * g.nc3 * 2 * g.ng, s0 = tile * kRevisionItem;
+    for (int64_t slot = s0 + threadIdx.x; slot < min(s0 + kRevisionItem, n); slot += blockDim.x)
+      x1_ghost_revision32(g, p, mem[m].b, slot);
   }
 }
 
@@ -803,15 +802,18 @@ __global__ void __launch_bounds__(256) k_bc32_batch(const Member32* __restrict__
   while (queue_next(q, m, tile)) {
     const Geo& g = mem[m].g;
     const Member32& mb = mem[m];
-    const int64_t slot = tile * blockDim.x + threadIdx.x;
-    if (slot >= bc_shell_slots(g)) continue;
     AxisBC32 a1{g.nc1, g.ng, mb.bc[0], mb.bc[1]};
     AxisBC32 a2{g.nc2, g.ng, mb.bc[2], mb.bc[3]};
     AxisBC32 a3{g.nc3, g.ng, mb.bc[4], mb.bc[5]};
     float* var = kind == SNAPB_SCALAR ? mb.b.s : mb.b.u;
     const int nv = kind == SNAPB_SCALAR ? p.nscalar : 5;
-    bc32_cell(g.nc1, g.nc2, g.nc3, g.sv, a1, a2, a3, var, nv, kind, mb.b.rb, mb.b.pb, igm1,
-              bc_shell_cell(g, slot));
+    const int64_t n = bc_shell_slots(g), s0 = tile * kShellItem;
+    for (int64_t slot = s0 + threadIdx.x; slot < min(s0 + kShellItem, n); slot += blockDim.x) {
+      int i, j, k;
+      const int64_t t = bc_shell_cell(g, slot, i, j, k);
+      bc32_cell(g.nc1, g.nc2, g.sv, a1, a2, a3, var, nv, kind, mb.b.rb, mb.b.pb, igm1, t, i, j,
+                k);
+    }
   }
 }
 
