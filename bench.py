@@ -620,6 +620,43 @@ def perturbation_fields(u, cfg, rb, pb):
     return [(rho - rbv)[it], (theta - theta_bar)[it], (u[1] / rho)[it]]
 
 
+def run_cpp_host_ensemble(members, tuning, args, stream, barrier, max_ms, cells_total):
+    """Mcell-updates/s of the ensemble stepped by the C++ host module's
+    Ensemble (eager launches on the current stream), or None if that module
+    is not built."""
+    import torch
+
+    try:
+        from snapy_linfel_b200 import _snapb_host
+    except ImportError as e:
+        return {"value": None, "unavailable": f"C++ host module not built: {e}"}
+    from snapy_linfel_b200.config import config_dict
+
+    blocks = []
+    for opts, w, r in members:
+        b = _snapb_host.MeshBlockF32(config_dict(opts.hydro), opts.integration.cfl, 0)
+        b.initialize(torch.from_numpy(w), None if r is None else torch.from_numpy(r), "mean")
+        blocks.append(b)
+    keys = ("x1_columns", "march_segment", "ctas_per_sm", "vic_block", "vic_regs", "vic_kernel")
+    ens = _snapb_host.Ensemble(blocks, members[0][0].integration.cfl,
+                               [int(tuning.get(k, 0)) for k in keys])
+    for _ in range(args.warmup):
+        ens.step()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        ens.step()
+    e1.record(stream)
+    barrier()
+    ms = max_ms(e0.elapsed_time(e1))
+    del ens, blocks
+    torch.cuda.empty_cache()
+    return {"value": cells_total * 3 * args.steps / (ms / 1e3) / 1e6,
+            "ms_per_step": ms / args.steps,
+            "form": "C++ host module (_snapb_host.Ensemble over MeshBlockF32), eager launches"}
+
+
 def run_ensemble(args):
     import torch
     import torch.distributed as dist
@@ -698,6 +735,11 @@ def run_ensemble(args):
     torch.cuda.synchronize()
     kern32 = _lib.timing_query()
     _lib.timing_enable(False)
+    # the same ensemble stepped through the C++ host module (libtorch host
+    # code over the C ABI: MeshBlockF32 members and the Ensemble plan), eager
+    host_cpp = run_cpp_host_ensemble(members, tune["best"], args, stream, barrier, max_ms,
+                                     cells_total)
+
     # end to end: every member's state from pinned host memory and back, per
     # step.  (a) StreamedEnsemble: members in groups, each on its own stream,
     # so one group's copies overlap the other groups' steps; (b) one stream:
@@ -859,6 +901,7 @@ def run_ensemble(args):
                                                       "ms_per_step": ms64 / args.steps},
                 "plain_fp64_member_by_member_eager": {"value": value64_eager,
                                                       "ms_per_step": ms64_eager / args.steps},
+                "batched_fp32_cpp_host": host_cpp,
                 "batched_fp32_over_plain_fp64": value32 / value64,
                 "batched_fp32_over_plain_fp64_eager": value32 / value64_eager,
                 "single_domain_384x384x192": single,

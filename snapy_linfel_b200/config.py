@@ -195,6 +195,15 @@ def _get(d, *keys, default=None):
     return d
 
 
+def config_dict(c) -> dict:
+    """A HydroConfig as the plain dict the C++ host module's constructors take
+    (every field of snapb_hydro_config; bc and disable_flux as lists)."""
+    d = {f: getattr(c, f) for f, _ in c._fields_ if f not in ("bc", "disable_flux", "reserved")}
+    d["bc"] = list(c.bc)
+    d["disable_flux"] = list(c.disable_flux)
+    return d
+
+
 def _from_dict(cfg: dict) -> MeshBlockOptions:
     geo = cfg.get("geometry", {}) or {}
     if geo.get("type", "cartesian") != "cartesian":

@@ -12,10 +12,9 @@ torch = pytest.importorskip("torch")
 
 
 def _cfg_dict(c):
-    d = {f: getattr(c, f) for f, _ in c._fields_ if f not in ("bc", "disable_flux", "reserved")}
-    d["bc"] = list(c.bc)
-    d["disable_flux"] = list(c.disable_flux)
-    return d
+    from snapy_linfel_b200.config import config_dict
+
+    return config_dict(c)
 
 
 def test_host_meshblock_matches_oracle(oracle):
