@@ -6,7 +6,9 @@
 //                   the Roe-averaged |A| = R |Lambda| R^-1 once per interface
 //                   (the reference forms it twice, once per neighbouring cell)
 //                   and the flux Jacobian once per cell, a layer ahead of the
-//                   elimination that consumes them — then the block-Thomas
+//                   elimination that consumes them (formed in the iteration
+//                   that eliminates the layer below, so the two independent
+//                   dependency chains interleave) — then the block-Thomas
 //                   elimination, back substitution and the MS-VIC column
 //                   sums.  Only the reduced blocks and the partial solutions
 //                   go through HBM;
@@ -311,46 +313,56 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
   const double dt = *b.dt;
   const double V = g.vol;
   const BT Aa = (BT)g.A1, hiv = (BT)(0.5 / g.vol), idt = (BT)(1. / dt), grav = (BT)p.grav1;
-  // Forward sweep inputs (w of cell L and the rows of du at layer L-1,
-  // 1 <= L <= nl) arrive kFwdDepth layers ahead through the same per-thread
-  // shared-memory ring as the back substitution, layout [slot][element][thread].
+  // Forward sweep inputs of iteration i — w of cell i+2 (for the blocks of
+  // layer i+1) and the rows of du at layer i — arrive kFwdDepth iterations
+  // ahead through the same per-thread shared-memory ring as the back
+  // substitution, layout [slot][element][thread].  The blocks of layer i+1
+  // (|A| at its upper face, J of the cell above it) are formed in iteration i,
+  // beside the elimination of layer i that does not depend on them, so the
+  // two dependency chains interleave.
   constexpr int DF = kFwdDepth, FE = 5 + N;
   static_assert(DF * FE <= BackRing<N>::depth * BackRing<N>::elems, "ring too small");
   extern __shared__ double vic_ring[];
   const int nt = blockDim.x, lane = threadIdx.x;
   auto fring = [&](int slot, int e) { return vic_ring + ((size_t)(slot * FE + e) * nt + lane); };
-  auto ffetch = [&](int L, int slot) {
-    if (L <= nl) {
+  auto ffetch = [&](int i, int slot) {
+    if (i < nl) {
+      const int L = min(i + 2, nl);  // cell nl is the ghost above the column
 #pragma unroll
       for (int v = 0; v < 5; ++v) cp_async_elem(fring(slot, v), b.w + v * sv + cb + L);
 #pragma unroll
       for (int r = 0; r < N; ++r)
-        cp_async_elem(fring(slot, 5 + r), b.D + sel<N>(r) * sv + cb + L - 1);
+        cp_async_elem(fring(slot, 5 + r), b.D + sel<N>(r) * sv + cb + i);
     }
     cp_async_commit();
   };
 #pragma unroll
-  for (int k = 0; k < DF; ++k) ffetch(1 + k, k);
-  double wc[5], wn[5];
-  BT Am[N][N], Jp[N][N], Jc[N][N];
-  double ap[N][N], dp[N];
+  for (int k = 0; k < DF; ++k) ffetch(k, k);
+  double wc[5], wn[5], wn2[5];
+  BT Am[N][N], Jp[N][N], Jc[N][N], Ap[N][N], Jn[N][N];
+  // (the first elimination step uses no previous layer: zeros keep it branch-free)
+  double ap[N][N] = {}, dp[N] = {};
   load_w(-1, wn);
   jac_of<N>(b, gm1c, wn, Jp);
   load_w(0, wc);
   absA_of<N>(b, gm1f, wn, wc, Am);
   jac_of<N>(b, gm1c, wc, Jc);
+  load_w(min(1, nl), wn);  // cell 1 (the ghost cell nl when nl = 1)
+  absA_of<N>(b, gm1f, wc, wn, Ap);
+  jac_of<N>(b, gm1c, wn, Jn);
   double sum_a2 = 0.;
   for (int i = 0, fslot = 0; i < nl; ++i) {
-    BT Ap[N][N], Jn[N][N];
     double rhs[N];
-    cp_async_wait<DF - 1>();  // the group of cell i+1 has landed
+    cp_async_wait<DF - 1>();  // the group of iteration i has landed
 #pragma unroll
-    for (int v = 0; v < 5; ++v)  // cell i+1 (the ghost cell nl at the top)
-      wn[v] = vic_full(b, ring_elem(fring(fslot, v), b.w), v, g.il + i + 1);
+    for (int v = 0; v < 5; ++v)
+      wn2[v] = vic_full(b, ring_elem(fring(fslot, v), b.w), v, g.il + min(i + 2, nl));
 #pragma unroll
     for (int r = 0; r < N; ++r) rhs[r] = ring_elem(fring(fslot, 5 + r), b.D) / dt;
-    absA_of<N>(b, gm1f, wc, wn, Ap);
-    jac_of<N>(b, gm1c, wn, Jn);
+    // blocks of layer i+1 (unused after the last layer)
+    BT Apn[N][N], Jnn[N][N];
+    absA_of<N>(b, gm1f, wn, wn2, Apn);
+    jac_of<N>(b, gm1c, wn2, Jnn);
     double ai = wc[IDN] * V;
     sum_a2 += ai * ai;
     // assembly in the block precision, then widened for the elimination
@@ -369,18 +381,16 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
       }
 #pragma unroll
     for (int r = 0; r < N; ++r) af[r][r] += idt;
-    if (i == 0) {
+    // boundary folds of the first and last layers, branch-free (weight 0
+    // elsewhere, which adds an exact zero)
+    const BT f0 = i == 0 ? BT(1) : BT(0), f1 = i == nl - 1 ? BT(1) : BT(0);
 #pragma unroll
-      for (int r = 0; r < N; ++r)
+    for (int r = 0; r < N; ++r)
 #pragma unroll
-        for (int q = 0; q < N; ++q) af[r][q] += bf[r][q] * (q == 1 ? BT(-1) : BT(1));
-    }
-    if (i == nl - 1) {
-#pragma unroll
-      for (int r = 0; r < N; ++r)
-#pragma unroll
-        for (int q = 0; q < N; ++q) af[r][q] += cf[r][q] * (q == 1 ? BT(-1) : BT(1));
-    }
+      for (int q = 0; q < N; ++q) {
+        af[r][q] += bf[r][q] * (q == 1 ? -f0 : f0);
+        af[r][q] += cf[r][q] * (q == 1 ? -f1 : f1);
+      }
     double a[N][N], bb[N][N], c[N][N];
 #pragma unroll
     for (int r = 0; r < N; ++r)
@@ -390,24 +400,22 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
         bb[r][q] = (double)bf[r][q];
         c[r][q] = (double)cf[r][q];
       }
-    if (i > 0) {
 #pragma unroll
-      for (int r = 0; r < N; ++r) {
-        double bd = 0.;
+    for (int r = 0; r < N; ++r) {
+      double bd = 0.;
 #pragma unroll
-        for (int q = 0; q < N; ++q) {
-          double t = 0.;
+      for (int q = 0; q < N; ++q) {
+        double t = 0.;
 #pragma unroll
-          for (int kk = 0; kk < N; ++kk) t += bb[r][kk] * ap[kk][q];
-          a[r][q] -= t;
-          bd += bb[r][q] * dp[q];
-        }
-        rhs[r] = rhs[r] - bd;
+        for (int kk = 0; kk < N; ++kk) t += bb[r][kk] * ap[kk][q];
+        a[r][q] -= t;
+        bd += bb[r][q] * dp[q];
       }
+      rhs[r] = rhs[r] - bd;
     }
     block_solve<N>(a, c, rhs);
     // the slot's values are consumed (the solve depends on them): refill it
-    ffetch(i + 1 + DF, fslot);
+    ffetch(i + DF, fslot);
     fslot = fslot + 1 == DF ? 0 : fslot + 1;
 #pragma unroll
     for (int r = 0; r < N; ++r) {
@@ -426,9 +434,14 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
         Am[r][q] = Ap[r][q];
         Jp[r][q] = Jc[r][q];
         Jc[r][q] = Jn[r][q];
+        Ap[r][q] = Apn[r][q];
+        Jn[r][q] = Jnn[r][q];
       }
 #pragma unroll
-    for (int v = 0; v < 5; ++v) wc[v] = wn[v];
+    for (int v = 0; v < 5; ++v) {
+      wc[v] = wn[v];
+      wn[v] = wn2[v];
+    }
   }
   // back substitution: delta_i -= a'_i delta_{i+1}; B_dry accumulated on the
   // way, the inputs of each layer arriving through the shared-memory ring.
