@@ -163,6 +163,18 @@ __host__ __device__ __forceinline__ T sqr(T x) {
   return x * x;
 }
 
+// Quotient of the face and block formulas: the correctly rounded division for
+// FP64 (and the adjoint's dual numbers); for the FP32 perturbation form the
+// fast single-precision division (__fdividef: within 2 ulp for divisors of
+// magnitude below 2^126), since its FP32 face states and blocks are FP32
+// approximations in any case and the correctly rounded quotient costs several
+// times the instructions.
+template <class T>
+__device__ __forceinline__ T fdiv(T a, T b) {
+  return a / b;
+}
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
+
 // ---------------------------------------------------------------------------
 // Reconstruction point kernels.  A face f (between cells f-1 and f) sees the
 // six cells q[0..5] = w[f-3 .. f+2].  The left state wl is the value at the
@@ -178,9 +190,9 @@ template <class T>
 __device__ __forceinline__ T weno5_face(T a, T b, T c, T d, T e, bool scale) {
   T vs = T(1);
   if (scale) {
-    vs = (fabs(a) + fabs(b) + fabs(c) + fabs(d) + fabs(e)) / T(5);
+    vs = fdiv(fabs(a) + fabs(b) + fabs(c) + fabs(d) + fabs(e), T(5));
     if (vs == T(0)) return T(0);
-    T iv = T(1) / vs;
+    T iv = fdiv(T(1), vs);
     a *= iv;
     b *= iv;
     c *= iv;
@@ -203,8 +215,8 @@ __device__ __forceinline__ T weno5_face(T a, T b, T c, T d, T e, bool scale) {
     T n0 = T(0.3) * s12, n1 = T(0.6) * s02, n2 = T(0.1) * s01;
     out = (n0 * p0 + n1 * p1 + n2 * p2) / (n0 + n1 + n2);
   } else {
-    T a0 = T(0.3) / s0, a1 = T(0.6) / s1, a2 = T(0.1) / s2;
-    out = (a0 * p0 + a1 * p1 + a2 * p2) / (a0 + a1 + a2);
+    T a0 = fdiv(T(0.3), s0), a1 = fdiv(T(0.6), s1), a2 = fdiv(T(0.1), s2);
+    out = fdiv(a0 * p0 + a1 * p1 + a2 * p2, a0 + a1 + a2);
   }
   return vs * out;
 }
@@ -215,19 +227,19 @@ template <class T>
 __device__ __forceinline__ T weno3_face(T a, T b, T c, bool scale) {
   T vs = T(1);
   if (scale) {
-    vs = (fabs(a) + fabs(b) + fabs(c)) / T(3);
+    vs = fdiv(fabs(a) + fabs(b) + fabs(c), T(3));
     if (vs == T(0)) return T(0);
-    a /= vs;
-    b /= vs;
-    c /= vs;
+    a = fdiv(a, vs);
+    b = fdiv(b, vs);
+    c = fdiv(c, vs);
   }
   T p0 = T(0.5) * a + T(0.5) * b;
   T p1 = T(1.5) * b - T(0.5) * c;
   T b0 = sqr(a - b);
   T b1 = sqr(b - c);
-  T a0 = T(2.0 / 3.0) / sqr(b0 + T(1e-6));
-  T a1 = T(1.0 / 3.0) / sqr(b1 + T(1e-6));
-  return (a0 * p0 + a1 * p1) / (a0 + a1) * vs;
+  T a0 = fdiv(T(2.0 / 3.0), sqr(b0 + T(1e-6)));
+  T a1 = fdiv(T(1.0 / 3.0), sqr(b1 + T(1e-6)));
+  return fdiv(a0 * p0 + a1 * p1, a0 + a1) * vs;
 }
 
 // face states from a six-cell window for one variable
@@ -260,13 +272,13 @@ __device__ __forceinline__ void face_states(int type, bool scale, const T* q, T&
       const T tiny = T(1.1754943508222875e-38);
       T dl = q[2] - q[1], dr = q[3] - q[2];
       T d2 = dl * dr;
-      T m = T(2) * d2 / (dl + dr + tiny);
+      T m = fdiv(T(2) * d2, dl + dr + tiny);
       m = d2 >= T(0) ? m : T(0);
       wl = q[2] + T(0.5) * m;
       dl = q[3] - q[2];
       dr = q[4] - q[3];
       d2 = dl * dr;
-      m = T(2) * d2 / (dl + dr + tiny);
+      m = fdiv(T(2) * d2, dl + dr + tiny);
       m = d2 >= T(0) ? m : T(0);
       wr = q[3] - T(0.5) * m;
       break;

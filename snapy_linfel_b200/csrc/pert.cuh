@@ -22,17 +22,17 @@ __device__ __forceinline__ void hllc_flux_split(const float* L, const float* R, 
   const float TINY = 1.0e-10f;
   int ivy = IVX + (ivx - IVX + 1) % 3;
   int ivz = IVX + (ivx - IVX + 2) % 3;
-  float igm1 = 1.f / (gamma - 1.f);
-  float cl = sqrtf(gamma * L[IPR] / L[IDN]);
-  float cr = sqrtf(gamma * R[IPR] / R[IDN]);
+  float igm1 = fdiv(1.f, gamma - 1.f);
+  float cl = sqrtf(fdiv(gamma * L[IPR], L[IDN]));
+  float cr = sqrtf(fdiv(gamma * R[IPR], R[IDN]));
   float el = L[IPR] * igm1 + 0.5f * L[IDN] * (sqr(L[IVX]) + sqr(L[IVY]) + sqr(L[IVZ]));
   float er = R[IPR] * igm1 + 0.5f * R[IDN] * (sqr(R[IVX]) + sqr(R[IVY]) + sqr(R[IVZ]));
   float rhoa = 0.5f * (L[IDN] + R[IDN]);
   float ca = 0.5f * (cl + cr);
   float pmid = 0.5f * (L[IPR] + R[IPR] + (L[ivx] - R[ivx]) * rhoa * ca);
-  float gf = (gamma + 1.f) / (2.f * gamma);
-  float ql = pmid <= L[IPR] ? 1.f : sqrtf(1.f + gf * (pmid / L[IPR] - 1.f));
-  float qr = pmid <= R[IPR] ? 1.f : sqrtf(1.f + gf * (pmid / R[IPR] - 1.f));
+  float gf = fdiv(gamma + 1.f, 2.f * gamma);
+  float ql = pmid <= L[IPR] ? 1.f : sqrtf(1.f + gf * (fdiv(pmid, L[IPR]) - 1.f));
+  float qr = pmid <= R[IPR] ? 1.f : sqrtf(1.f + gf * (fdiv(pmid, R[IPR]) - 1.f));
   float al = L[ivx] - cl * ql;
   float ar = R[ivx] + cr * qr;
   float bp = ar > 0.f ? ar : TINY;
@@ -43,7 +43,7 @@ __device__ __forceinline__ void hllc_flux_split(const float* L, const float* R, 
   float tr = pr + vxr * R[IDN] * R[ivx];
   float ml = L[IDN] * vxl;
   float mr = -(R[IDN] * vxr);
-  float ims = 1.f / (ml + mr);
+  float ims = fdiv(1.f, ml + mr);
   float am = (tl - tr) * ims;
   float cpp = (ml * tr + mr * tl) * ims;  // contact pressure minus pf
   if (pf + cpp <= 0.f) cpp = -pf;         // clamp of the full contact pressure at 0
@@ -52,12 +52,12 @@ __device__ __forceinline__ void hllc_flux_split(const float* L, const float* R, 
   vxr = R[ivx] - bp;
   float sl, sr, sm;
   if (am >= 0.f) {
-    float id = 1.f / (am - bm);
+    float id = fdiv(1.f, am - bm);
     sl = am * id;
     sr = 0.f;
     sm = -bm * id;
   } else {
-    float id = 1.f / (bp - am);
+    float id = fdiv(1.f, bp - am);
     sl = 0.f;
     sr = -am * id;
     sm = bp * id;
@@ -78,14 +78,14 @@ __device__ __forceinline__ void lmars_flux_split(const float* L, const float* R,
                                                  float pr, int ivx, float gamma, float* F) {
   int ivy = IVX + (ivx - IVX + 1) % 3;
   int ivz = IVX + (ivx - IVX + 2) % 3;
-  float igm1 = 1.f / (gamma - 1.f);
-  float irl = 1.f / L[IDN], irr = 1.f / R[IDN];
+  float igm1 = fdiv(1.f, gamma - 1.f);
+  float irl = fdiv(1.f, L[IDN]), irr = fdiv(1.f, R[IDN]);
   float hl = L[IPR] * igm1 * irl + 0.5f * (sqr(L[ivx]) + sqr(L[ivy]) + sqr(L[ivz])) + L[IPR] * irl;
   float hr = R[IPR] * igm1 * irr + 0.5f * (sqr(R[ivx]) + sqr(R[ivy]) + sqr(R[ivz])) + R[IPR] * irr;
   float rhobar = 0.5f * (L[IDN] + R[IDN]);
-  float cbar = sqrtf(0.5f * gamma * (L[IPR] + R[IPR]) / rhobar);
+  float cbar = sqrtf(fdiv(0.5f * gamma * (L[IPR] + R[IPR]), rhobar));
   float pbarp = 0.5f * (pl + pr) + 0.5f * (rhobar * cbar) * (L[ivx] - R[ivx]);
-  float ubar = 0.5f * (L[ivx] + R[ivx]) + 0.5f / (rhobar * cbar) * (pl - pr);
+  float ubar = 0.5f * (L[ivx] + R[ivx]) + fdiv(0.5f, rhobar * cbar) * (pl - pr);
   const float* S = ubar > 0.f ? L : R;
   float h = ubar > 0.f ? hl : hr;
   float m = ubar * S[IDN];
@@ -101,17 +101,17 @@ __device__ __forceinline__ void roe_flux_split(const float* L, const float* R, f
   const float TINY = 1.0e-10f;
   int ivy = IVX + (ivx - IVX + 1) % 3;
   int ivz = IVX + (ivx - IVX + 2) % 3;
-  float igm1 = 1.f / (gamma - 1.f);
+  float igm1 = fdiv(1.f, gamma - 1.f);
   float etl = L[IPR] * igm1 + 0.5f * L[IDN] * (sqr(L[IVX]) + sqr(L[IVY]) + sqr(L[IVZ]));
   float etr = R[IPR] * igm1 + 0.5f * R[IDN] * (sqr(R[IVX]) + sqr(R[IVY]) + sqr(R[IVZ]));
   float sdl = sqrtf(L[IDN]), sdr = sqrtf(R[IDN]);
-  float isd = 1.f / (sdl + sdr);
+  float isd = fdiv(1.f, sdl + sdr);
   float rhobar = sdl * sdr;
   float v1 = (sdl * L[ivx] + sdr * R[ivx]) * isd;
   float v2 = (sdl * L[ivy] + sdr * R[ivy]) * isd;
   float v3 = (sdl * L[ivz] + sdr * R[ivz]) * isd;
-  float hl = (etl + L[IPR]) / L[IDN];
-  float hr = (etr + R[IPR]) / R[IDN];
+  float hl = fdiv(etl + L[IPR], L[IDN]);
+  float hr = fdiv(etr + R[IPR], R[IDN]);
   float h = (hl * sdl + hr * sdr) * isd;
   float rl0 = L[IDN], rr0 = R[IDN];
   float fl0 = rl0 * L[ivx], fr0 = rr0 * R[ivx];
@@ -119,7 +119,7 @@ __device__ __forceinline__ void roe_flux_split(const float* L, const float* R, f
   float fl2 = L[IDN] * L[ivx] * L[ivy], fr2 = R[IDN] * R[ivx] * R[ivy];
   float fl3 = L[IDN] * L[ivx] * L[ivz], fr3 = R[IDN] * R[ivx] * R[ivz];
   float fl4 = (etl + L[IPR]) * L[ivx], fr4 = (etr + R[IPR]) * R[ivx];
-  float qbar = (rl0 / sdl + rr0 / sdr) * isd;
+  float qbar = (fdiv(rl0, sdl) + fdiv(rr0, sdr)) * isd;
   float vsq = v1 * v1 + v2 * v2 + v3 * v3;
   float q = h - 0.5f * vsq;
   float qq = q > TINY ? q : TINY;
@@ -130,15 +130,15 @@ __device__ __forceinline__ void roe_flux_split(const float* L, const float* R, f
   float spd_m = fabsf(lam_m), spd_0 = fabsf(v1), spd_p = fabsf(lam_p);
   float du = R[ivx] - L[ivx], dv = R[ivy] - L[ivy], dw = R[ivz] - L[ivz];
   float dp = pr - pl;
-  float ics = 1.f / cs, ics2 = 1.f / cs_sq;
+  float ics = fdiv(1.f, cs), ics2 = fdiv(1.f, cs_sq);
   float alpha_m = -0.5f * rhobar * ics * du + 0.5f * dp * ics2;
   float alpha_p = 0.5f * rhobar * ics * du + 0.5f * dp * ics2;
   float ac0 = rr0 - rl0 - dp * ics2 * qbar;
   float rho1 = rl0 + alpha_m * qbar;
   bool llf = (rho1 < 0.f) || (rho1 + ac0 < 0.f);
   if (llf) {
-    float cl = sqrtf(gamma * L[IPR] / L[IDN]);
-    float cr = sqrtf(gamma * R[IPR] / R[IDN]);
+    float cl = sqrtf(fdiv(gamma * L[IPR], L[IDN]));
+    float cr = sqrtf(fdiv(gamma * R[IPR], R[IDN]));
     float a = 0.5f * fmaxf(fabsf(L[ivx]) + cl, fabsf(R[ivx]) + cr);
     F[IDN] = 0.5f * (fl0 + fr0) - a * (rr0 - rl0);
     F[ivx] = 0.5f * (fl1 + fr1) - a * (R[IDN] * R[ivx] - L[IDN] * L[ivx]);

@@ -142,7 +142,7 @@ __device__ __forceinline__ void finalize32(const Geo& g, const Phys& p, const St
 // reference-sized cancellation)
 __device__ __forceinline__ void cons2prim_pert(const float* u, float* w, float rbar, float gm1) {
   float rho = rbar + u[IDN];
-  float ir = 1.f / rho;
+  float ir = fdiv(1.f, rho);
   w[IDN] = u[IDN];
   w[IVX] = u[IVX] * ir;
   w[IVY] = u[IVY] * ir;
@@ -298,7 +298,7 @@ __device__ __forceinline__ void x1_32_convert(const Geo& g, const Phys& p, const
     sr[(size_t)cc * nc1 + i] = b.rbf[i] + wc[IDN];
 #pragma unroll
     for (int n = 0; n < NS; ++n) {
-      float rr = st[sbase[5 + n] + e] / (b.rbf[i] + uc[IDN]);
+      float rr = fdiv(st[sbase[5 + n] + e], b.rbf[i] + uc[IDN]);
       base[(5 + n) * nc1 + i] = rr;
       b.R[n * sv + off] = rr;
     }

@@ -18,22 +18,12 @@ __device__ __forceinline__ int sel(int r) {
   return r;
 }
 
-// Quotient inside the block formulas: exact for FP64 (and the adjoint's dual
-// numbers); for the FP32 blocks of the FP32 perturbation form the fast
-// single-precision division (__fdividef, a couple of ulps), since those
-// blocks are FP32 approximations of the operator in any case.
-template <class T>
-__device__ __forceinline__ T bdiv(T a, T b) {
-  return a / b;
-}
-__device__ __forceinline__ float bdiv(float a, float b) { return __fdividef(a, b); }
-
 // N x N block of the x1 flux Jacobian dF/dU at primitive state w
 template <int N, class T>
 __device__ __forceinline__ void jac_block(T gm1, const T* w, T (&J)[N][N]) {
   T v1 = w[IVX], v2 = w[IVY], v3 = w[IVZ], rho = w[IDN], pres = w[IPR];
   T s2 = v1 * v1 + v2 * v2 + v3 * v3;
-  T hp = bdiv(bdiv(gm1 + T(1), gm1) * pres, rho);
+  T hp = fdiv(fdiv(gm1 + T(1), gm1) * pres, rho);
   T c1 = ((gm1 - T(1)) * s2 / T(2) - hp) * v1;
   T c2 = hp + s2 / T(2) - gm1 * v1 * v1;
   T full[5][5] = {{T(0.), T(1.), T(0.), T(0.), T(0.)},
@@ -51,21 +41,21 @@ __device__ __forceinline__ void jac_block(T gm1, const T* w, T (&J)[N][N]) {
 template <int N, class T>
 __device__ __forceinline__ void absA_block(T gm1, const T* wl, const T* wr, T (&A)[N][N]) {
   T sdl = sqrt(wl[IDN]), sdr = sqrt(wr[IDN]);
-  T isd = bdiv(T(1.0), sdl + sdr);
+  T isd = fdiv(T(1.0), sdl + sdr);
   T r = sdl * sdr;
   T u = (sdl * wl[IVX] + sdr * wr[IVX]) * isd;
   T v = (sdl * wl[IVY] + sdr * wr[IVY]) * isd;
   T w = (sdl * wl[IVZ] + sdr * wr[IVZ]) * isd;
-  T el = bdiv(wl[IPR], gm1) + T(0.5) * wl[IDN] * (sqr(wl[IVX]) + sqr(wl[IVY]) + sqr(wl[IVZ]));
-  T er = bdiv(wr[IPR], gm1) + T(0.5) * wr[IDN] * (sqr(wr[IVX]) + sqr(wr[IVY]) + sqr(wr[IVZ]));
-  T hbar = (bdiv(el + wl[IPR], sdl) + bdiv(er + wr[IPR], sdr)) * isd;
-  T p = bdiv((hbar - T(0.5) * (u * u + v * v + w * w)) * gm1, gm1 + T(1.)) * r;
-  T cs = sqrt(bdiv(p * (gm1 + T(1.)), r));
+  T el = fdiv(wl[IPR], gm1) + T(0.5) * wl[IDN] * (sqr(wl[IVX]) + sqr(wl[IVY]) + sqr(wl[IVZ]));
+  T er = fdiv(wr[IPR], gm1) + T(0.5) * wr[IDN] * (sqr(wr[IVX]) + sqr(wr[IVY]) + sqr(wr[IVZ]));
+  T hbar = (fdiv(el + wl[IPR], sdl) + fdiv(er + wr[IPR], sdr)) * isd;
+  T p = fdiv((hbar - T(0.5) * (u * u + v * v + w * w)) * gm1, gm1 + T(1.)) * r;
+  T cs = sqrt(fdiv(p * (gm1 + T(1.)), r));
   T lam[5] = {fabs(u - cs), fabs(u), fabs(u + cs), fabs(u), fabs(u)};
   T ke = T(0.5) * (u * u + v * v + w * w);
-  T hp = bdiv(bdiv(gm1 + T(1.), gm1) * p, r);
+  T hp = fdiv(fdiv(gm1 + T(1.), gm1) * p, r);
   T h = hp + ke;
-  T i2chp = bdiv(T(1.), T(2.) * cs * hp), ihp = bdiv(T(1.), hp), i2hp = T(0.5) * ihp;
+  T i2chp = fdiv(T(1.), T(2.) * cs * hp), ihp = fdiv(T(1.), hp), i2hp = T(0.5) * ihp;
   T R[5][5] = {{T(1.), T(1.), T(1.), T(0.), T(0.)},
                {u - cs, u, u + cs, T(0.), T(0.)},
                {v, v, v, T(1.), T(0.)},
