@@ -33,6 +33,11 @@ __device__ __forceinline__ double ring_elem(const double* slot, const double*) {
 __device__ __forceinline__ double ring_elem(const double* slot, const float*) {
   return (double)*reinterpret_cast<const float*>(slot);
 }
+// the element in the stored precision
+__device__ __forceinline__ double ring_stored(const double* slot, const double*) { return *slot; }
+__device__ __forceinline__ float ring_stored(const double* slot, const float*) {
+  return *reinterpret_cast<const float*>(slot);
+}
 
 // Slot-element address of this thread in a ring of E elements per slot.
 struct Ring {

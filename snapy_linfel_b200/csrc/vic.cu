@@ -174,6 +174,17 @@ __device__ __forceinline__ void jac_of(const StageBufs32&, double gm1, const dou
 #pragma unroll
     for (int q = 0; q < N; ++q) J[r][q] = (double)F[r][q];
 }
+// the same from full states already rounded to FP32
+template <int N>
+__device__ __forceinline__ void absA_of(const StageBufs32&, double gm1, const float* wl,
+                                        const float* wr, float (&A)[N][N]) {
+  absA_block<N, float>((float)gm1, wl, wr, A);
+}
+template <int N>
+__device__ __forceinline__ void jac_of(const StageBufs32&, double gm1, const float* w,
+                                       float (&J)[N][N]) {
+  jac_block<N, float>((float)gm1, w, J);
+}
 
 // One layer of the block-Thomas forward elimination: a_i, b_i, c_i from |A|
 // at the layer's lower / upper faces (Am, Ap) and J of the cells below /
@@ -304,13 +315,17 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
   double* S = b.vic + col;
   double* Z = S + (int64_t)nl * ES * ncol;
   auto Sat = [&](int i, int e) -> double& { return S[((int64_t)i * ES + e) * ncol]; };
-  auto load_w = [&](int i, double* w) {
+  // full primitives of a cell in the block precision, with the full density
+  // in FP64 beside them (the column sum)
+  auto load_w = [&](int i, BT* w, double& rho) {
+    rho = vic_w(b, sv, IDN, cb + i, g.il + i);
+    w[IDN] = (BT)rho;
 #pragma unroll
-    for (int v = 0; v < 5; ++v) w[v] = vic_w(b, sv, v, cb + i, g.il + i);
+    for (int v = 1; v < 5; ++v) w[v] = (BT)vic_w(b, sv, v, cb + i, g.il + i);
   };
   const double gm1c = p.gammad - 1.;
   const double gm1f = 0.5 * (p.gammad + p.gammad) - 1.;
-  const double dt = *b.dt;
+  const double dt = *b.dt, idtd = 1. / dt;
   const double V = g.vol;
   const BT Aa = (BT)g.A1, hiv = (BT)(0.5 / g.vol), idt = (BT)(1. / dt), grav = (BT)p.grav1;
   // Forward sweep inputs of iteration i — w of cell i+2 (for the blocks of
@@ -338,32 +353,37 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
   };
 #pragma unroll
   for (int k = 0; k < DF; ++k) ffetch(k, k);
-  double wc[5], wn[5], wn2[5];
+  BT wc[5], wn[5], wn2[5];
+  double rc, rn, rn2;
   BT Am[N][N], Jp[N][N], Jc[N][N], Ap[N][N], Jn[N][N];
   // (the first elimination step uses no previous layer: zeros keep it branch-free)
   double ap[N][N] = {}, dp[N] = {};
-  load_w(-1, wn);
+  load_w(-1, wn, rn);
   jac_of<N>(b, gm1c, wn, Jp);
-  load_w(0, wc);
+  load_w(0, wc, rc);
   absA_of<N>(b, gm1f, wn, wc, Am);
   jac_of<N>(b, gm1c, wc, Jc);
-  load_w(min(1, nl), wn);  // cell 1 (the ghost cell nl when nl = 1)
+  load_w(min(1, nl), wn, rn);  // cell 1 (the ghost cell nl when nl = 1)
   absA_of<N>(b, gm1f, wc, wn, Ap);
   jac_of<N>(b, gm1c, wn, Jn);
   double sum_a2 = 0.;
   for (int i = 0, fslot = 0; i < nl; ++i) {
     double rhs[N];
     cp_async_wait<DF - 1>();  // the group of iteration i has landed
+    {
+      const int xi = g.il + min(i + 2, nl);
+      rn2 = vic_full(b, (double)ring_stored(fring(fslot, IDN), b.w), IDN, xi);
+      wn2[IDN] = (BT)rn2;
 #pragma unroll
-    for (int v = 0; v < 5; ++v)
-      wn2[v] = vic_full(b, ring_elem(fring(fslot, v), b.w), v, g.il + min(i + 2, nl));
+      for (int v = 1; v < 5; ++v) wn2[v] = vic_full_blk(b, ring_stored(fring(fslot, v), b.w), v, xi);
+    }
 #pragma unroll
-    for (int r = 0; r < N; ++r) rhs[r] = ring_elem(fring(fslot, 5 + r), b.D) / dt;
+    for (int r = 0; r < N; ++r) rhs[r] = ring_elem(fring(fslot, 5 + r), b.D) * idtd;
     // blocks of layer i+1 (unused after the last layer)
     BT Apn[N][N], Jnn[N][N];
     absA_of<N>(b, gm1f, wn, wn2, Apn);
     jac_of<N>(b, gm1c, wn2, Jnn);
-    double ai = wc[IDN] * V;
+    double ai = rc * V;
     sum_a2 += ai * ai;
     // assembly in the block precision, then widened for the elimination
     BT af[N][N], bf[N][N], cf[N][N];
@@ -442,6 +462,8 @@ __device__ __forceinline__ void vic_column(const Geo& g, const Phys& p, const B&
       wc[v] = wn[v];
       wn[v] = wn2[v];
     }
+    rc = rn;
+    rn = rn2;
   }
   // back substitution: delta_i -= a'_i delta_{i+1}; B_dry accumulated on the
   // way, the inputs of each layer arriving through the shared-memory ring.

@@ -42,6 +42,17 @@ __device__ __forceinline__ double vic_full(const StageBufs32& b, double x, int v
   if (v == IPR) x += b.pb[xi];
   return x;
 }
+// the same in the precision the blocks are formed in: the FP64 plain form's
+// value as is; for the FP32 perturbation form the stored velocities as they
+// are, density and pressure summed with the reference in FP64 and rounded
+__device__ __forceinline__ double vic_full_blk(const StageBufs&, double x, int v, int xi) {
+  return x;
+}
+__device__ __forceinline__ float vic_full_blk(const StageBufs32& b, float x, int v, int xi) {
+  if (v == IDN) return (float)((double)x + b.rb[xi]);
+  if (v == IPR) return (float)((double)x + b.pb[xi]);
+  return x;
+}
 __device__ __forceinline__ double vic_d(const StageBufs& b, int64_t idx) { return b.D[idx]; }
 __device__ __forceinline__ double vic_d(const StageBufs32& b, int64_t idx) {
   return (double)b.D[idx];
