@@ -665,31 +665,55 @@ __global__ void __launch_bounds__(128) k_vic_column(Geo g, Phys p, B b) {
 // arrays are read and written along x1.
 // one tile: columns col0 .. col0+kTC-1, layers i0 .. i0+kTL-1 (whole CTA)
 // Shared memory of one finish tile: the back-substituted solution rows
-// [N][kTC][kTL+1] (doubles), the column sums and offsets, then the tile's cell
-// inputs [element][kTC][kTL] in the stored precision T: w'[IDN], the du rows
-// the solve does not replace, and (RK update) u, u0, and per scalar s, s0, r
-// and its du row.
+// [N][kTC][kTL+1] (doubles), the column sums and offsets, the layers'
+// reference densities, then the tile's cell inputs [element][kTC][kTL] in the
+// stored precision T: w'[IDN], the du rows the solve does not replace, and
+// (RK update) u, u0, and per scalar s, s0, r and its du row.
 template <int N, int NS>
 struct FinSmem {
   static constexpr int TL = 16;  // layers per staged tile
   static constexpr int du_rows = N == 3 ? 3 : 1;           // IDN (+ IVY, IVZ)
   static constexpr int elems = 1 + du_rows + 10 + 4 * NS;  // upper bound
-  static constexpr size_t head = ((size_t)N * kTC * (TL + 1) + 3 * kTC) * sizeof(double);
+  static constexpr size_t head = ((size_t)N * kTC * (TL + 1) + 3 * kTC + TL) * sizeof(double);
 };
 template <int N, int NS, class T>
 constexpr size_t finish_smem_bytes() {
   return FinSmem<N, NS>::head + (size_t)FinSmem<N, NS>::elems * kTC * FinSmem<N, NS>::TL * sizeof(T);
 }
 
-// One tile: columns col0 .. col0+kTC-1, layers i0 .. i0+kTL-1 (whole CTA).
-// Every input of the tile is fetched with cp.async (coalesced: the solution
-// rows along columns, the cell values along x1) and waited for once, so all
-// of a tile's loads are in flight together without holding registers; the
-// threads then finish the tile's cells from shared memory.
+// Views of a staged tile's shared memory, in the order above (the reference
+// densities are used by the FP32 form only).
+template <int N, int NS, class T>
+struct FinTile {
+  static constexpr int kTL = FinSmem<N, NS>::TL;
+  double *dl, *zs, *rbs;
+  int64_t* cbs;
+  T* cell;
+  __device__ __forceinline__ explicit FinTile(double* base) {
+    dl = base;
+    zs = dl + (size_t)N * kTC * (kTL + 1);
+    cbs = reinterpret_cast<int64_t*>(zs + 2 * kTC);
+    rbs = reinterpret_cast<double*>(cbs + kTC);
+    cell = reinterpret_cast<T*>(rbs + kTL);
+  }
+  __device__ __forceinline__ double& DL(int r, int c, int s) const {
+    return dl[((size_t)r * kTC + c) * (kTL + 1) + s];
+  }
+  __device__ __forceinline__ T* CE(int e, int c, int s) const {
+    return cell + ((size_t)e * kTC + c) * kTL + s;
+  }
+};
+
+// One tile, columns col0 .. col0+kTC-1, layers i0 .. i0+kTL-1 (whole CTA), in
+// two halves.  The issue half fetches every input of the tile with cp.async
+// (coalesced: the solution rows along columns, the cell values along x1) and
+// commits them as one group, so all of a tile's loads are in flight together
+// without holding registers; after the caller's wait and CTA barrier the
+// compute half finishes the tile's cells from shared memory.
 template <int N, int NS, class B>
-__device__ __forceinline__ void vic_finish_tile_staged(const Geo& g, const Phys& p, const B& b,
-                                                int64_t col0, int i0) {
-  constexpr int ES = VicDims<N>::ES, DR = FinSmem<N, NS>::du_rows, kTL = FinSmem<N, NS>::TL;
+__device__ __forceinline__ void vic_finish_issue(const Geo& g, const B& b, int64_t col0, int i0) {
+  constexpr int ES = VicDims<N>::ES, kTL = FinSmem<N, NS>::TL;
+  constexpr bool kPert = std::is_same_v<B, StageBufs32>;
   using T = std::remove_pointer_t<decltype(b.u)>;  // stored precision (FP32 / FP64)
   const int nl = g.nx1;
   const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
@@ -697,24 +721,21 @@ __device__ __forceinline__ void vic_finish_tile_staged(const Geo& g, const Phys&
   const double* S = b.vic;
   const double* Z = S + (int64_t)nl * ES * ncol;
   extern __shared__ double fin_smem[];
-  double* dl = fin_smem;                                     // [N][kTC][kTL+1]
-  double* zs = dl + (size_t)N * kTC * (kTL + 1);             // [2][kTC]
-  int64_t* cbs = reinterpret_cast<int64_t*>(zs + 2 * kTC);   // [kTC]
-  T* cell = reinterpret_cast<T*>(cbs + kTC);                 // [element][kTC][kTL]
-  auto DL = [&](int r, int c, int s) -> double& {
-    return dl[((size_t)r * kTC + c) * (kTL + 1) + s];
-  };
-  auto CE = [&](int e, int c, int s) -> T* { return cell + ((size_t)e * kTC + c) * kTL + s; };
+  const FinTile<N, NS, T> t(fin_smem);
   const bool du_only = b.vic_du_only, first = b.stage == 0;
-  // element slots; per scalar n: s, s0, r, its du row at eS + 4 n
+  constexpr int DR = FinSmem<N, NS>::du_rows;
   const int eRHO = 0, eDU = 1, eU = 1 + DR, eU0 = eU + 5, eS = eU0 + 5;
   const int tid = threadIdx.x;
-  if (tid < 2 * kTC) {
-    int c = tid % kTC, k = tid / kTC;
-    zs[k * kTC + c] = col0 + c < ncol ? Z[k * ncol + col0 + c] : 1.;
-    if (k == 0) cbs[c] = col0 + c < ncol ? column_base(g, col0 + c) : 0;
+  if (tid < 2 * kTC) {  // column sums (1 past the last column)
+    const int c = tid % kTC, k = tid / kTC;
+    if (col0 + c < ncol)
+      cp_async_bytes8(&t.zs[k * kTC + c], Z + k * ncol + col0 + c);
+    else
+      t.zs[k * kTC + c] = 1.;
+    if (k == 0) t.cbs[c] = col0 + c < ncol ? column_base(g, col0 + c) : 0;
   }
-  __syncthreads();
+  if constexpr (kPert)
+    if (tid < kTL && i0 + tid < nl) cp_async_bytes8(&t.rbs[tid], b.rb + g.il + i0 + tid);
   // Each thread copies the same CPT cells of every element: their offsets are
   // formed once, and the element loops pick one source array per pass.
   constexpr int CPT = kTC * kTL / kFinThreads;
@@ -733,7 +754,7 @@ __device__ __forceinline__ void vic_finish_tile_staged(const Geo& g, const Phys&
 #pragma unroll
       for (int j = 0; j < CPT; ++j) {
         const int idx = tid + j * kFinThreads;
-        if (sok[j]) cp_async_bytes8(&DL(r, idx % kTC, idx / kTC), S + soff[j] + (int64_t)r * ncol);
+        if (sok[j]) cp_async_bytes8(&t.DL(r, idx % kTC, idx / kTC), S + soff[j] + (int64_t)r * ncol);
       }
   }
   // cell inputs, layers fastest (the state arrays run along x1)
@@ -743,10 +764,10 @@ __device__ __forceinline__ void vic_finish_tile_staged(const Geo& g, const Phys&
   for (int j = 0; j < CPT; ++j) {
     const int idx = tid + j * kFinThreads, s = idx % kTL, c = idx / kTL;
     gok[j] = col0 + c < ncol && i0 + s < nl;
-    goff[j] = gok[j] ? cbs[c] + i0 + s : 0;
+    goff[j] = gok[j] ? column_base(g, col0 + c) + i0 + s : 0;
   }
   auto stage_elem = [&](int e, const T* base) {
-    T* dst = CE(e, 0, 0);
+    T* dst = t.CE(e, 0, 0);
 #pragma unroll
     for (int j = 0; j < CPT; ++j)
       if (gok[j]) cp_async_elem(dst + tid + j * kFinThreads, base + goff[j]);
@@ -770,28 +791,43 @@ __device__ __forceinline__ void vic_finish_tile_staged(const Geo& g, const Phys&
     }
   }
   cp_async_commit();
-  cp_async_wait<0>();
-  __syncthreads();
-  for (int idx = tid; idx < kTC * kTL; idx += blockDim.x) {
+}
+
+template <int N, int NS, class B>
+__device__ __forceinline__ void vic_finish_compute(const Geo& g, const Phys& p, const B& b,
+                                                   int64_t col0, int i0) {
+  constexpr int kTL = FinSmem<N, NS>::TL, DR = FinSmem<N, NS>::du_rows;
+  constexpr bool kPert = std::is_same_v<B, StageBufs32>;
+  using T = std::remove_pointer_t<decltype(b.u)>;
+  const int nl = g.nx1;
+  const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
+  const int64_t sv = g.sv;
+  extern __shared__ double fin_smem[];
+  const FinTile<N, NS, T> t(fin_smem);
+  const bool du_only = b.vic_du_only, first = b.stage == 0;
+  (void)p;
+  // element slots; per scalar n: s, s0, r, its du row at eS + 4 n
+  const int eRHO = 0, eDU = 1, eU = 1 + DR, eU0 = eU + 5, eS = eU0 + 5;
+  for (int idx = threadIdx.x; idx < kTC * kTL; idx += blockDim.x) {
     const int s = idx % kTL, c = idx / kTL;
     const int i = i0 + s;
     if (col0 + c >= ncol || i >= nl) continue;
-    const int64_t off = cbs[c] + i;
-    const int xi = g.il + i;
-    const double rhok = vic_full(b, (double)*CE(eRHO, c, s), IDN, xi);
-    const double etk = *CE(eDU, c, s);
+    const int64_t off = t.cbs[c] + i;
+    double rhok = (double)*t.CE(eRHO, c, s);  // full density
+    if constexpr (kPert) rhok += t.rbs[s];
+    const double etk = *t.CE(eDU, c, s);
     double ai = rhok * g.vol;
-    double fix = DL(0, c, s) - etk;
+    double fix = t.DL(0, c, s) - etk;
     double du[5];
-    du[IDN] = etk + fix * 1. + rhok * ai * zs[kTC + c] / zs[c];
+    du[IDN] = etk + fix * 1. + rhok * ai * t.zs[kTC + c] / t.zs[c];
     if constexpr (N == 3) {
-      du[IVX] = DL(1, c, s);
-      du[IVY] = *CE(eDU + 1, c, s);
-      du[IVZ] = *CE(eDU + 2, c, s);
-      du[IPR] = DL(2, c, s);
+      du[IVX] = t.DL(1, c, s);
+      du[IVY] = *t.CE(eDU + 1, c, s);
+      du[IVZ] = *t.CE(eDU + 2, c, s);
+      du[IPR] = t.DL(2, c, s);
     } else {
 #pragma unroll
-      for (int v = 1; v < 5; ++v) du[v] = DL(v, c, s);
+      for (int v = 1; v < 5; ++v) du[v] = t.DL(v, c, s);
     }
     if (b.M) b.M[IDN * sv + off] = fix;
     if (du_only) {
@@ -802,22 +838,34 @@ __device__ __forceinline__ void vic_finish_tile_staged(const Geo& g, const Phys&
     double unew_rho = 0.;
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
-      const double uo = *CE(eU + v, c, s), u0o = first ? 0. : (double)*CE(eU0 + v, c, s);
+      const double uo = *t.CE(eU + v, c, s), u0o = first ? 0. : (double)*t.CE(eU0 + v, c, s);
       double un = vic_rk_from(b.u, b.u0, v * sv + off, first, uo, u0o, b.wgt0, b.wgt1, b.wgt2,
                               du[v]);
-      if (v == IDN) unew_rho = vic_full_rho(b, un, xi);
+      if (v == IDN) {
+        unew_rho = un;  // full density of the new state
+        if constexpr (kPert) unew_rho += t.rbs[s];
+      }
     }
 #pragma unroll
     for (int n = 0; n < NS; ++n) {
       const int64_t o = n * sv + off;
-      const double so = *CE(eS + 4 * n, c, s);
-      const double s0o = first ? 0. : (double)*CE(eS + 4 * n + 1, c, s);
-      const double ro = *CE(eS + 4 * n + 2, c, s), dso = *CE(eS + 4 * n + 3, c, s);
+      const double so = *t.CE(eS + 4 * n, c, s);
+      const double s0o = first ? 0. : (double)*t.CE(eS + 4 * n + 1, c, s);
+      const double ro = *t.CE(eS + 4 * n + 2, c, s), dso = *t.CE(eS + 4 * n + 3, c, s);
       double ds = dso + fix * ro;
       double sn = vic_rk_from(b.s, b.s0, o, first, so, s0o, b.wgt0, b.wgt1, b.wgt2, ds);
       b.r[o] = sn / unew_rho;
     }
   }
+}
+
+template <int N, int NS, class B>
+__device__ __forceinline__ void vic_finish_tile_staged(const Geo& g, const Phys& p, const B& b,
+                                                       int64_t col0, int i0) {
+  vic_finish_issue<N, NS, B>(g, b, col0, i0);
+  cp_async_wait<0>();
+  __syncthreads();
+  vic_finish_compute<N, NS, B>(g, p, b, col0, i0);
 }
 
 // Register variant (scalars, or FP64 state: the staged inputs would not fit
@@ -1060,22 +1108,80 @@ __global__ void __launch_bounds__(128, V == 0 ? 1 : (V == 1 ? 3 : 4))
   (void)stage;
 }
 
+// Batched finish.  Staged tiles run as a pipeline: while a tile's inputs are
+// in flight, warp 0 claims the next work item and, when it belongs to another
+// member, copies that member's descriptor into the second descriptor buffer,
+// so the only latency between two tiles of a CTA is the tile's own loads.
 template <int N, int NS>
 __global__ void __launch_bounds__(FinCfg<N, NS, float>::threads,
                                   FinCfg<N, NS, float>::min_ctas) k_vic_finish_batch(const Member32* __restrict__ mem,
                                                           Phys p, WorkQueue q, int stage) {
-  __shared__ Member32 s_mem;  // the member's descriptor, read as needed (see the column kernel)
-  int m;
-  int64_t tile;
-  while (queue_next(q, m, tile)) {  // (starts with a barrier: the last tile is done)
-    load_member(s_mem, mem, m);
-    if (threadIdx.x == 0) set_stage32(s_mem.b, stage);
+  using FC = FinCfg<N, NS, float>;
+  constexpr int TLY = FC::layers;
+  // descriptors of the current and the next tile's member, read as needed
+  // (see the column kernel)
+  __shared__ Member32 s_mem[2];
+  if constexpr (!FC::staged) {
+    int m;
+    int64_t tile;
+    while (queue_next(q, m, tile)) {  // (starts with a barrier: the last tile is done)
+      load_member(s_mem[0], mem, m);
+      if (threadIdx.x == 0) set_stage32(s_mem[0].b, stage);
+      __syncthreads();
+      const int nlb = (s_mem[0].g.nx1 + TLY - 1) / TLY;
+      const int64_t cb = tile / nlb;
+      const int lb = (int)(tile - cb * nlb);
+      vic_finish_tile<N, NS, StageBufs32>(s_mem[0].g, p, s_mem[0].b, cb * kTC, lb * TLY);
+    }
+  } else {
+    __shared__ unsigned long long s_item;
+    const int tid = threadIdx.x;
+    if (tid == 0) s_item = atomicAdd(q.counter, 1ULL);
     __syncthreads();
-    constexpr int TLY = FinCfg<N, NS, float>::layers;
-    const int nlb = (s_mem.g.nx1 + TLY - 1) / TLY;
-    const int64_t cb = tile / nlb;
-    const int lb = (int)(tile - cb * nlb);
-    vic_finish_tile<N, NS, StageBufs32>(s_mem.g, p, s_mem.b, cb * kTC, lb * TLY);
+    int m;
+    int64_t tile;
+    if (!queue_find(q, (int64_t)s_item, m, tile)) return;
+    if (tid < 32) {
+      load_member_warp(s_mem[0], mem, m);
+      if (tid == 0) set_stage32(s_mem[0].b, stage);
+    }
+    __syncthreads();
+    int buf = 0;
+    while (true) {
+      const Member32& cur = s_mem[buf];
+      const int nlb = (cur.g.nx1 + TLY - 1) / TLY;
+      const int64_t cb = tile / nlb;
+      const int lb = (int)(tile - cb * nlb);
+      vic_finish_issue<N, NS, StageBufs32>(cur.g, cur.b, cb * kTC, lb * TLY);
+      if (tid < 32) {  // the next item, and its member's descriptor if that changes
+        unsigned long long it = 0;
+        if (tid == 0) it = atomicAdd(q.counter, 1ULL);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (tid == 0) s_item = it;
+        int nm;
+        int64_t nt;
+        if (queue_find(q, (int64_t)it, nm, nt) && nm != m) {
+          const int* src = reinterpret_cast<const int*>(mem + nm);
+          int* dst = reinterpret_cast<int*>(&s_mem[buf ^ 1]);
+          for (int k = tid; k < (int)(sizeof(Member32) / sizeof(int)); k += 32)
+            cp_async_bytes4(dst + k, src + k);
+        }
+        cp_async_commit();
+      }
+      cp_async_wait<0>();
+      __syncthreads();  // the tile's inputs, the next item and its descriptor are in place
+      int nm;
+      int64_t ntile;
+      const bool more = queue_find(q, (int64_t)s_item, nm, ntile);
+      const int nbuf = more && nm != m ? buf ^ 1 : buf;
+      if (tid == 0 && nbuf != buf) set_stage32(s_mem[nbuf].b, stage);
+      vic_finish_compute<N, NS, StageBufs32>(cur.g, p, cur.b, cb * kTC, lb * TLY);
+      if (!more) return;
+      __syncthreads();  // the tile's shared memory is free; s_item is read
+      buf = nbuf;
+      m = nm;
+      tile = ntile;
+    }
   }
 }
 
