@@ -179,6 +179,32 @@ __device__ __forceinline__ void riemann_flux_split(int solver, const float* L, c
     roe_flux_split(L, R, pl, pr, ivx, gamma, F);
 }
 
+// Face profiles: compile-time specializations of the FP32 sweeps.  Profile 0
+// reads every reconstruction and solver choice at run time; profiles 1, 2 and
+// 3 are the default reconstruction (WENO5 for density and scalars, the linear
+// 5-point interpolation for velocities and pressure, no scaling) with the
+// LMARS, HLLC and Roe solvers.  The host picks the profile (face_profile32).
+template <int FP>
+__device__ __forceinline__ void sweep_face_states(int typ, bool scale, int v, const float* q,
+                                                  float& wl, float& wr) {
+  if constexpr (FP == 0)
+    face_states<float>(typ, scale, q, wl, wr);
+  else
+    face_states<float>(v == IDN || v >= 5 ? SNAPB_RECON_WENO5 : SNAPB_RECON_CP5, false, q, wl, wr);
+}
+template <int FP>
+__device__ __forceinline__ void sweep_riemann(int solver, const float* L, const float* R, float pl,
+                                              float pr, float pf, int ivx, float gamma, float* F) {
+  if constexpr (FP == 1)
+    lmars_flux_split(L, R, pl, pr, ivx, gamma, F);
+  else if constexpr (FP == 2)
+    hllc_flux_split(L, R, pl, pr, pf, ivx, gamma, F);
+  else if constexpr (FP == 3)
+    roe_flux_split(L, R, pl, pr, ivx, gamma, F);
+  else
+    riemann_flux_split(solver, L, R, pl, pr, pf, ivx, gamma, F);
+}
+
 // linear interpolation weights of the face states (cp5, cp3, dc): the value at
 // the right face of q[2] (wl) and the left face of q[3] (wr) from six cells
 __device__ __forceinline__ bool linear_face_states(int type, const float* q, float& wl,

@@ -14,6 +14,7 @@
 // The momentum fluxes carry the pressure as p' = p - pf (pert.cuh), so the
 // large hydrostatic pressure never enters an FP32 difference.
 #include <algorithm>
+#include <type_traits>
 
 #include "kernels.cuh"
 #include "bulk.cuh"
@@ -312,7 +313,7 @@ __device__ __forceinline__ void x1_32_convert(const Geo& g, const Phys& p, const
   __syncthreads();
 }
 
-template <int NS>
+template <int NS, int FP>
 __device__ __forceinline__ void x1_32_faces(const Geo& g, const Phys& p, const StageBufs32& b,
                                             int C, int last, int64_t col0, const float* smf) {
   constexpr int NV = 5 + NS;
@@ -342,14 +343,14 @@ __device__ __forceinline__ void x1_32_faces(const Geo& g, const Phys& p, const S
 #pragma unroll
       for (int s6 = 0; s6 < 6; ++s6) q[s6] = v == IDN ? rho[s6] : base[v * nc1 + s6];
       if (v == IPR) {
-        face_states<float>(ptype, p.r1_scale != 0, q, pl, pr);
+        sweep_face_states<FP>(ptype, p.r1_scale != 0, v, q, pl, pr);
         pl += b.offL[f];
         pr += b.offR[f];
       } else if (v < 5) {
         int typ = (p.r1_shock || v == IDN) ? p.r1_type : interp2_of(p.r1_type);
-        face_states<float>(typ, p.r1_scale != 0, q, L[v], R[v]);
+        sweep_face_states<FP>(typ, p.r1_scale != 0, v, q, L[v], R[v]);
       } else {
-        face_states<float>(p.rs_type, p.rs_scale != 0, q, L[v], R[v]);
+        sweep_face_states<FP>(p.rs_type, p.rs_scale != 0, v, q, L[v], R[v]);
         L[v] = L[v] < 0.f ? 0.f : L[v];
         R[v] = R[v] < 0.f ? 0.f : R[v];
       }
@@ -371,7 +372,7 @@ __device__ __forceinline__ void x1_32_faces(const Geo& g, const Phys& p, const S
 #pragma unroll
       for (int v = 0; v < 5; ++v) F[v] = 0.f;
     } else {
-      riemann_flux_split(p.riemann, L, R, pl, pr, pfv, IVX, gamma, F);
+      sweep_riemann<FP>(p.riemann, L, R, pl, pr, pfv, IVX, gamma, F);
     }
 #pragma unroll
     for (int n = 0; n < NS; ++n) F[5 + n] = F[IDN] > 0.f ? F[IDN] * L[5 + n] : F[IDN] * R[5 + n];
@@ -426,7 +427,7 @@ __device__ __forceinline__ void x1_32_faces(const Geo& g, const Phys& p, const S
 }
 
 // one tile per CTA: stage, convert, faces
-template <int NS>
+template <int NS, int FP>
 __global__ void __launch_bounds__(512, 2) k_x1_32(Geo g, Phys p, StageBufs32 b, int C, int last) {
   extern __shared__ __align__(16) float smf[];
   __shared__ uint64_t bar;
@@ -440,7 +441,7 @@ __global__ void __launch_bounds__(512, 2) k_x1_32(Geo g, Phys p, StageBufs32 b, 
     return;
   }
   x1_32_convert<NS>(g, p, b, C, col0, smf, g.nc1);
-  x1_32_faces<NS>(g, p, b, C, last, col0, smf);
+  x1_32_faces<NS, FP>(g, p, b, C, last, col0, smf);
 }
 
 // ---------------------------------------------------------------------------
@@ -448,7 +449,7 @@ __global__ void __launch_bounds__(512, 2) k_x1_32(Geo g, Phys p, StageBufs32 b, 
 // ---------------------------------------------------------------------------
 // One thread's work: line tid (x1 cell x other horizontal index) and face
 // segment seg of the sweep axis.
-template <int NS, int AX>
+template <int NS, int AX, int FP>
 __device__ __forceinline__ void march32_line(const Geo& g, const Phys& p, const StageBufs32& b,
                                              int seglen, int first, int last, int64_t tid,
                                              int seg) {
@@ -507,9 +508,9 @@ __device__ __forceinline__ void march32_line(const Geo& g, const Phys& p, const 
     for (int v = 0; v < NV; ++v) {
       if (v < 5) {
         int typ = (p.r23_shock || v == IDN) ? p.r23_type : interp2_of(p.r23_type);
-        face_states<float>(typ, p.r23_scale != 0, q[v], L[v], R[v]);
+        sweep_face_states<FP>(typ, p.r23_scale != 0, v, q[v], L[v], R[v]);
       } else {
-        face_states<float>(p.rs_type, p.rs_scale != 0, q[v], L[v], R[v]);
+        sweep_face_states<FP>(p.rs_type, p.rs_scale != 0, v, q[v], L[v], R[v]);
         L[v] = L[v] < 0.f ? 0.f : L[v];
         R[v] = R[v] < 0.f ? 0.f : R[v];
       }
@@ -523,7 +524,7 @@ __device__ __forceinline__ void march32_line(const Geo& g, const Phys& p, const 
 #pragma unroll
       for (int v = 0; v < 5; ++v) F[v] = 0.f;
     } else {
-      riemann_flux_split(p.riemann, L, R, pl, pr, pref, ivx, gamma, F);
+      sweep_riemann<FP>(p.riemann, L, R, pl, pr, pref, ivx, gamma, F);
     }
 #pragma unroll
     for (int n = 0; n < NS; ++n) F[5 + n] = F[IDN] > 0.f ? F[IDN] * L[5 + n] : F[IDN] * R[5 + n];
@@ -554,10 +555,10 @@ __device__ __forceinline__ void march32_line(const Geo& g, const Phys& p, const 
   }
 }
 
-template <int NS, int AX>
+template <int NS, int AX, int FP>
 __global__ void __launch_bounds__(128) k_march32(Geo g, Phys p, StageBufs32 b, int seglen,
                                                  int first, int last) {
-  march32_line<NS, AX>(g, p, b, seglen, first, last,
+  march32_line<NS, AX, FP>(g, p, b, seglen, first, last,
                        (int64_t)blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y);
 }
 
@@ -705,7 +706,7 @@ __global__ void k_cfl32(Geo g, double gammad, int use1, int use2, int use3, cons
 // Persistent batched x1 sweep (CTA of 32 C threads, C the ensemble's tile
 // width): tiles are taken from the queue one ahead, so warp 0 stages the next
 // tile's slabs by bulk copies while the current tile's faces are computed.
-template <int NS>
+template <int NS, int FP>
 __global__ void __launch_bounds__(512, 2) k_x1_32_batch(const Member32* __restrict__ mem, Phys p,
                                                         WorkQueue q, int stage, int last,
                                                         int nc1max) {
@@ -754,7 +755,7 @@ __global__ void __launch_bounds__(512, 2) k_x1_32_batch(const Member32* __restri
       __syncwarp();
       x1_32_stage<NS>(nxt.g, nxt.b, nxt.x1_cols, ntile * nxt.x1_cols, smf, nc1max, &bar);
     }
-    x1_32_faces<NS>(cur.g, p, cur.b, C, last, col0, smf);
+    x1_32_faces<NS, FP>(cur.g, p, cur.b, C, last, col0, smf);
     if (!more) return;
     __syncthreads();  // this tile's rows are read; the next descriptor is in place
     buf ^= 1;
@@ -776,7 +777,7 @@ __global__ void __launch_bounds__(256) k_x1_ghost_revision32_batch(const Member3
   }
 }
 
-template <int NS, int AX>
+template <int NS, int AX, int FP>
 __global__ void __launch_bounds__(128, 6) k_march32_batch(const Member32* __restrict__ mem, Phys p,
                                                        WorkQueue q, int stage, int first,
                                                        int last) {
@@ -790,7 +791,7 @@ __global__ void __launch_bounds__(128, 6) k_march32_batch(const Member32* __rest
     const int nseg = AX == 2 ? mem[m].nseg2 : mem[m].nseg3;
     const int64_t blk = tile / nseg;
     const int seg = (int)(tile - blk * nseg);
-    march32_line<NS, AX>(g, p, b, seglen, first, last, blk * blockDim.x + threadIdx.x, seg);
+    march32_line<NS, AX, FP>(g, p, b, seglen, first, last, blk * blockDim.x + threadIdx.x, seg);
   }
 }
 
@@ -817,26 +818,50 @@ __global__ void __launch_bounds__(256) k_bc32_batch(const Member32* __restrict__
   }
 }
 
+// Face profile of the FP32 sweeps along `axis` (sweep_face_states, pert.cuh):
+// 1, 2, 3 for the default reconstruction with LMARS, HLLC, Roe; 0 otherwise.
+int face_profile32(const Phys& p, int axis) {
+  const int typ = axis == 1 ? p.r1_type : p.r23_type;
+  const int shock = axis == 1 ? p.r1_shock : p.r23_shock;
+  const int scale = axis == 1 ? p.r1_scale : p.r23_scale;
+  if (typ != SNAPB_RECON_WENO5 || shock || scale) return 0;
+  if (p.nscalar > 0 && (p.rs_type != SNAPB_RECON_WENO5 || p.rs_scale)) return 0;
+  switch (p.riemann) {
+    case SNAPB_RIEMANN_LMARS: return 1;
+    case SNAPB_RIEMANN_HLLC: return 2;
+    case SNAPB_RIEMANN_ROE: return 3;
+  }
+  return 0;
+}
+
+// f(NS, FP) with the scalar count and the face profile as compile-time constants
+template <class F>
+static cudaError_t with_ns_profile(int ns, int fp, F&& f) {
+#define SNAPB_NF(NS, FP) \
+  case NS * 4 + FP:      \
+    return f(std::integral_constant<int, NS>{}, std::integral_constant<int, FP>{});
+  if (ns < 0 || ns > 3 || fp < 0 || fp > 3) return cudaErrorInvalidValue;
+  switch (ns * 4 + fp) {
+    SNAPB_NF(0, 0) SNAPB_NF(0, 1) SNAPB_NF(0, 2) SNAPB_NF(0, 3)
+    SNAPB_NF(1, 0) SNAPB_NF(1, 1) SNAPB_NF(1, 2) SNAPB_NF(1, 3)
+    SNAPB_NF(2, 0) SNAPB_NF(2, 1) SNAPB_NF(2, 2) SNAPB_NF(2, 3)
+    SNAPB_NF(3, 0) SNAPB_NF(3, 1) SNAPB_NF(3, 2) SNAPB_NF(3, 3)
+  }
+#undef SNAPB_NF
+  return cudaErrorInvalidValue;
+}
+
 cudaError_t launch_x1_32_batch(const Member32* mem, const Phys& p, const WorkQueue& q,
                                int stage, bool last, const PersistGrid& pg, size_t smem, int C,
                                int nc1max, cudaStream_t st) {
   const int nt = 32 * C;  // one warp per column of a tile
-#define SNAPB_X1B(NS)                                                                         \
-  case NS: {                                                                                  \
-    raise_smem_limit(k_x1_32_batch<NS>, 200 * 1024);                                        \
-    int grid = persistent_grid(k_x1_32_batch<NS>, nt, smem, pg);                              \
-    k_x1_32_batch<NS><<<grid, nt, smem, st>>>(mem, p, q, stage, last ? 1 : 0, nc1max);        \
-    break;                                                                                    \
-  }
-  switch (p.nscalar) {
-    SNAPB_X1B(0)
-    SNAPB_X1B(1)
-    SNAPB_X1B(2)
-    SNAPB_X1B(3)
-    default: return cudaErrorInvalidValue;
-  }
-#undef SNAPB_X1B
-  return cudaGetLastError();
+  return with_ns_profile(p.nscalar, face_profile32(p, 1), [&](auto ns, auto fp) {
+    constexpr int NS = decltype(ns)::value, FP = decltype(fp)::value;
+    raise_smem_limit(k_x1_32_batch<NS, FP>, 200 * 1024);
+    const int grid = persistent_grid(k_x1_32_batch<NS, FP>, nt, smem, pg);
+    k_x1_32_batch<NS, FP><<<grid, nt, smem, st>>>(mem, p, q, stage, last ? 1 : 0, nc1max);
+    return cudaGetLastError();
+  });
 }
 
 cudaError_t launch_x1_ghost_revision32_batch(const Member32* mem, const Phys& p,
@@ -850,24 +875,16 @@ cudaError_t launch_x1_ghost_revision32_batch(const Member32* mem, const Phys& p,
 cudaError_t launch_march32_batch(int axis, const Member32* mem, const Phys& p,
                                  const WorkQueue& q, int stage, bool first, bool last,
                                  const PersistGrid& pg, cudaStream_t st) {
-#define SNAPB_MB(NS)                                                                         \
-  case NS:                                                                                   \
-    if (axis == 2)                                                                           \
-      k_march32_batch<NS, 2><<<persistent_grid(k_march32_batch<NS, 2>, 128, 0, pg), 128, 0,   \
-                               st>>>(mem, p, q, stage, first, last);                         \
-    else                                                                                     \
-      k_march32_batch<NS, 3><<<persistent_grid(k_march32_batch<NS, 3>, 128, 0, pg), 128, 0,   \
-                               st>>>(mem, p, q, stage, first, last);                         \
-    break;
-  switch (p.nscalar) {
-    SNAPB_MB(0)
-    SNAPB_MB(1)
-    SNAPB_MB(2)
-    SNAPB_MB(3)
-    default: return cudaErrorInvalidValue;
-  }
-#undef SNAPB_MB
-  return cudaGetLastError();
+  return with_ns_profile(p.nscalar, face_profile32(p, axis), [&](auto ns, auto fp) {
+    constexpr int NS = decltype(ns)::value, FP = decltype(fp)::value;
+    if (axis == 2)
+      k_march32_batch<NS, 2, FP><<<persistent_grid(k_march32_batch<NS, 2, FP>, 128, 0, pg), 128,
+                                   0, st>>>(mem, p, q, stage, first, last);
+    else
+      k_march32_batch<NS, 3, FP><<<persistent_grid(k_march32_batch<NS, 3, FP>, 128, 0, pg), 128,
+                                   0, st>>>(mem, p, q, stage, first, last);
+    return cudaGetLastError();
+  });
 }
 
 cudaError_t launch_bc32_batch(const Member32* mem, const Phys& p, const WorkQueue& q, int kind,
@@ -907,33 +924,30 @@ cudaError_t launch_x1_ghost_revision32(const Geo& g, const Phys& p, const StageB
   return cudaGetLastError();
 }
 
-template <int NS>
+template <int NS, int FP>
 static cudaError_t launch_x1_32t(const Geo& g, const Phys& p, const StageBufs32& b, bool last,
                                  cudaStream_t st) {
   const int nvt = 5 + NS;
   int C = x1_columns_per_cta32(g, nvt);
   size_t smem = x1_smem32_bytes(g.nc1, nvt, C);
   if (smem > 200 * 1024) return cudaErrorInvalidConfiguration;
-  raise_smem_limit(k_x1_32<NS>, 200 * 1024);
+  raise_smem_limit(k_x1_32<NS, FP>, 200 * 1024);
   cudaError_t e = launch_x1_ghost_revision32(g, p, b, st);
   if (e != cudaSuccess) return e;
   int64_t ncol = (int64_t)g.nc2 * g.nc3;
-  k_x1_32<NS><<<(unsigned)((ncol + C - 1) / C), 32 * C, smem, st>>>(g, p, b, C, last ? 1 : 0);
+  k_x1_32<NS, FP><<<(unsigned)((ncol + C - 1) / C), 32 * C, smem, st>>>(g, p, b, C,
+                                                                      last ? 1 : 0);
   return cudaGetLastError();
 }
 
 cudaError_t launch_x1_32(const Geo& g, const Phys& p, const StageBufs32& b, bool last,
                          cudaStream_t st) {
-  switch (p.nscalar) {
-    case 0: return launch_x1_32t<0>(g, p, b, last, st);
-    case 1: return launch_x1_32t<1>(g, p, b, last, st);
-    case 2: return launch_x1_32t<2>(g, p, b, last, st);
-    case 3: return launch_x1_32t<3>(g, p, b, last, st);
-  }
-  return cudaErrorInvalidValue;
+  return with_ns_profile(p.nscalar, face_profile32(p, 1), [&](auto ns, auto fp) {
+    return launch_x1_32t<decltype(ns)::value, decltype(fp)::value>(g, p, b, last, st);
+  });
 }
 
-template <int NS, int AX>
+template <int NS, int AX, int FP>
 static cudaError_t launch_march32_t(const Geo& g, const Phys& p, const StageBufs32& b,
                                     bool first, bool last, cudaStream_t st) {
   int ni = g.iu - g.il + 1;
@@ -943,24 +957,17 @@ static cudaError_t launch_march32_t(const Geo& g, const Phys& p, const StageBufs
   int64_t threads = (int64_t)ni * no;
   while (seglen > 8 && threads * ((n + seglen - 1) / seglen) < 148LL * 1024 * 2) seglen /= 2;
   dim3 grid((unsigned)((threads + 127) / 128), (unsigned)((n + seglen - 1) / seglen));
-  k_march32<NS, AX><<<grid, 128, 0, st>>>(g, p, b, seglen, first ? 1 : 0, last ? 1 : 0);
+  k_march32<NS, AX, FP><<<grid, 128, 0, st>>>(g, p, b, seglen, first ? 1 : 0, last ? 1 : 0);
   return cudaGetLastError();
 }
 
 cudaError_t launch_march32(int axis, const Geo& g, const Phys& p, const StageBufs32& b,
                            bool first, bool last, cudaStream_t st) {
-#define SNAPB_MARCH32(NS)                                                  \
-  case NS:                                                                 \
-    return axis == 2 ? launch_march32_t<NS, 2>(g, p, b, first, last, st)  \
-                     : launch_march32_t<NS, 3>(g, p, b, first, last, st);
-  switch (p.nscalar) {
-    SNAPB_MARCH32(0)
-    SNAPB_MARCH32(1)
-    SNAPB_MARCH32(2)
-    SNAPB_MARCH32(3)
-  }
-#undef SNAPB_MARCH32
-  return cudaErrorInvalidValue;
+  return with_ns_profile(p.nscalar, face_profile32(p, axis), [&](auto ns, auto fp) {
+    constexpr int NS = decltype(ns)::value, FP = decltype(fp)::value;
+    return axis == 2 ? launch_march32_t<NS, 2, FP>(g, p, b, first, last, st)
+                     : launch_march32_t<NS, 3, FP>(g, p, b, first, last, st);
+  });
 }
 
 cudaError_t launch_bc32(const Geo& g, const snapb_hydro_config& c, float* var, int nv, int kind,
