@@ -822,7 +822,7 @@ __global__ void k_cell_adj(Geo g, Phys p, AdjBufs b) {
 template <int N>
 struct VadjDims {
   static constexpr int E1 = 2 * N * N + 2 * N + 2;
-  static constexpr int ES = 2 * N * N + 2 * N;
+  static constexpr int ES = 2 * N * N + 3 * N;
 };
 
 static inline int vic_n_adj(const Phys& p) { return ((p.implicit_scheme >> 3) & 1) ? 5 : 3; }
@@ -832,7 +832,7 @@ size_t vic_adj_scratch_bytes(const Geo& g, const Phys& p) {
   int N = vic_n_adj(p);
   int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
   int64_t nl = g.nx1;
-  int64_t e1 = 2 * N * N + 2 * N + 2, es = 2 * N * N + 2 * N;
+  int64_t e1 = 2 * N * N + 2 * N + 2, es = 2 * N * N + 3 * N;
   return (size_t)((nl + 2) * e1 * ncol + nl * es * ncol + 3 * ncol) * sizeof(double);
 }
 
@@ -947,13 +947,14 @@ __device__ __noinline__ void solve_transposed(const double (&M)[N][N], double (&
   block_solve<N>(Mt, Z, y);
 }
 
-// Per-thread ring (see ring.cuh) for the five sequential passes of
+// Per-thread ring (see ring.cuh) for the two sequential passes of
 // k_vadj_sweep: depth layers ahead, elems doubles per slot (the widest pass,
-// the transposed sweep: t rows, |A| and J of the face / cell above, ahat).
+// the backward one: the reduced block and partial solution, h0 and h1, ahat
+// or its inverse, |A| and J of the face / cell above).
 template <int N>
 struct VadjRing {
   static constexpr int depth = N == 3 ? 4 : 2;
-  static constexpr int elems = 3 * N * N + N;
+  static constexpr int elems = 4 * N * N + 3 * N + 1;
 };
 template <int N>
 constexpr size_t vadj_ring_bytes(int threads) {
@@ -973,7 +974,7 @@ __global__ void __launch_bounds__(128) k_vadj_sweep(Geo g, Phys p, AdjBufs b) {
   double* Z = S + (int64_t)nl * ES * ncol;
   auto Tp = [&](int t, int e) { return T + ((int64_t)t * E1 + e) * ncol; };
   auto Sat = [&](int i, int e) -> double& { return S[((int64_t)i * ES + e) * ncol]; };
-  const int oAT = 0, oAH = NN, oD = 2 * NN, oT = 2 * NN + N;
+  const int oAT = 0, oAH = NN, oD = 2 * NN, oT = 2 * NN + N, oH1 = 2 * NN + 2 * N;
   // T entries of index t: |A| (0), J (NN), du rows (2NN), rho (2NN+N),
   // output cotangent rows (2NN+N+1), g_fix (2NN+2N+1)
   const int tA = 0, tJ = NN, tDU = 2 * NN, tRHO = 2 * NN + N, tG = 2 * NN + N + 1,
@@ -993,8 +994,14 @@ __global__ void __launch_bounds__(128) k_vadj_sweep(Geo g, Phys p, AdjBufs b) {
   const double dt = *b.dt;
   const double Aa = g.A1, hiv = 0.5 / g.vol, idt = 1. / dt, grav = p.grav1, V = g.vol;
 
-  // (1) forward elimination, as the forward column sweep, keeping ahat_i
-  constexpr int E_1 = 2 * NN + N + 2;
+  // (A) forward elimination as the forward column sweep, keeping the
+  // inverse of each reduced diagonal block ahat_i (N = 3; the block itself
+  // for N = 5), with the forward recurrence of the transposed solve beside
+  // it: h_i = g_delta_i - a~_{i-1}^T h_{i-1}.  Its redistribution term
+  // -V g_B e_0 is linear in g_B, which is known only at the end of this pass,
+  // so it runs as h = h0 + g_B h1.
+  constexpr int E_1 = 2 * NN + 2 * N + 2;
+  static_assert(E_1 <= VadjRing<N>::elems, "ring slot");
   Ring r1{vadj_ring, E_1, nt, lane};
   auto fetch1 = [&](int i, int slot) {
     if (i < nl) {
@@ -1005,20 +1012,27 @@ __global__ void __launch_bounds__(128) k_vadj_sweep(Geo g, Phys p, AdjBufs b) {
 #pragma unroll
       for (int r = 0; r < N; ++r) cp_async_bytes8(r1.at(slot, 2 * NN + r), Tp(i, tDU + r));
       cp_async_bytes8(r1.at(slot, 2 * NN + N), Tp(i, tRHO));
-      cp_async_bytes8(r1.at(slot, 2 * NN + N + 1), Tp(i, tG));  // cotangent of du_out[IDN]
+#pragma unroll
+      for (int r = 0; r < N; ++r)  // output cotangent rows
+        cp_async_bytes8(r1.at(slot, 2 * NN + N + 1 + r), Tp(i, tG + r));
+      cp_async_bytes8(r1.at(slot, 2 * NN + 2 * N + 1), Tp(i, tGF));
     }
     cp_async_commit();
   };
   prologue(fetch1, 0, 1, D);
-  double Am[N][N], Jp[N][N], Jc[N][N], ap[N][N], dp[N];
+  double Am[N][N], Jp[N][N], Jc[N][N], ap[N][N], dp[N], h0[N], h1[N];
 #pragma unroll
-  for (int r = 0; r < N; ++r)
+  for (int r = 0; r < N; ++r) {
+    h0[r] = 0.;
+    h1[r] = 0.;
 #pragma unroll
     for (int q = 0; q < N; ++q) {
       Am[r][q] = *Tp(0, tA + r * N + q);
       Jp[r][q] = *Tp(0, tJ + r * N + q);
       Jc[r][q] = *Tp(1, tJ + r * N + q);
+      ap[r][q] = 0.;
     }
+  }
   // sum (rho V)^2 and Q = sum g_out[IDN] rho (rho V): the redistribution's
   // cotangents are g_B = Q / S and g_S = -Q B_dry / S^2
   double sum_a2 = 0., qg = 0.;
@@ -1037,6 +1051,34 @@ __global__ void __launch_bounds__(128) k_vadj_sweep(Geo g, Phys p, AdjBufs b) {
     const double rho = *r1.at(slot, 2 * NN + N), ai = rho * V;
     sum_a2 += ai * ai;
     qg += *r1.at(slot, 2 * NN + N + 1) * rho * ai;
+    {  // h_i from h_{i-1} and the reduced block of layer i-1 (ap)
+      double g0[N], g1[N];
+#pragma unroll
+      for (int r = 0; r < N; ++r) {
+        g0[r] = *r1.at(slot, 2 * NN + N + 1 + r);
+        g1[r] = 0.;
+      }
+      g0[0] += *r1.at(slot, 2 * NN + 2 * N + 1);
+      g1[0] = -V;
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        double s0 = 0., s1 = 0.;
+#pragma unroll
+        for (int r = 0; r < N; ++r) {
+          s0 += ap[r][q] * h0[r];
+          s1 += ap[r][q] * h1[r];
+        }
+        g0[q] -= s0;
+        g1[q] -= s1;
+      }
+#pragma unroll
+      for (int r = 0; r < N; ++r) {
+        h0[r] = g0[r];
+        h1[r] = g1[r];
+        Sat(i, oT + r) = g0[r];
+        Sat(i, oH1 + r) = g1[r];
+      }
+    }
     double a[N][N], bb[N][N], c[N][N];
 #pragma unroll
     for (int r = 0; r < N; ++r)
@@ -1079,11 +1121,21 @@ __global__ void __launch_bounds__(128) k_vadj_sweep(Geo g, Phys p, AdjBufs b) {
         rhs[r] = rhs[r] - bd;
       }
     }
+    if constexpr (N == 3) {
+      double inv[3][3];
+      inverse3(a, inv);
 #pragma unroll
-    for (int r = 0; r < N; ++r)
+      for (int r = 0; r < N; ++r)
 #pragma unroll
-      for (int q = 0; q < N; ++q) Sat(i, oAH + r * N + q) = a[r][q];
-    block_solve<N>(a, c, rhs);
+        for (int q = 0; q < N; ++q) Sat(i, oAH + r * N + q) = inv[r][q];
+      apply_inverse3(inv, c, rhs);
+    } else {
+#pragma unroll
+      for (int r = 0; r < N; ++r)
+#pragma unroll
+        for (int q = 0; q < N; ++q) Sat(i, oAH + r * N + q) = a[r][q];
+      block_solve<N>(a, c, rhs);
+    }
     fetch1(i + D, slot);  // consumed: refill
     slot = slot + 1 == D ? 0 : slot + 1;
 #pragma unroll
@@ -1106,158 +1158,118 @@ __global__ void __launch_bounds__(128) k_vadj_sweep(Geo g, Phys p, AdjBufs b) {
       }
   }
   cp_async_wait<0>();
+  const double gb = qg / sum_a2;
 
-  // (2) back substitution, B_dry accumulated from the top as in the forward
-  constexpr int E_2 = NN + N + 1;
+  // (B) back substitution (B_dry accumulated from the top as in the forward
+  // sweep) with the backward recurrence of the transposed solve beside it:
+  // t_i = ahat_i^-T (h_i - b_{i+1}^T t_{i+1}),
+  // b_{i+1} = -(|A|_{face i+1} + J_{cell i}) A hiv
+  constexpr int E_2 = 4 * NN + 3 * N + 1;
+  static_assert(E_2 <= VadjRing<N>::elems, "ring slot");
+  // slot: a~_i (0), d'_i (NN), du_i[IDN] (NN+N), h0_i (NN+N+1), h1_i
+  // (NN+2N+1), ahat_i or its inverse (NN+3N+1), |A| and J of index i+1
+  // (2NN+3N+1, 3NN+3N+1)
+  const int sD = NN, sDU = NN + N, sH0 = NN + N + 1, sH1 = NN + 2 * N + 1, sM = NN + 3 * N + 1,
+            sA = 2 * NN + 3 * N + 1, sJ = 3 * NN + 3 * N + 1;
   Ring r2{vadj_ring, E_2, nt, lane};
-  // the reduced block and the partial solution of layer i (not adjacent in S)
-  auto fetch2d = [&](int i, int slot) {
+  auto fetch2 = [&](int i, int slot) {
     if (i >= 0) {
 #pragma unroll
-      for (int e = 0; e < NN; ++e) cp_async_bytes8(r2.at(slot, e), &Sat(i, oAT + e));
-#pragma unroll
-      for (int r = 0; r < N; ++r) cp_async_bytes8(r2.at(slot, NN + r), &Sat(i, oD + r));
-      cp_async_bytes8(r2.at(slot, NN + N), Tp(i, tDU));
-    }
-    cp_async_commit();
-  };
-  double dn[N];
-#pragma unroll
-  for (int r = 0; r < N; ++r) dn[r] = dp[r];
-  double b_dry = (*Tp(nl - 1, tDU) - dn[0]) * 1. * V;
-  prologue(fetch2d, nl - 2, -1, nl - 1);
-  for (int i = nl - 2, slot = 0; i >= 0; --i) {
-    cp_async_wait<D - 1>();
-    double cur[NN + N];
-#pragma unroll
-    for (int e = 0; e < NN + N; ++e) cur[e] = *r2.at(slot, e);
-    const double du0 = *r2.at(slot, NN + N);
-    double d[N];
-#pragma unroll
-    for (int r = 0; r < N; ++r) {
-      double t = 0.;
-#pragma unroll
-      for (int q = 0; q < N; ++q) t += cur[r * N + q] * dn[q];
-      d[r] = cur[NN + r] - t;
-    }
-    b_dry += (du0 - d[0]) * 1. * V;
-    fetch2d(i - D, slot);
-    slot = slot + 1 == D ? 0 : slot + 1;
-#pragma unroll
-    for (int r = 0; r < N; ++r) {
-      dn[r] = d[r];
-      Sat(i, oD + r) = d[r];
-    }
-  }
-  cp_async_wait<0>();
-
-  // (3) cotangents of the redistribution's B_dry and S
-  const double gb = qg / sum_a2, gS = -qg * b_dry / (sum_a2 * sum_a2);
-  Z[0] = b_dry / sum_a2;
-  Z[ncol] = gS;
-  Z[2 * ncol] = gb;
-
-  // (4) h_i = g_delta_i - a~_{i-1}^T h_{i-1}
-  constexpr int E_4 = N + 1 + NN;
-  Ring r4{vadj_ring, E_4, nt, lane};
-  auto fetch4 = [&](int i, int slot) {
-    if (i < nl) {
-#pragma unroll
-      for (int r = 0; r < N; ++r) cp_async_bytes8(r4.at(slot, r), Tp(i, tG + r));
-      cp_async_bytes8(r4.at(slot, N), Tp(i, tGF));
-      if (i > 0) {
-#pragma unroll
-        for (int e = 0; e < NN; ++e) cp_async_bytes8(r4.at(slot, N + 1 + e), &Sat(i - 1, oAT + e));
+      for (int e = 0; e < NN; ++e) {
+        cp_async_bytes8(r2.at(slot, e), &Sat(i, oAT + e));
+        cp_async_bytes8(r2.at(slot, sM + e), &Sat(i, oAH + e));
       }
-    }
-    cp_async_commit();
-  };
-  prologue(fetch4, 0, 1, D);
-  double hp[N];
 #pragma unroll
-  for (int r = 0; r < N; ++r) hp[r] = 0.;
-  for (int i = 0, slot = 0; i < nl; ++i) {
-    cp_async_wait<D - 1>();
-    double h[N];
-#pragma unroll
-    for (int r = 0; r < N; ++r) h[r] = *r4.at(slot, r);
-    h[0] += -V * gb + *r4.at(slot, N);
-    if (i > 0) {
-#pragma unroll
-      for (int q = 0; q < N; ++q) {
-        double sacc = 0.;
-#pragma unroll
-        for (int r = 0; r < N; ++r) sacc += *r4.at(slot, N + 1 + r * N + q) * hp[r];
-        h[q] -= sacc;
+      for (int r = 0; r < N; ++r) {
+        cp_async_bytes8(r2.at(slot, sD + r), &Sat(i, oD + r));
+        cp_async_bytes8(r2.at(slot, sH0 + r), &Sat(i, oT + r));
+        cp_async_bytes8(r2.at(slot, sH1 + r), &Sat(i, oH1 + r));
       }
-    }
-    fetch4(i + D, slot);
-    slot = slot + 1 == D ? 0 : slot + 1;
-#pragma unroll
-    for (int r = 0; r < N; ++r) {
-      hp[r] = h[r];
-      Sat(i, oT + r) = h[r];
-    }
-  }
-  cp_async_wait<0>();
-
-  // (5) t_i = ahat_i^-T (h_i - b_{i+1}^T t_{i+1}),
-  //     b_{i+1} = -(|A|_{face i+1} + J_{cell i}) A hiv
-  constexpr int E_5 = 3 * NN + N;
-  Ring r5{vadj_ring, E_5, nt, lane};
-  auto fetch5 = [&](int i, int slot) {
-    if (i >= 0) {
-#pragma unroll
-      for (int r = 0; r < N; ++r) cp_async_bytes8(r5.at(slot, r), &Sat(i, oT + r));
-#pragma unroll
-      for (int e = 0; e < NN; ++e) cp_async_bytes8(r5.at(slot, N + e), &Sat(i, oAH + e));
+      cp_async_bytes8(r2.at(slot, sDU), Tp(i, tDU));
       if (i + 1 < nl) {
 #pragma unroll
         for (int e = 0; e < NN; ++e) {
-          cp_async_bytes8(r5.at(slot, N + NN + e), Tp(i + 1, tA + e));
-          cp_async_bytes8(r5.at(slot, N + 2 * NN + e), Tp(i + 1, tJ + e));
+          cp_async_bytes8(r2.at(slot, sA + e), Tp(i + 1, tA + e));
+          cp_async_bytes8(r2.at(slot, sJ + e), Tp(i + 1, tJ + e));
         }
       }
     }
     cp_async_commit();
   };
-  prologue(fetch5, nl - 1, -1, nl);
-  double tn[N];
+  double dn[N], tn[N];
 #pragma unroll
-  for (int r = 0; r < N; ++r) tn[r] = 0.;
+  for (int r = 0; r < N; ++r) {
+    dn[r] = dp[r];
+    tn[r] = 0.;
+  }
+  double b_dry = (*Tp(nl - 1, tDU) - dn[0]) * 1. * V;
+  prologue(fetch2, nl - 1, -1, nl);
   for (int i = nl - 1, slot = 0; i >= 0; --i) {
     cp_async_wait<D - 1>();
+    if (i < nl - 1) {  // delta_i = d'_i - a~_i delta_{i+1}
+      double d[N];
+#pragma unroll
+      for (int r = 0; r < N; ++r) {
+        double t = 0.;
+#pragma unroll
+        for (int q = 0; q < N; ++q) t += *r2.at(slot, r * N + q) * dn[q];
+        d[r] = *r2.at(slot, sD + r) - t;
+      }
+      b_dry += (*r2.at(slot, sDU) - d[0]) * 1. * V;
+#pragma unroll
+      for (int r = 0; r < N; ++r) {
+        dn[r] = d[r];
+        Sat(i, oD + r) = d[r];
+      }
+    }
     double y[N];
 #pragma unroll
-    for (int r = 0; r < N; ++r) y[r] = *r5.at(slot, r);
+    for (int r = 0; r < N; ++r) y[r] = *r2.at(slot, sH0 + r) + gb * *r2.at(slot, sH1 + r);
     if (i + 1 < nl) {
 #pragma unroll
       for (int q = 0; q < N; ++q) {
         double sacc = 0.;
 #pragma unroll
         for (int r = 0; r < N; ++r) {
-          double bq = -(*r5.at(slot, N + NN + r * N + q) + *r5.at(slot, N + 2 * NN + r * N + q)) *
-                      Aa * hiv;
+          double bq = -(*r2.at(slot, sA + r * N + q) + *r2.at(slot, sJ + r * N + q)) * Aa * hiv;
           sacc += bq * tn[r];
         }
         y[q] -= sacc;
       }
     }
-    double M[N][N];
+    double tv[N];
+    if constexpr (N == 3) {
 #pragma unroll
-    for (int r = 0; r < N; ++r)
+      for (int q = 0; q < N; ++q) {  // ahat^-T y
+        double s = 0.;
 #pragma unroll
-      for (int q = 0; q < N; ++q) M[r][q] = *r5.at(slot, N + r * N + q);
-    solve_transposed<N>(M, y);
-    fetch5(i - D, slot);
+        for (int r = 0; r < N; ++r) s += *r2.at(slot, sM + r * N + q) * y[r];
+        tv[q] = s;
+      }
+    } else {
+      double M[N][N];
+#pragma unroll
+      for (int r = 0; r < N; ++r)
+#pragma unroll
+        for (int q = 0; q < N; ++q) M[r][q] = *r2.at(slot, sM + r * N + q);
+      solve_transposed<N>(M, y);
+#pragma unroll
+      for (int r = 0; r < N; ++r) tv[r] = y[r];
+    }
+    fetch2(i - D, slot);  // consumed: refill
     slot = slot + 1 == D ? 0 : slot + 1;
 #pragma unroll
     for (int r = 0; r < N; ++r) {
-      tn[r] = y[r];
-      Sat(i, oT + r) = y[r];
+      tn[r] = tv[r];
+      Sat(i, oT + r) = tv[r];
     }
   }
   cp_async_wait<0>();
+
+  // cotangents of the redistribution's B_dry and S
+  Z[0] = b_dry / sum_a2;
+  Z[ncol] = -qg * b_dry / (sum_a2 * sum_a2);
+  Z[2 * ncol] = gb;
 }
 
 // d/dw of y^T |A|(wl, wr) x, one primitive slot of one side per dual pass
@@ -1429,6 +1441,7 @@ static cudaError_t launch_vic_adj_n(const Geo& g, const Phys& p, const AdjBufs& 
   k_vadj_assemble<N, NS><<<ga, 256, 0, st>>>(g, p, b);
   // the ring takes vadj_ring_bytes per thread: 32-thread CTAs
   const int bs = 32;
+  raise_smem_limit(k_vadj_sweep<N>, vadj_ring_bytes<N>(bs));
   k_vadj_sweep<N><<<(unsigned)((ncol + bs - 1) / bs), bs, vadj_ring_bytes<N>(bs), st>>>(g, p, b);
   dim3 gc((unsigned)((ncol + kCTC - 1) / kCTC), (unsigned)((nl + 2 + kCTL - 1) / kCTL));
   k_vadj_contract<N, NS><<<gc, 128, 0, st>>>(g, p, b);

@@ -79,37 +79,49 @@ __device__ __forceinline__ void absA_block(T gm1, const T* wl, const T* wr, T (&
 }
 
 
+// cofactor inverse of a 3 x 3 block
+template <class T>
+__device__ __forceinline__ void inverse3(const T (&M)[3][3], T (&inv)[3][3]) {
+  auto cof = [&](int i, int j) {
+    int i1 = (i + 1) % 3, i2 = (i + 2) % 3, j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+    return M[i1][j1] * M[i2][j2] - M[i1][j2] * M[i2][j1];
+  };
+  T c00 = cof(0, 0), c10 = cof(1, 0), c20 = cof(2, 0);
+  T det = c00 * M[0][0] + c10 * M[1][0] + c20 * M[2][0];
+  T id = T(1) / det;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) inv[i][j] = cof(j, i) * id;
+}
+
+// [C | rhs] <- inv [C | rhs] for a 3 x 3 inverse
+template <class T>
+__device__ __forceinline__ void apply_inverse3(const T (&inv)[3][3], T (&C)[3][3], T (&rhs)[3]) {
+  T x[3], X[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    x[i] = inv[i][0] * rhs[0] + inv[i][1] * rhs[1] + inv[i][2] * rhs[2];
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      X[i][j] = inv[i][0] * C[0][j] + inv[i][1] * C[1][j] + inv[i][2] * C[2][j];
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    rhs[i] = x[i];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) C[i][j] = X[i][j];
+  }
+}
+
 // X = M^-1 [C | rhs] for an N x N block: cofactor inverse for N = 3,
 // LU with implicit-scaling partial pivoting (Crout) for N = 5
 template <int N, class T>
 __device__ __forceinline__ void block_solve(T (&M)[N][N], T (&C)[N][N], T (&rhs)[N]) {
   if constexpr (N == 3) {
-    auto cof = [&](int i, int j) {
-      int i1 = (i + 1) % 3, i2 = (i + 2) % 3, j1 = (j + 1) % 3, j2 = (j + 2) % 3;
-      return M[i1][j1] * M[i2][j2] - M[i1][j2] * M[i2][j1];
-    };
-    T c00 = cof(0, 0), c10 = cof(1, 0), c20 = cof(2, 0);
-    T det = c00 * M[0][0] + c10 * M[1][0] + c20 * M[2][0];
-    T id = T(1) / det;
     T inv[3][3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-      for (int j = 0; j < 3; ++j) inv[i][j] = cof(j, i) * id;
-    T x[3], X[3][3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      x[i] = inv[i][0] * rhs[0] + inv[i][1] * rhs[1] + inv[i][2] * rhs[2];
-#pragma unroll
-      for (int j = 0; j < 3; ++j)
-        X[i][j] = inv[i][0] * C[0][j] + inv[i][1] * C[1][j] + inv[i][2] * C[2][j];
-    }
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      rhs[i] = x[i];
-#pragma unroll
-      for (int j = 0; j < 3; ++j) C[i][j] = X[i][j];
-    }
+    inverse3(M, inv);
+    apply_inverse3(inv, C, rhs);
   } else {
     T vv[N];
 #pragma unroll
