@@ -37,6 +37,7 @@
 // ImplicitHydroImpl::forward (src/implicit/implicit_hydro.cpp:99-189),
 // MeshBlockImpl::forward (src/mesh/meshblock.cpp:577-786), bc_func (src/bc/bc_func.cpp:7-63).
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 
@@ -44,6 +45,7 @@
 #include "kernels.cuh"
 #include "ring.cuh"
 #include "riemann_adj.cuh"
+#include "block_cr.cuh"
 #include "vic_blocks.cuh"
 
 namespace snapb {
@@ -1272,6 +1274,137 @@ __global__ void __launch_bounds__(128) k_vadj_sweep(Geo g, Phys p, AdjBufs b) {
   Z[2 * ncol] = gb;
 }
 
+// Few columns (3x3 blocks): the two solves of the adjoint column sweep by
+// block cyclic reduction, one CTA per column, the column's system in shared
+// memory.  g_B = Q / S needs only the column sums, so the right-hand side of
+// the transposed solve is known before either solve: A delta = du / dt gives
+// the forward solution (and B_dry), A^T t = g_delta + (g_fix - V g_B) e_0 the
+// transposed one, each in log2(nl) parallel steps instead of nl sequential
+// layers.  The blocks are those of k_vadj_sweep (|A| and J from the assembly
+// in T, the same folds at the first and last layers); the outputs (delta and
+// t in S, the cotangents in Z) are the sweep's, up to FP64 rounding.
+constexpr int kVadjCrThreads = 128;
+constexpr int64_t kVadjCrMaxCols = 148 * 64;  // above this the sweep fills the GPU
+inline size_t vadj_cr_smem_bytes(int nl) {
+  return ((size_t)nl * 30 + 2 * (kVadjCrThreads / 32)) * sizeof(double);
+}
+
+__global__ void __launch_bounds__(kVadjCrThreads) k_vadj_cr3(Geo g, Phys p, AdjBufs b) {
+  constexpr int N = 3, NN = 9;
+  constexpr int E1 = VadjDims<N>::E1, ES = VadjDims<N>::ES;
+  extern __shared__ __align__(16) double vadj_cr[];
+  const int64_t ncol = (int64_t)(g.ju - g.jl + 1) * (g.ku - g.kl + 1);
+  const int64_t col = blockIdx.x;
+  const int nl = g.nx1, tid = threadIdx.x, nt = blockDim.x;
+  const double* T = b.vic + col;
+  double* S = b.vic + (int64_t)(nl + 2) * E1 * ncol + col;
+  double* Z = S + (int64_t)nl * ES * ncol;
+  auto Tp = [&](int t, int e) { return T[((int64_t)t * E1 + e) * ncol]; };
+  auto Sat = [&](int i, int e) -> double& { return S[((int64_t)i * ES + e) * ncol]; };
+  const int tA = 0, tJ = NN, tDU = 2 * NN, tRHO = 2 * NN + N, tG = 2 * NN + N + 1,
+            tGF = 2 * NN + 2 * N + 1;
+  const int oD = 2 * NN, oT = 2 * NN + N;
+  double* Bl = vadj_cr;         // [nl][9] block of x_{i-1}
+  double* Dg = Bl + 9 * nl;     // [nl][9] diagonal block
+  double* Ab = Dg + 9 * nl;     // [nl][9] block of x_{i+1}
+  double* R = Ab + 9 * nl;      // [nl][3] right-hand side, then solution
+  double* red = R + 3 * nl;     // reduction scratch
+  const double dt = *b.dt;
+  const double Aa = g.A1, hiv = 0.5 / g.vol, idt = 1. / dt, grav = p.grav1, V = g.vol;
+  // b_i (x_{i-1}), a_i (folded) and c_i (x_{i+1}) of layer i, as the sweep
+  // forms them
+  auto blocks = [&](int i, double (&a)[N][N], double (&bb)[N][N], double (&c)[N][N]) {
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        const int k = r * N + q;
+        const double Am = Tp(i, tA + k), Ap = Tp(i + 1, tA + k);
+        const double Jp = Tp(i, tJ + k), Jn = Tp(i + 2, tJ + k);
+        double phi = 0.;
+        if (r == 1 && q == 0) phi = grav;
+        if (r == 2 && q == 1) phi = grav;
+        a[r][q] = (Am * Aa + Ap * Aa) * hiv - phi;
+        bb[r][q] = -(Am + Jp) * Aa * hiv;
+        c[r][q] = -(Ap - Jn) * Aa * hiv;
+      }
+#pragma unroll
+    for (int r = 0; r < N; ++r) a[r][r] += idt;
+    if (i == 0) {
+#pragma unroll
+      for (int r = 0; r < N; ++r)
+#pragma unroll
+        for (int q = 0; q < N; ++q) a[r][q] += bb[r][q] * (q == 1 ? -1. : 1.);
+    }
+    if (i == nl - 1) {
+#pragma unroll
+      for (int r = 0; r < N; ++r)
+#pragma unroll
+        for (int q = 0; q < N; ++q) a[r][q] += c[r][q] * (q == 1 ? -1. : 1.);
+    }
+  };
+  // (1) the system A delta = du / dt; sum (rho V)^2 and Q = sum g_out[IDN] rho (rho V)
+  double sa2 = 0., qg = 0.;
+  for (int i = tid; i < nl; i += nt) {
+    double a[N][N], bb[N][N], c[N][N];
+    blocks(i, a, bb, c);
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        Dg[i * 9 + r * 3 + q] = a[r][q];
+        Bl[i * 9 + r * 3 + q] = i == 0 ? 0. : bb[r][q];
+        Ab[i * 9 + r * 3 + q] = i == nl - 1 ? 0. : c[r][q];
+      }
+#pragma unroll
+    for (int r = 0; r < N; ++r) R[i * 3 + r] = Tp(i, tDU + r) / dt;
+    const double rho = Tp(i, tRHO), ai = rho * V;
+    sa2 += ai * ai;
+    qg += Tp(i, tG) * rho * ai;
+  }
+  cta_sum2(sa2, qg, red);  // (its barrier also completes the system)
+  const double gb = qg / sa2;
+  block_cr3_solve(Bl, Dg, Ab, R, nl);
+  // (2) delta and B_dry; then the transposed system: row i of A^T couples
+  // x_{i-1} by c_{i-1}^T and x_{i+1} by b_{i+1}^T
+  double bdry = 0., unused = 0.;
+  for (int i = tid; i < nl; i += nt) {
+#pragma unroll
+    for (int r = 0; r < N; ++r) Sat(i, oD + r) = R[i * 3 + r];
+    bdry += (Tp(i, tDU) - R[i * 3]) * 1. * V;
+  }
+  __syncthreads();  // R is read
+  for (int i = tid; i < nl; i += nt) {
+    double a[N][N], bb[N][N], c[N][N];
+    blocks(i, a, bb, c);
+#pragma unroll
+    for (int r = 0; r < N; ++r)
+#pragma unroll
+      for (int q = 0; q < N; ++q) {
+        Dg[i * 9 + r * 3 + q] = a[q][r];
+        const int k = q * N + r;  // transposed
+        // c_{i-1} = -(|A|_{face i} - J_{cell i}) A hiv, b_{i+1} = -(|A|_{face i+1} + J_{cell i}) A hiv
+        Bl[i * 9 + r * 3 + q] = i == 0 ? 0. : -(Tp(i, tA + k) - Tp(i + 1, tJ + k)) * Aa * hiv;
+        Ab[i * 9 + r * 3 + q] =
+            i == nl - 1 ? 0. : -(Tp(i + 1, tA + k) + Tp(i + 1, tJ + k)) * Aa * hiv;
+      }
+#pragma unroll
+    for (int r = 0; r < N; ++r) R[i * 3 + r] = Tp(i, tG + r);
+    R[i * 3] += -V * gb + Tp(i, tGF);
+  }
+  cta_sum2(bdry, unused, red);  // (its barrier also completes the system)
+  block_cr3_solve(Bl, Dg, Ab, R, nl);
+  for (int i = tid; i < nl; i += nt) {
+#pragma unroll
+    for (int r = 0; r < N; ++r) Sat(i, oT + r) = R[i * 3 + r];
+  }
+  if (tid == 0) {
+    Z[0] = bdry / sa2;
+    Z[ncol] = -qg * bdry / (sa2 * sa2);
+    Z[2 * ncol] = gb;
+  }
+}
+
 // d/dw of y^T |A|(wl, wr) x, one primitive slot of one side per dual pass
 template <int N>
 __device__ __forceinline__ void absA_bilinear_grad(double gm1f, const double* wl, const double* wr,
@@ -1432,6 +1565,17 @@ __global__ void __launch_bounds__(128) k_vadj_contract(Geo g, Phys p, AdjBufs b)
   }
 }
 
+// SNAPB_VADJ_SOLVE = "sweep" or "cr" forces the adjoint's column solver (the
+// sweep, or cyclic reduction where it applies); by default cyclic reduction
+// takes up to kVadjCrMaxCols columns of 3x3 blocks
+static int vadj_solver_env() {
+  const char* e = std::getenv("SNAPB_VADJ_SOLVE");
+  if (!e) return 0;
+  if (std::strcmp(e, "sweep") == 0) return 1;
+  if (std::strcmp(e, "cr") == 0) return 2;
+  return 0;
+}
+
 template <int N, int NS>
 static cudaError_t launch_vic_adj_n(const Geo& g, const Phys& p, const AdjBufs& b,
                                     cudaStream_t st) {
@@ -1439,10 +1583,19 @@ static cudaError_t launch_vic_adj_n(const Geo& g, const Phys& p, const AdjBufs& 
   const int nl = g.nx1;
   dim3 ga((unsigned)((ncol + kATC - 1) / kATC), (unsigned)((nl + 2 + kATL<N> - 1) / kATL<N>));
   k_vadj_assemble<N, NS><<<ga, 256, 0, st>>>(g, p, b);
-  // the ring takes vadj_ring_bytes per thread: 32-thread CTAs
-  const int bs = 32;
-  raise_smem_limit(k_vadj_sweep<N>, vadj_ring_bytes<N>(bs));
-  k_vadj_sweep<N><<<(unsigned)((ncol + bs - 1) / bs), bs, vadj_ring_bytes<N>(bs), st>>>(g, p, b);
+  const size_t cr_smem = vadj_cr_smem_bytes(nl);
+  const int forced = vadj_solver_env();
+  const bool cr_fits = N == 3 && cr_smem <= 200 * 1024;
+  if (cr_fits && (forced == 2 || (forced == 0 && ncol <= kVadjCrMaxCols))) {
+    raise_smem_limit(k_vadj_cr3, 200 * 1024);  // once per kernel: the largest plan
+    k_vadj_cr3<<<(unsigned)ncol, kVadjCrThreads, cr_smem, st>>>(g, p, b);
+  } else {
+    // the ring takes vadj_ring_bytes per thread: 32-thread CTAs
+    const int bs = 32;
+    raise_smem_limit(k_vadj_sweep<N>, vadj_ring_bytes<N>(bs));
+    k_vadj_sweep<N><<<(unsigned)((ncol + bs - 1) / bs), bs, vadj_ring_bytes<N>(bs), st>>>(g, p,
+                                                                                         b);
+  }
   dim3 gc((unsigned)((ncol + kCTC - 1) / kCTC), (unsigned)((nl + 2 + kCTL - 1) / kCTL));
   k_vadj_contract<N, NS><<<gc, 128, 0, st>>>(g, p, b);
   return cudaGetLastError();
