@@ -310,8 +310,8 @@ def rel_errors(a, b, it):
 # member groups of the end-to-end form (copies of one group overlap the others' steps)
 E2E_GROUPS = 4
 
-NCU_TRAFFIC_PER_CELL_F32 = {"x1_sweep": 70.7, "x2_sweep": 66.2, "x3_sweep": 66.2,
-                            "implicit_vic": 348.5}
+NCU_TRAFFIC_PER_CELL_F32 = {"x1_sweep": 69.3, "x2_sweep": 66.1, "x3_sweep": 66.1,
+                            "implicit_vic": 347.2}
 
 
 def dominant_roofline(kern, cfg, cells, elem, peak, peak_src):
