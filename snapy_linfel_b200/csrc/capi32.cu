@@ -19,8 +19,8 @@ cudaError_t launch_to_pert(const Geo& g, const Phys& p, int kind, const double* 
                            const double* rb, const double* pb, float* out, cudaStream_t st);
 cudaError_t launch_from_pert(const Geo& g, const Phys& p, int kind, const float* in,
                              const double* rb, const double* pb, double* out, cudaStream_t st);
-cudaError_t launch_cfl32(const Geo& g, const Phys& p, const float* w, const double* rb,
-                         const double* pb, unsigned long long* slots, cudaStream_t st);
+cudaError_t launch_cfl32(const Geo& g, const Phys& p, const float* w, const float* rbf,
+                         const float* pbf, unsigned long long* slots, cudaStream_t st);
 size_t x1_smem32_per_column(const Geo& g, int nvt);
 }  // namespace snapb
 
@@ -261,7 +261,7 @@ int snapb_max_time_step_f32(const snapb_hydro_config* cfg, const float* w, doubl
   cudaStream_t st = (cudaStream_t)stream;
   auto* slots = at<unsigned long long>(workspace, L.SLOTS);
   cudaError_t e = cudaMemsetAsync(slots, 0x7f, 3 * sizeof(unsigned long long), st);
-  if (e == cudaSuccess) e = launch_cfl32(g, p, w, b.rb, b.pb, slots, st);
+  if (e == cudaSuccess) e = launch_cfl32(g, p, w, b.rbf, b.pbf, slots, st);
   if (e == cudaSuccess) e = launch_cfl_final(g, p, slots, dt_out, st);
   return cuda32(e, "max_time_step_f32");
 }

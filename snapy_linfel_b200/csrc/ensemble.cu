@@ -40,23 +40,22 @@ __global__ void __launch_bounds__(256) k_cfl32_batch(const Member32* __restrict_
   while (queue_next(q, m, tile)) {
     const Geo& g = mem[m].g;
     const float* w = mem[m].b.w;
-    const double* rb = mem[m].b.rb;
-    const double* pb = mem[m].b.pb;
+    const float* rbf = mem[m].b.rbf;
+    const float* pbf = mem[m].b.pbf;
     const int ni = g.iu - g.il + 1, nj = g.ju - g.jl + 1, nk = g.ku - g.kl + 1;
     const int64_t n = (int64_t)ni * nj * nk;
-    double m1 = 1.7e308, m2 = 1.7e308, m3 = 1.7e308;
+    const float gamma = (float)p.gammad;
+    float a[3] = {0.f, 0.f, 0.f};
     const int64_t t0 = tile * kCflItem;
     for (int64_t t = t0 + threadIdx.x; t < min(t0 + kCflItem, n); t += blockDim.x) {
       int i = g.il + umod(t, ni);
       int j = g.jl + umod(udiv(t, ni), nj);
       int k = g.kl + udiv(t, (int64_t)ni * nj);
       int64_t o = (int64_t)k * g.s3 + (int64_t)j * g.s2 + i;
-      double rho = rb[i] + w[IDN * g.sv + o], pr = pb[i] + w[IPR * g.sv + o];
-      double cs = sqrt(p.gammad * pr / rho);
-      if (use1) m1 = fmin(m1, g.dx1 / (fabs((double)w[IVX * g.sv + o]) + cs));
-      if (use2) m2 = fmin(m2, g.dx2 / (fabs((double)w[IVY * g.sv + o]) + cs));
-      if (use3) m3 = fmin(m3, g.dx3 / (fabs((double)w[IVZ * g.sv + o]) + cs));
+      cfl32_speeds(w, g.sv, o, rbf[i], pbf[i], gamma, a);
     }
+    double m1, m2, m3;
+    cfl32_limits(g, use1, use2, use3, a, m1, m2, m3);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       m1 = fmin(m1, __shfl_xor_sync(0xffffffffu, m1, o));

@@ -234,6 +234,32 @@ __device__ __forceinline__ void set_stage32(StageBufs32& b, int stage) {
   b.wgt2 = w2;
 }
 
+// CFL limit of the FP32 form: the signal speeds |v_d| + cs of one cell in
+// FP32 (full density and pressure from the FP32 copies of the reference).  A
+// thread keeps the largest speed per axis and turns it into dx_d / a_max_d
+// (FP64) once: correctly rounded division is monotone, so the minimum over
+// cells of dx / a equals dx / (max over cells of a) however the cells are
+// split between threads, and the single-domain and batched reductions agree
+// to the bit.
+__device__ __forceinline__ void cfl32_speeds(const float* w, int64_t sv, int64_t o, float rbf,
+                                             float pbf, float gamma, float (&a)[3]) {
+  const float rho = rbf + w[IDN * sv + o], pr = pbf + w[IPR * sv + o];
+  const float cs = sqrtf(fdiv(gamma * pr, rho));
+#pragma unroll
+  for (int d = 0; d < 3; ++d) a[d] = fmaxf(a[d], fabsf(w[(IVX + d) * sv + o]) + cs);
+}
+// dx_d / a_d for the used axes (1.7e308 for the others)
+__device__ __forceinline__ void cfl32_limits(const Geo& g, int use1, int use2, int use3,
+                                             const float (&a)[3], double& m1, double& m2,
+                                             double& m3) {
+  m1 = use1 ? g.dx1 / (double)a[0] : 1.7e308;
+  m2 = use2 ? g.dx2 / (double)a[1] : 1.7e308;
+  m3 = use3 ? g.dx3 / (double)a[2] : 1.7e308;
+  m1 = fmin(m1, 1.7e308);  // (a thread without cells: dx / 0)
+  m2 = fmin(m2, 1.7e308);
+  m3 = fmin(m3, 1.7e308);
+}
+
 // launchers (return a cudaError_t of the launch)
 cudaError_t launch_x1(const Geo& g, const Phys& p, const StageBufs& b, bool last,
                       cudaStream_t st);

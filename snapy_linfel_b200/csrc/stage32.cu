@@ -657,22 +657,21 @@ __device__ __forceinline__ double warp_min32(double x) {
 }
 
 __global__ void k_cfl32(Geo g, double gammad, int use1, int use2, int use3, const float* w,
-                        const double* rb, const double* pb, unsigned long long* slots) {
+                        const float* rbf, const float* pbf, unsigned long long* slots) {
   const int ni = g.iu - g.il + 1, nj = g.ju - g.jl + 1, nk = g.ku - g.kl + 1;
   const int64_t n = (int64_t)ni * nj * nk;
-  double m1 = 1.7e308, m2 = 1.7e308, m3 = 1.7e308;
+  const float gamma = (float)gammad;
+  float a[3] = {0.f, 0.f, 0.f};
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
        t += (int64_t)gridDim.x * blockDim.x) {
     int i = g.il + umod(t, ni);
     int j = g.jl + umod(udiv(t, ni), nj);
     int k = g.kl + udiv(t, (int64_t)ni * nj);
     int64_t o = (int64_t)k * g.s3 + (int64_t)j * g.s2 + i;
-    double rho = rb[i] + w[IDN * g.sv + o], pr = pb[i] + w[IPR * g.sv + o];
-    double cs = sqrt(gammad * pr / rho);
-    if (use1) m1 = fmin(m1, g.dx1 / (fabs((double)w[IVX * g.sv + o]) + cs));
-    if (use2) m2 = fmin(m2, g.dx2 / (fabs((double)w[IVY * g.sv + o]) + cs));
-    if (use3) m3 = fmin(m3, g.dx3 / (fabs((double)w[IVZ * g.sv + o]) + cs));
+    cfl32_speeds(w, g.sv, o, rbf[i], pbf[i], gamma, a);
   }
+  double m1, m2, m3;
+  cfl32_limits(g, use1, use2, use3, a, m1, m2, m3);
   __shared__ double red[3][32];
   m1 = warp_min32(m1);
   m2 = warp_min32(m2);
@@ -998,8 +997,8 @@ cudaError_t launch_from_pert(const Geo& g, const Phys& p, int kind, const float*
   return cudaGetLastError();
 }
 
-cudaError_t launch_cfl32(const Geo& g, const Phys& p, const float* w, const double* rb,
-                         const double* pb, unsigned long long* slots, cudaStream_t st) {
+cudaError_t launch_cfl32(const Geo& g, const Phys& p, const float* w, const float* rbf,
+                         const float* pbf, unsigned long long* slots, cudaStream_t st) {
   int scheme = p.implicit_scheme;
   int use1 = g.nc1 > 1, use2 = g.nc2 > 1, use3 = g.nc3 > 1;
   if (scheme != 0) {
@@ -1009,7 +1008,7 @@ cudaError_t launch_cfl32(const Geo& g, const Phys& p, const float* w, const doub
   }
   int64_t n = (int64_t)(g.iu - g.il + 1) * (g.ju - g.jl + 1) * (g.ku - g.kl + 1);
   int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
-  k_cfl32<<<blocks, 256, 0, st>>>(g, p.gammad, use1, use2, use3, w, rb, pb, slots);
+  k_cfl32<<<blocks, 256, 0, st>>>(g, p.gammad, use1, use2, use3, w, rbf, pbf, slots);
   return cudaGetLastError();
 }
 
