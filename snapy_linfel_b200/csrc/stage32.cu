@@ -714,9 +714,14 @@ __global__ void __launch_bounds__(512, 2) k_x1_32_batch(const Member32* __restri
   __shared__ uint64_t bar;       // completion of a tile's bulk copies
   __shared__ unsigned long long s_item;
   const int tid = threadIdx.x;
+  // Thread 0 claims work items one tile ahead of their use: the claim of the
+  // item after next is issued while the next one is being staged, so the
+  // atomic's latency overlaps a whole tile.
+  unsigned long long ahead = 0;
   if (tid == 0) {
     mbar_init(&bar, 1);
     s_item = atomicAdd(q.counter, 1ULL);
+    ahead = atomicAdd(q.counter, 1ULL);
   }
   __syncthreads();
   int m;
@@ -738,7 +743,7 @@ __global__ void __launch_bounds__(512, 2) k_x1_32_batch(const Member32* __restri
     const int64_t col0 = tile * C;
     bool ok = true;
     if (tid < 32) ok = mbar_wait(&bar, parity, &snapb_x1_bulk_timeout);
-    if (tid == 0) s_item = atomicAdd(q.counter, 1ULL);  // the next item
+    if (tid == 0) s_item = ahead;  // the next item, claimed a tile ago
     if (__syncthreads_or(!ok)) {
       if (tid < 32) mbar_wait(&bar, parity, &snapb_x1_bulk_timeout);  // copies in flight
       return;
@@ -746,18 +751,24 @@ __global__ void __launch_bounds__(512, 2) k_x1_32_batch(const Member32* __restri
     int nm;
     int64_t ntile;
     const bool more = queue_find(q, (int64_t)s_item, nm, ntile);
+    // the next tile's descriptor: the current one when the member is the same
+    const int nbuf = more && nm != m ? buf ^ 1 : buf;
     x1_32_convert<NS>(cur.g, p, cur.b, C, col0, smf, nc1max);  // (ends with a CTA barrier)
     if (more && tid < 32) {  // stage the next tile while this one's faces run
-      Member32& nxt = s_mem[buf ^ 1];
-      load_member_warp(nxt, mem, nm);
-      if (tid == 0) set_stage32(nxt.b, stage);
-      __syncwarp();
+      Member32& nxt = s_mem[nbuf];
+      if (nbuf != buf) {
+        load_member_warp(nxt, mem, nm);
+        if (tid == 0) set_stage32(nxt.b, stage);
+        __syncwarp();
+      }
       x1_32_stage<NS>(nxt.g, nxt.b, nxt.x1_cols, ntile * nxt.x1_cols, smf, nc1max, &bar);
+      if (tid == 0) ahead = atomicAdd(q.counter, 1ULL);  // the item after next
     }
     x1_32_faces<NS, FP>(cur.g, p, cur.b, C, last, col0, smf);
     if (!more) return;
     __syncthreads();  // this tile's rows are read; the next descriptor is in place
-    buf ^= 1;
+    buf = nbuf;
+    m = nm;
     parity ^= 1;
     tile = ntile;
   }
