@@ -742,40 +742,30 @@ def run_ensemble(args):
 
     # end to end: every member's state from pinned host memory and back, per
     # step.  (a) StreamedEnsemble: members in groups, each on its own stream,
-    # so one group's copies overlap the other groups' steps; (b) one stream:
-    # all copies in, the step, all copies out.
-    sens = StreamedEnsemble(members, groups=E2E_GROUPS, device=dev, tuning=tune["best"])
-    sens.capture()
-    hus = sens.host_states()
-    nbytes = sum(h.numel() * 4 for h in hus)
-    for _ in range(args.warmup):
-        sens.step(hus)
-    sens.wait()
-    barrier()
-    ev0.record(stream)
-    for _ in range(args.steps):
-        sens.step(hus)
-    sens.wait()
-    ev1.record(stream)
-    barrier()
-    e2e = cells_total * 3 * args.steps / (max_ms(ev0.elapsed_time(ev1)) / 1e3) / 1e6
-    del sens, hus
-    hus = [torch.empty(b.hydro_u.shape, dtype=torch.float32).pin_memory() for b in ens.blocks]
-    for h, b in zip(hus, ens.blocks):
-        h.copy_(b.hydro_u.cpu())
-    barrier()
-    ev0.record(stream)
-    for _ in range(args.steps):
-        for h, b in zip(hus, ens.blocks):
-            b.hydro_u.copy_(h, non_blocking=True)
-        ens.step()
-        for h, b in zip(hus, ens.blocks):
-            h.copy_(b.hydro_u, non_blocking=True)
-    ev1.record(stream)
-    barrier()
-    e2e_serial = cells_total * 3 * args.steps / (max_ms(ev0.elapsed_time(ev1)) / 1e3) / 1e6
-    del hus
-    torch.cuda.empty_cache()
+    # so one group's copies overlap the other groups' steps; (b) one group:
+    # all copies in, the step, all copies out on one stream.
+    def e2e_rate(groups):
+        sens = StreamedEnsemble(members, groups=groups, device=dev, tuning=tune["best"])
+        sens.capture()
+        hus = sens.host_states()
+        nb = sum(h.numel() * 4 for h in hus)
+        for _ in range(args.warmup):
+            sens.step(hus)
+        sens.wait()
+        barrier()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            sens.step(hus)
+        sens.wait()
+        ev1.record(stream)
+        barrier()
+        rate = cells_total * 3 * args.steps / (max_ms(ev0.elapsed_time(ev1)) / 1e3) / 1e6
+        del sens, hus
+        torch.cuda.empty_cache()
+        return rate, nb
+
+    e2e, nbytes = e2e_rate(E2E_GROUPS)
+    e2e_serial, _ = e2e_rate(1)
 
     # ---- plain FP64: member after member through snapb_stage, the whole
     # step (every member's CFL and three stages) replayed from one CUDA graph
