@@ -45,6 +45,7 @@
 #include "kernels.cuh"
 #include "ring.cuh"
 #include "riemann_adj.cuh"
+#include "bilinear_adj.cuh"
 #include "block_cr.cuh"
 #include "vic_blocks.cuh"
 
@@ -1405,50 +1406,6 @@ __global__ void __launch_bounds__(kVadjCrThreads) k_vadj_cr3(Geo g, Phys p, AdjB
   }
 }
 
-// d/dw of y^T |A|(wl, wr) x, one primitive slot of one side per dual pass
-template <int N>
-__device__ __forceinline__ void absA_bilinear_grad(double gm1f, const double* wl, const double* wr,
-                                                   int side, const double* y, const double* x,
-                                                   double* gw) {
-#pragma unroll 1
-  for (int comp = 0; comp < 5; ++comp) {
-    Dual l[5], r[5];
-#pragma unroll
-    for (int v = 0; v < 5; ++v) {
-      l[v] = Dual(wl[v], (side == 0 && v == comp) ? 1. : 0.);
-      r[v] = Dual(wr[v], (side == 1 && v == comp) ? 1. : 0.);
-    }
-    Dual A[N][N];
-    absA_block<N, Dual>(Dual(gm1f), l, r, A);
-    double s = 0.;
-#pragma unroll
-    for (int a = 0; a < N; ++a)
-#pragma unroll
-      for (int c = 0; c < N; ++c) s += y[a] * A[a][c].d * x[c];
-    gw[comp] += s;
-  }
-}
-
-// d/dw of y^T J(w) x
-template <int N>
-__device__ __forceinline__ void jac_bilinear_grad(double gm1c, const double* w, const double* y,
-                                                  const double* x, double* gw) {
-#pragma unroll 1
-  for (int comp = 0; comp < 5; ++comp) {
-    Dual wd[5];
-#pragma unroll
-    for (int v = 0; v < 5; ++v) wd[v] = Dual(w[v], v == comp ? 1. : 0.);
-    Dual J[N][N];
-    jac_block<N, Dual>(Dual(gm1c), wd, J);
-    double s = 0.;
-#pragma unroll
-    for (int a = 0; a < N; ++a)
-#pragma unroll
-      for (int c = 0; c < N; ++c) s += y[a] * J[a][c].d * x[c];
-    gw[comp] += s;
-  }
-}
-
 // Per cell m in [-1, nl] of every interior column: the block-dependence
 // contraction into GW, and (interior cells) the redistribution's density
 // term, the scalar mass-fix term and the cotangent of the explicit du.
@@ -1523,7 +1480,7 @@ __global__ void __launch_bounds__(128) k_vadj_contract(Geo g, Phys p, AdjBufs b)
         y[r] = coef * (T_(sm1, r) - T_(s0, r));
         x[r] = D_(s0, r) - D_(sm1, r);
       }
-      absA_bilinear_grad<N>(gm1f, wm, wc, 1, y, x, gw);
+      absA_bilinear_vjp<N>(gm1f, wm, wc, y, x, nullptr, gw);
     }
     // interface m+1 (cells m, m+1): w_m is its left state
     if (m + 1 <= nl) {
@@ -1532,7 +1489,7 @@ __global__ void __launch_bounds__(128) k_vadj_contract(Geo g, Phys p, AdjBufs b)
         y[r] = coef * (T_(s0, r) - T_(sp1, r));
         x[r] = D_(sp1, r) - D_(s0, r);
       }
-      absA_bilinear_grad<N>(gm1f, wc, wp, 0, y, x, gw);
+      absA_bilinear_vjp<N>(gm1f, wc, wp, y, x, gw, nullptr);
     }
     // flux Jacobian of cell m
 #pragma unroll
@@ -1540,7 +1497,7 @@ __global__ void __launch_bounds__(128) k_vadj_contract(Geo g, Phys p, AdjBufs b)
       y[r] = coef * (T_(sp1, r) - T_(sm1, r));
       x[r] = D_(s0, r);
     }
-    jac_bilinear_grad<N>(gm1c, wc, y, x, gw);
+    jac_bilinear_vjp<N>(gm1c, wc, y, x, gw);
     if (m >= 0 && m < nl) {
       // redistribution: du_out[IDN] = delta_0 + rho (rho V) B / S
       double go = b.GD[IDN * sv + off];
