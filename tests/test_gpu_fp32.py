@@ -67,6 +67,29 @@ def test_fp32_straka_implicit(riemann):
     assert np.abs(rp32 - rp64).sum() / np.abs(rp64).sum() < 1e-3
 
 
+@pytest.mark.parametrize("recon23", ["plm", "weno3"])
+def test_fp32_run_time_dispatch(recon23):
+    """A configuration outside the FP32 sweeps' compile-time face profiles
+    (WENO3 along x1, whose pressure interpolation is the linear cp3 that the
+    reference pressure needs, and PLM or WENO3 along x2), so every face takes
+    the run-time reconstruction and solver dispatch: the same bounds as the
+    profiled Straka runs."""
+    from snapy_linfel_b200.config import RECON
+
+    opts, w, _ = problems.straka(nx2=96, nx1=32, implicit_scheme=1, riemann="hllc")
+    opts.hydro.nu_iso = opts.hydro.kappa_iso = 0.0
+    opts.hydro.recon1_type = RECON["weno3"]
+    opts.hydro.recon23_type = RECON[recon23]
+    u32, u64, rho_bar, *_ = _run_pair(opts, w, None, [0.5] * 10)
+    it = opts.hydro.interior()
+    err = _errors(u32, u64, it)
+    for v in range(5):
+        assert err[v][0] < 1e-5, (v, err[v])
+    rp32 = u32[0][it] - rho_bar[None, None, it[2]]
+    rp64 = u64[0][it] - rho_bar[None, None, it[2]]
+    assert np.abs(rp32 - rp64).sum() / np.abs(rp64).sum() < 1e-3
+
+
 def test_fp32_3d_roe_vic_tracers():
     opts, w, r = problems.large_3d(nx3=24, nx2=24, nx1=48, nscalar=2)
     u32, u64, rho_bar, m32, m64 = _run_pair(opts, w, r, [0.5] * 6)
