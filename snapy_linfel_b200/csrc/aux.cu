@@ -95,12 +95,24 @@ __global__ void k_bc(Geo g, AxisBC a1, AxisBC a2, AxisBC a3, double* var, int nv
   int si = bc_map(a1, i, f1), sj = bc_map(a2, j, f2), sk = bc_map(a3, k, f3);
   if (si == i && sj == j && sk == k) return;  // interior (or identity-mapped) cell
   int64_t src = ((int64_t)sk * nc2 + sj) * nc1 + si;
-  for (int v = 0; v < nv; ++v) {
-    double x = var[v * sv + src];
-    if (flip_normals) {
-      if ((v == IVX && f1) || (v == IVY && f2) || (v == IVZ && f3)) x = -x;
+  // loads of a group of variables before its stores (a thread's source cell
+  // is never its target; the compiler cannot see that the stores miss it)
+  constexpr int kGroup = 8;
+  for (int v0 = 0; v0 < nv; v0 += kGroup) {
+    double xs[kGroup];
+#pragma unroll
+    for (int q = 0; q < kGroup; ++q)
+      if (v0 + q < nv) xs[q] = var[(v0 + q) * sv + src];
+#pragma unroll
+    for (int q = 0; q < kGroup; ++q) {
+      const int v = v0 + q;
+      if (v >= nv) break;
+      double x = xs[q];
+      if (flip_normals) {
+        if ((v == IVX && f1) || (v == IVY && f2) || (v == IVZ && f3)) x = -x;
+      }
+      var[v * sv + t] = x;
     }
-    var[v * sv + t] = x;
   }
 }
 

@@ -602,14 +602,28 @@ __device__ __forceinline__ void bc32_cell(int nc1, int nc2, int64_t sv, AxisBC32
   if (si == i && sj == j && sk == k) return;
   int64_t src = ((int64_t)sk * nc2 + sj) * nc1 + si;
   bool flip = kind != SNAPB_SCALAR;
-  for (int v = 0; v < nv; ++v) {
-    double x = var[v * sv + src];
-    if (flip && ((v == IVX && f1) || (v == IVY && f2) || (v == IVZ && f3))) x = -x;
-    if (kind != SNAPB_SCALAR && si != i) {
-      if (v == IDN) x += rb[si] - rb[i];
-      if (v == IPR) x += (pb[si] - pb[i]) * (kind == SNAPB_CONSERVED ? igm1 : 1.0);
+  // A thread's source cell is never its target, so the loads of a group of
+  // variables are issued before its stores: the compiler cannot see that the
+  // stores miss the sources and would otherwise wait for one load per
+  // variable.
+  constexpr int kGroup = 8;
+  for (int v0 = 0; v0 < nv; v0 += kGroup) {
+    float xs[kGroup];
+#pragma unroll
+    for (int q = 0; q < kGroup; ++q)
+      if (v0 + q < nv) xs[q] = var[(v0 + q) * sv + src];
+#pragma unroll
+    for (int q = 0; q < kGroup; ++q) {
+      const int v = v0 + q;
+      if (v >= nv) break;
+      double x = xs[q];
+      if (flip && ((v == IVX && f1) || (v == IVY && f2) || (v == IVZ && f3))) x = -x;
+      if (kind != SNAPB_SCALAR && si != i) {
+        if (v == IDN) x += rb[si] - rb[i];
+        if (v == IPR) x += (pb[si] - pb[i]) * (kind == SNAPB_CONSERVED ? igm1 : 1.0);
+      }
+      var[v * sv + t] = (float)x;
     }
-    var[v * sv + t] = (float)x;
   }
 }
 
